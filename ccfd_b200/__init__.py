@@ -1,0 +1,224 @@
+"""ccfd_b200: the residual-and-update path of the 2-D finite-volume solver ccfd
+(hheinzer/ccfd) on NVIDIA B200, behind a C ABI (include/ccfd_b200.h).
+
+The Python layer mirrors the reference's interface for this path:
+
+* :class:`CaseData` -- a case read from a reference ``.ini`` file with the
+  reference's parser semantics (main's init sequence, src/main.c:53-118).
+* :class:`Solver`   -- device state of one case: ``fv_time_derivative``
+  (fvTimeDerivative, src/finiteVolume.c:78), ``calc_time_step``
+  (calcTimeStep, src/timeDiscretization.c:249), ``run`` (the time loop of
+  timeDisc with explicitTimeStepRK / implicitTimeStep), ``global_residual``
+  (src/analyze.c:521) and ``clcd`` (calcCoef, src/analyze.c:292).
+
+Every call goes to the CUDA kernels in ``lib/libccfd_b200.so``; there is no
+CPU implementation behind this package.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+from . import _native as N
+
+__all__ = ["CaseData", "Solver", "CcfdError", "mesh_arrays", "PRIMITIVE", "CONSERVATIVE"]
+
+PRIMITIVE, CONSERVATIVE = N.PRIMITIVE, N.CONSERVATIVE
+
+FLUX_NAMES = {1: "Godunov", 2: "Roe", 3: "HLL", 4: "HLLE", 5: "HLLC", 6: "Lax-Friedrichs",
+              7: "Steger-Warming", 8: "central", 9: "AUSMD", 10: "AUSMDV", 11: "van Leer"}
+
+
+class CcfdError(RuntimeError):
+    def __init__(self, status: int, where: str):
+        msg = N.lib.ccfd_strerror(status).decode()
+        super().__init__(f"{where}: {msg} (status {status})")
+        self.status = status
+
+
+def _check(st: int, where: str) -> None:
+    if st != 0:
+        raise CcfdError(st, where)
+
+
+def _dptr(a: np.ndarray):
+    return a.ctypes.data_as(C.POINTER(C.c_double))
+
+
+def _lptr(a: np.ndarray):
+    return a.ctypes.data_as(C.POINTER(C.c_long))
+
+
+def _arr(ptr, shape, dtype):
+    n = int(np.prod(shape))
+    if n == 0:
+        return np.zeros(shape, dtype=dtype)
+    return np.ctypeslib.as_array(ptr, shape=(n,)).astype(dtype, copy=True).reshape(shape)
+
+
+def mesh_arrays(m: N.Mesh) -> dict:
+    """Copy a ccfd_mesh into numpy arrays (reference element / face order)."""
+    n, f, b, h = m.n_cells, m.n_faces, m.n_bc, m.n_half_sides
+    return {
+        "n_cells": n, "n_faces": f, "n_bc": b, "n_half_sides": h,
+        "cell_type": _arr(m.cell_type, (n,), np.int32),
+        "cell_domain": _arr(m.cell_domain, (n,), np.int32),
+        "cell_bary": _arr(m.cell_bary, (n, 2), np.float64),
+        "cell_geo": _arr(m.cell_geo, (n, 4), np.float64),
+        "hs_offset": _arr(m.hs_offset, (n + 1,), np.int64),
+        "hs_face": _arr(m.hs_face, (h,), np.int64),
+        "hs_sign": _arr(m.hs_sign, (h,), np.int32),
+        "hs_nb": _arr(m.hs_nb, (h,), np.int64),
+        "hs_gp": _arr(m.hs_gp, (h, 2), np.float64),
+        "hs_w": _arr(m.hs_w, (h, 2), np.float64),
+        "face_cells": _arr(m.face_cells, (f, 2), np.int64),
+        "face_hs": _arr(m.face_hs, (f, 2), np.int64),
+        "face_n": _arr(m.face_n, (f, 2), np.float64),
+        "face_len": _arr(m.face_len, (f,), np.float64),
+        "face_bb": _arr(m.face_bb, (f, 3), np.float64),
+        "ghost_gp": _arr(m.ghost_gp, (b, 2), np.float64),
+        "bc_face": _arr(m.bc_face, (b,), np.int64),
+        "bc_index": _arr(m.bc_index, (b,), np.int32),
+        "bc_ghost_bary": _arr(m.bc_ghost_bary, (b, 2), np.float64),
+        "bc_x": _arr(m.bc_x, (b, 2), np.float64),
+        "total_area_q": m.total_area_q, "dx_ref": m.dx_ref,
+        "x_min": m.x_min, "x_max": m.x_max, "y_min": m.y_min, "y_max": m.y_max,
+    }
+
+
+class CaseData:
+    """A case built by the C host layer from a reference ``.ini`` file."""
+
+    def __init__(self, ptr):
+        self._ptr = ptr
+
+    @classmethod
+    def from_ini(cls, path: str) -> "CaseData":
+        p = C.POINTER(N.Case)()
+        _check(N.lib.ccfd_case_load(os.fsencode(path), C.byref(p)), f"load {path}")
+        return cls(p)
+
+    @classmethod
+    def from_text(cls, text: str, base_dir: str | None = None) -> "CaseData":
+        p = C.POINTER(N.Case)()
+        bd = os.fsencode(base_dir) if base_dir else None
+        _check(N.lib.ccfd_case_load_text(text.encode(), bd, C.byref(p)), "load ini text")
+        return cls(p)
+
+    def __del__(self):
+        if getattr(self, "_ptr", None):
+            N.lib.ccfd_case_free(self._ptr)
+            self._ptr = None
+
+    @property
+    def c(self) -> N.Case:
+        return self._ptr.contents
+
+    @property
+    def params(self) -> N.Params:
+        return self.c.params
+
+    @property
+    def n_cells(self) -> int:
+        return self.c.mesh.n_cells
+
+    def mesh(self) -> dict:
+        return mesh_arrays(self.c.mesh)
+
+    def prim0(self) -> np.ndarray:
+        return _arr(self.c.prim0, (self.n_cells, 4), np.float64)
+
+    def venk_eps2(self, venk_k: float | None = None) -> np.ndarray:
+        k = self.params.venk_k if venk_k is None else venk_k
+        out = np.zeros(self.n_cells)
+        N.lib.ccfd_venk_eps2(C.byref(self.c.mesh), k, _dptr(out))
+        return out
+
+    @property
+    def file_name(self) -> str:
+        return self.c.file_name.decode()
+
+
+class Solver:
+    """One case resident on the current CUDA device."""
+
+    def __init__(self, case: CaseData, reorder: bool = True, params: N.Params | None = None):
+        self.case = case
+        self._ctx = C.c_void_p()
+        prm = params if params is not None else case.params
+        _check(N.lib.ccfd_create(C.byref(prm), C.byref(self._ctx)), "ccfd_create")
+        c = case.c
+        _check(N.lib.ccfd_upload_case(self._ctx, C.byref(c.mesh), c.bc_table, c.n_bc_table,
+                                      C.byref(c.exact), int(reorder)), "ccfd_upload_case")
+        self.n = case.n_cells
+        self.set_state(case.prim0(), PRIMITIVE)
+
+    def close(self):
+        if self._ctx:
+            N.lib.ccfd_destroy(self._ctx)
+            self._ctx = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set_state(self, state: np.ndarray, kind: int = PRIMITIVE) -> None:
+        s = np.ascontiguousarray(state, dtype=np.float64).reshape(self.n, 4)
+        _check(N.lib.ccfd_set_state(self._ctx, _dptr(s), kind), "ccfd_set_state")
+
+    def get_state(self, kind: int = PRIMITIVE) -> np.ndarray:
+        out = np.empty((self.n, 4))
+        _check(N.lib.ccfd_get_state(self._ctx, _dptr(out), kind), "ccfd_get_state")
+        return out
+
+    @property
+    def time(self) -> float:
+        t = C.c_double()
+        _check(N.lib.ccfd_get_time(self._ctx, C.byref(t)), "ccfd_get_time")
+        return t.value
+
+    @time.setter
+    def time(self, t: float) -> None:
+        _check(N.lib.ccfd_set_time(self._ctx, float(t)), "ccfd_set_time")
+
+    def fv_time_derivative(self, time: float = 0.0, with_grad: bool = False):
+        """R(U) of the current state; [N, 4] (and [N, 8] limited gradients)."""
+        ut = np.empty((self.n, 4))
+        gr = np.empty((self.n, 8)) if with_grad else None
+        _check(N.lib.ccfd_residual(self._ctx, float(time), _dptr(ut),
+                                   _dptr(gr) if with_grad else None), "ccfd_residual")
+        return (ut, gr) if with_grad else ut
+
+    def calc_time_step(self) -> float:
+        dt = C.c_double()
+        _check(N.lib.ccfd_time_step(self._ctx, C.byref(dt)), "ccfd_time_step")
+        return dt.value
+
+    def global_residual(self) -> np.ndarray:
+        r = np.zeros(4)
+        _check(N.lib.ccfd_global_residual(self._ctx, _dptr(r)), "ccfd_global_residual")
+        return r
+
+    def run(self, nsteps: int = 0) -> dict:
+        """Time steps (explicit or implicit per the case); nsteps <= 0: to the end."""
+        rep = N.Report()
+        fn = N.lib.ccfd_run_implicit if self.case.params.implicit else N.lib.ccfd_run_explicit
+        _check(fn(self._ctx, int(nsteps), C.byref(rep)), "ccfd_run")
+        return report_dict(rep)
+
+    def clcd(self):
+        cl, cd = C.c_double(), C.c_double()
+        _check(N.lib.ccfd_clcd(self._ctx, C.byref(cl), C.byref(cd)), "ccfd_clcd")
+        return cl.value, cd.value
+
+
+def report_dict(rep: N.Report) -> dict:
+    return {"t": rep.t, "dt": rep.dt, "iterations": rep.iterations,
+            "residual": list(rep.residual), "cl": rep.cl, "cd": rep.cd,
+            "converged": bool(rep.converged), "finished": bool(rep.finished),
+            "newton_iterations": rep.newton_iterations, "gmres_iterations": rep.gmres_iterations,
+            "first_residual": list(rep.first_residual), "status": rep.status}

@@ -1,0 +1,669 @@
+// C ABI of the device path: context, one-time mesh upload, state transfer,
+// residual evaluation and explicit time stepping under CUDA graphs.
+#include <cuda_runtime.h>
+#include <math.h>
+#include <stdlib.h>
+#include <string.h>
+
+#include <algorithm>
+#include <vector>
+
+#include "ccfd_b200.h"
+#include "ccfd_ctx.cuh"
+#include "kernels.cuh"
+#include "reorder.h"
+#include "host/ccfd_host.h"
+
+using namespace ccfd;
+
+#define CK(x)                                   \
+    do {                                        \
+        cudaError_t e_ = (x);                   \
+        if (e_ != cudaSuccess) {                \
+            ctx->last_cuda_error = (int)e_;     \
+            return CCFD_ERR_CUDA;               \
+        }                                       \
+    } while (0)
+
+static int status_from_flags(unsigned f) {
+    if (f & FLAG_DT) return CCFD_ERR_DT;
+    if (f & FLAG_VACUUM) return CCFD_ERR_VACUUM;
+    if (f & FLAG_STATE) return CCFD_ERR_STATE;
+    if (f & FLAG_SINGULAR) return CCFD_ERR_SINGULAR;
+    if (f & FLAG_GMRES) return CCFD_ERR_GMRES;
+    return CCFD_OK;
+}
+
+template <typename T>
+static int dalloc(ccfd_ctx* ctx, T** p, size_t n) {
+    void* q = nullptr;
+    if (n == 0) n = 1;
+    cudaError_t e = cudaMalloc(&q, n * sizeof(T));
+    if (e != cudaSuccess) {
+        ctx->last_cuda_error = (int)e;
+        return CCFD_ERR_NOMEM;
+    }
+    ctx->allocs.push_back(q);
+    ctx->device_bytes += n * sizeof(T);
+    *p = (T*)q;
+    return CCFD_OK;
+}
+
+template <typename T>
+static int dupload(ccfd_ctx* ctx, T** p, const std::vector<T>& h) {
+    int st = dalloc(ctx, p, h.size());
+    if (st) return st;
+    if (!h.empty()) CK(cudaMemcpyAsync(*p, h.data(), h.size() * sizeof(T), cudaMemcpyHostToDevice, ctx->stream));
+    return CCFD_OK;
+}
+
+static void free_device(ccfd_ctx* ctx) {
+    if (ctx->graph_many) cudaGraphExecDestroy(ctx->graph_many);
+    if (ctx->graph_one) cudaGraphExecDestroy(ctx->graph_one);
+    ctx->graph_many = ctx->graph_one = nullptr;
+    for (void* p : ctx->allocs) cudaFree(p);
+    ctx->allocs.clear();
+    ctx->device_bytes = 0;
+    ctx->uploaded = false;
+}
+
+extern "C" int ccfd_create(const ccfd_params* params, ccfd_ctx** out) {
+    if (!params || !out) return CCFD_ERR_ARG;
+    *out = nullptr;
+    const ccfd_params& p = *params;
+    if (p.flux < 1 || p.flux > 11 || p.spatial_order < 1 || p.spatial_order > 2 ||
+        (p.spatial_order == 2 && p.limiter != 1 && p.limiter != 2) ||
+        p.time_order < 1 || p.time_order > 3 ||
+        (!(p.n_rk_stages == 1 && p.time_order == 1) && (p.n_rk_stages < 3 || p.n_rk_stages > 5)))
+        return CCFD_ERR_ARG;
+    if (p.time_step_1d && p.mu > 1e-10) return CCFD_ERR_ARG; /* timeDiscretization.c:264-267 */
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) return CCFD_ERR_CUDA;
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return CCFD_ERR_CUDA;
+    ccfd_ctx* ctx = new ccfd_ctx();
+    ctx->params = p;
+    ctx->device = dev;
+    if (cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking) != cudaSuccess) {
+        delete ctx;
+        return CCFD_ERR_CUDA;
+    }
+    if (cudaMallocHost((void**)&ctx->h_ctrl, sizeof(Ctrl)) != cudaSuccess) {
+        cudaStreamDestroy(ctx->stream);
+        delete ctx;
+        return CCFD_ERR_CUDA;
+    }
+    memset(ctx->h_ctrl, 0, sizeof(Ctrl));
+    // RK coefficient tables, src/timeDiscretization.c:94-169
+    double* rk = ctx->rk;
+    for (int i = 0; i < 6; ++i) rk[i] = 0.0;
+    if (p.n_rk_stages == 1 && p.time_order == 1) {
+        rk[1] = 1.0;
+    } else {
+        static const double t3[3][3] = {{0.1418, 0.4, 1.0}, {0.1918, 0.4929, 1.0}, {0.2884, 0.5010, 1.0}};
+        static const double t4[3][4] = {{0.0833, 0.2069, 0.4265, 1.0},
+                                        {0.1084, 0.2602, 0.5052, 1.0},
+                                        {0.1666, 0.3027, 0.5275, 1.0}};
+        static const double t5[3][5] = {{0.0533, 0.1263, 0.2375, 0.4414, 1.0},
+                                        {0.0695, 0.1602, 0.2898, 0.5060, 1.0},
+                                        {0.1067, 0.1979, 0.3232, 0.5201, 1.0}};
+        int o = p.time_order - 1;
+        for (int s = 0; s < p.n_rk_stages; ++s)
+            rk[s + 1] = p.n_rk_stages == 3 ? t3[o][s] : p.n_rk_stages == 4 ? t4[o][s] : t5[o][s];
+    }
+    *out = ctx;
+    return CCFD_OK;
+}
+
+extern "C" void ccfd_destroy(ccfd_ctx* ctx) {
+    if (!ctx) return;
+    cudaStreamSynchronize(ctx->stream);
+    free_device(ctx);
+    if (ctx->h_ctrl) cudaFreeHost(ctx->h_ctrl);
+    cudaStreamDestroy(ctx->stream);
+    delete ctx;
+}
+
+// wing surface faces in the summation order of calcCoef: the pressure-side
+// list then the suction-side list, each built by the insertion of initWing
+// (src/analyze.c:95-184), keyed on the face midpoint x
+static void build_wall_list(const ccfd_mesh* m, const ccfd_bc* bc, int wall_code,
+                            std::vector<int>& order) {
+    std::vector<int> pressure, suction;
+    for (long g = 0; g < m->n_bc; ++g) {
+        const ccfd_bc& b = bc[m->bc_index[g]];
+        if (b.type * 100 + b.id != wall_code) continue;
+        long f = m->bc_face[g];
+        double ghost_ny = -m->face_n[2 * f + 1];
+        std::vector<int>& L = ghost_ny <= 0.0 ? suction : pressure;
+        double xi = m->bc_x[2 * g];
+        size_t pos = L.size();
+        for (size_t k = 0; k < L.size(); ++k)
+            if (xi < m->bc_x[2 * L[k]]) {
+                pos = k;
+                break;
+            }
+        L.insert(L.begin() + pos, (int)g);
+    }
+    order = pressure;
+    order.insert(order.end(), suction.begin(), suction.end());
+}
+
+extern "C" int ccfd_upload_case(ccfd_ctx* ctx, const ccfd_mesh* m, const ccfd_bc* bc, int n_bc,
+                                const ccfd_exact* ex, int reorder) {
+    if (!ctx || !m || (!bc && n_bc > 0) || !ex || n_bc > kMaxBC) return CCFD_ERR_ARG;
+    if (m->n_cells <= 0 || m->n_faces <= 0 || m->n_cells > (1L << 30) || m->n_faces > (1L << 30))
+        return CCFD_ERR_ARG;
+    for (long g = 0; g < m->n_bc; ++g)
+        if (m->bc_index[g] < 0 || m->bc_index[g] >= n_bc) return CCFD_ERR_ARG;
+    CK(cudaSetDevice(ctx->device));
+    free_device(ctx);
+    const ccfd_params& p = ctx->params;
+    const long N = m->n_cells, F = m->n_faces, B = m->n_bc, H = m->n_half_sides;
+    ctx->N = N;
+    ctx->F = F;
+    ctx->B = B;
+
+    // locality ordering of cells and faces (results do not depend on it:
+    // every per-cell and per-face operation keeps the reference's operand
+    // order; only the storage order changes)
+    std::vector<int> cperm, fperm;  // device index -> reference index
+    if (reorder) ccfd_rcm_order(m, cperm, fperm);
+    else {
+        cperm.resize(N);
+        fperm.resize(F);
+        for (long i = 0; i < N; ++i) cperm[i] = (int)i;
+        for (long i = 0; i < F; ++i) fperm[i] = (int)i;
+    }
+    ctx->cell_of_dev = cperm;
+    std::vector<int> cinv(N), finv(F);
+    for (long i = 0; i < N; ++i) cinv[cperm[i]] = (int)i;
+    for (long i = 0; i < F; ++i) finv[fperm[i]] = (int)i;
+    ctx->dev_of_cell = cinv;
+
+    std::vector<int> hs_off(N + 1), hs_nb(H), hs_fs(H);
+    std::vector<double4> hs_gw(H), cell_geo(N);
+    std::vector<double> venk(N, 0.0);
+    std::vector<int> hmap(H);  // reference half-side -> device half-side
+    long k = 0;
+    for (long d = 0; d < N; ++d) {
+        long c = cperm[d];
+        hs_off[d] = (int)k;
+        for (long h = m->hs_offset[c]; h < m->hs_offset[c + 1]; ++h, ++k) {
+            long nb = m->hs_nb[h];
+            hs_nb[k] = nb >= 0 ? cinv[nb] : (int)nb;
+            int fd = finv[m->hs_face[h]];
+            hs_fs[k] = m->hs_sign[h] > 0 ? fd : ~fd;
+            hs_gw[k] = make_double4(m->hs_gp[2 * h], m->hs_gp[2 * h + 1], m->hs_w[2 * h], m->hs_w[2 * h + 1]);
+            hmap[h] = (int)k;
+        }
+        cell_geo[d] = make_double4(m->cell_geo[4 * c], m->cell_geo[4 * c + 1], m->cell_geo[4 * c + 2],
+                                   m->cell_geo[4 * c + 3]);
+    }
+    hs_off[N] = (int)k;
+    if (p.spatial_order == 2 && p.limiter == 2) {
+        std::vector<double> e2(N);
+        ccfd_venk_eps2(m, p.venk_k, e2.data());
+        for (long d = 0; d < N; ++d) venk[d] = e2[cperm[d]];
+    }
+    std::vector<int2> face_c(F);
+    std::vector<double4> face_gp(F), face_nl(F), face_bb(F);
+    for (long fd = 0; fd < F; ++fd) {
+        long f = fperm[fd];
+        long c0 = m->face_cells[2 * f], c1 = m->face_cells[2 * f + 1];
+        face_c[fd] = make_int2(cinv[c0], c1 >= 0 ? cinv[c1] : (int)c1);
+        long h0 = m->face_hs[2 * f], h1 = m->face_hs[2 * f + 1];
+        double g1x = 0.0, g1y = 0.0;
+        if (h1 >= 0) {
+            g1x = m->hs_gp[2 * h1];
+            g1y = m->hs_gp[2 * h1 + 1];
+        }
+        face_gp[fd] = make_double4(m->hs_gp[2 * h0], m->hs_gp[2 * h0 + 1], g1x, g1y);
+        face_nl[fd] = make_double4(m->face_n[2 * f], m->face_n[2 * f + 1], m->face_len[f], 0.0);
+        face_bb[fd] = make_double4(m->face_bb[3 * f], m->face_bb[3 * f + 1], m->face_bb[3 * f + 2], 0.0);
+    }
+    std::vector<int> ghost_bc(B + 1);
+    std::vector<double4> ghost_gn(B + 1);
+    std::vector<double2> ghost_mid(B + 1);
+    for (long g = 0; g < B; ++g) {
+        long f = m->bc_face[g];
+        ghost_bc[g] = m->bc_index[g];
+        ghost_gn[g] = make_double4(m->bc_ghost_bary[2 * g], m->bc_ghost_bary[2 * g + 1], m->face_n[2 * f],
+                                   m->face_n[2 * f + 1]);
+        ghost_mid[g] = make_double2(m->bc_x[2 * g], m->bc_x[2 * g + 1]);
+    }
+
+    int st;
+    int *d_hs_off, *d_hs_nb, *d_hs_fs, *d_ghost_bc;
+    double4 *d_hs_gw, *d_cell_geo, *d_face_gp, *d_face_nl, *d_face_bb, *d_ghost_gn;
+    double* d_venk;
+    int2* d_face_c;
+    double2* d_ghost_mid;
+    if ((st = dupload(ctx, &d_hs_off, hs_off)) || (st = dupload(ctx, &d_hs_nb, hs_nb)) ||
+        (st = dupload(ctx, &d_hs_fs, hs_fs)) || (st = dupload(ctx, &d_hs_gw, hs_gw)) ||
+        (st = dupload(ctx, &d_cell_geo, cell_geo)) || (st = dupload(ctx, &d_venk, venk)) ||
+        (st = dupload(ctx, &d_face_c, face_c)) || (st = dupload(ctx, &d_face_gp, face_gp)) ||
+        (st = dupload(ctx, &d_face_nl, face_nl)) || (st = dupload(ctx, &d_face_bb, face_bb)) ||
+        (st = dupload(ctx, &d_ghost_bc, ghost_bc)) || (st = dupload(ctx, &d_ghost_gn, ghost_gn)) ||
+        (st = dupload(ctx, &d_ghost_mid, ghost_mid))) {
+        free_device(ctx);
+        return st;
+    }
+    DevMesh& dm = ctx->mesh;
+    dm.N = (int)N;
+    dm.F = (int)F;
+    dm.B = (int)B;
+    dm.H = (int)H;
+    dm.hs_off = d_hs_off;
+    dm.hs_nb = d_hs_nb;
+    dm.hs_fs = d_hs_fs;
+    dm.hs_gw = d_hs_gw;
+    dm.cell_geo = d_cell_geo;
+    dm.venk_eps2 = d_venk;
+    dm.face_c = d_face_c;
+    dm.face_gp = d_face_gp;
+    dm.face_nl = d_face_nl;
+    dm.face_bb = d_face_bb;
+    dm.ghost_bc = d_ghost_bc;
+    dm.ghost_gn = d_ghost_gn;
+    dm.ghost_mid = d_ghost_mid;
+
+    // physics constants (src/equation.c:572-578)
+    Phys& P = ctx->phys;
+    memset(&P, 0, sizeof(P));
+    P.gam = p.gamma;
+    P.gam1 = p.gamma - 1.0;
+    P.gam1q = 1.0 / P.gam1;
+    P.mu = p.eqn == CCFD_NAVIER_STOKES ? p.mu : 0.0;
+    P.Pr = p.eqn == CCFD_NAVIER_STOKES ? p.Pr : 0.72;
+    P.pi = acos(-1.0);
+    P.sqrt3q = 1 / sqrt(3.0);
+    P.nbc = n_bc;
+    P.order = p.spatial_order;
+    P.eqn = p.eqn;
+    for (int i = 0; i < n_bc; ++i) {
+        P.bc[i].type = bc[i].type;
+        P.bc[i].exact_func = bc[i].exact_func;
+        for (int v = 0; v < 4; ++v) P.bc[i].pvar[v] = bc[i].pvar[v];
+    }
+    memcpy(P.ex.ref_state, ex->ref_state, sizeof(P.ex.ref_state));
+    P.ex.rp1d_interface = ex->rp1d_interface;
+    P.ex.x_min = ex->x_min;
+    P.ex.x_max = ex->x_max;
+    P.ex.y_min = ex->y_min;
+    P.ex.y_max = ex->y_max;
+    P.ex.dx_ref = ex->dx_ref;
+    ctx->total_area_q = m->total_area_q;
+    ctx->exact = *ex;
+
+    // wing surface list for CL / CD
+    std::vector<int> wl;
+    std::vector<double> wnl;
+    if (p.calc_wing) build_wall_list(m, bc, p.wall_id, wl);
+    for (int g : wl) {
+        long f = m->bc_face[g];
+        wnl.push_back(m->face_n[2 * f]);
+        wnl.push_back(m->face_n[2 * f + 1]);
+        wnl.push_back(m->face_len[f]);
+    }
+    ctx->n_wall = (int)wl.size();
+    if ((st = dupload(ctx, &ctx->wall_ghost, wl)) || (st = dupload(ctx, &ctx->wall_nl, wnl))) {
+        free_device(ctx);
+        return st;
+    }
+
+    // state and scratch
+    ctx->nb_cells = (int)((N + 255) / 256);
+    if ((st = dalloc(ctx, &ctx->prim, N)) || (st = dalloc(ctx, &ctx->cons0, N)) ||
+        (st = dalloc(ctx, &ctx->grad, 2 * N)) || (st = dalloc(ctx, &ctx->flux, F)) ||
+        (st = dalloc(ctx, &ctx->u_t, N)) || (st = dalloc(ctx, &ctx->ghost_pface, B + 1)) ||
+        (st = dalloc(ctx, &ctx->flags, 1)) || (st = dalloc(ctx, &ctx->ctrl, 1)) ||
+        (st = dalloc(ctx, &ctx->dt_partial, ctx->nb_cells)) ||
+        (st = dalloc(ctx, &ctx->dt_bad, ctx->nb_cells)) ||
+        (st = dalloc(ctx, &ctx->res_partial, 4 * (size_t)ctx->nb_cells))) {
+        free_device(ctx);
+        return st;
+    }
+    CK(cudaMemsetAsync(ctx->flags, 0, sizeof(unsigned), ctx->stream));
+    CK(cudaMemsetAsync(ctx->ghost_pface, 0, sizeof(double) * (B + 1), ctx->stream));
+    CK(cudaMemsetAsync(ctx->grad, 0, sizeof(double4) * 2 * N, ctx->stream));
+
+    // control block: t = 0, printTime / printIter of initTimeDisc
+    // (src/timeDiscretization.c:238-239)
+    Ctrl& c = *ctx->h_ctrl;
+    memset(&c, 0, sizeof(Ctrl));
+    c.t = 0.0;
+    c.stop_time = p.t_end;
+    c.io_time_interval = p.io_time_interval;
+    c.io_iter_interval = p.io_iter_interval > 0 ? p.io_iter_interval : 1;
+    c.print_time = (floor(0.0 / p.io_time_interval) + 1) * p.io_time_interval;
+    c.print_iter = (0 / c.io_iter_interval + 1) * c.io_iter_interval;
+    c.max_iter = p.max_iter;
+    c.stop_at = 0;
+    CK(cudaMemcpyAsync(ctx->ctrl, ctx->h_ctrl, sizeof(Ctrl), cudaMemcpyHostToDevice, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+
+    // step parameters
+    StepParams& sp = ctx->sp;
+    memset(&sp, 0, sizeof(sp));
+    sp.cfl = p.cfl;
+    sp.dfl = p.dfl;
+    sp.gam_pr_max = fmax(4.0 / 3.0, P.gam / P.Pr);
+    for (int i = 0; i < 6; ++i) sp.rk[i] = ctx->rk[i];
+    sp.nrk = (p.n_rk_stages == 1 && p.time_order == 1) ? 1 : p.n_rk_stages;
+    sp.ts1d = p.time_step_1d;
+    sp.visc = P.mu > 1e-10;
+    sp.stationary = p.stationary;
+    sp.abort_variable = p.abort_variable;
+    sp.abort_residual = p.abort_residual;
+    sp.cl_abort = p.cl_abort_residual;
+    sp.cd_abort = p.cd_abort_residual;
+    sp.abort_on_cl = p.cl_abort_residual > 0.0;
+    sp.abort_on_cd = !sp.abort_on_cl && p.cd_abort_residual > 0.0;
+    sp.rel_abort = p.rel_abort_residual;
+    sp.calc_wing = p.calc_wing && ctx->n_wall > 0;
+    sp.n_wall = ctx->n_wall;
+    {
+        double pi = acos(-1.0);
+        double v = ex->ref_state[0][1] / cos(ex->alpha * pi / 180.0);
+        double q_inf_q = 1.0 / (ex->ref_state[0][0] * 0.5 * v * v);
+        sp.q_inf_lq = q_inf_q / p.ref_length;
+        double a = ex->alpha * pi / 180.0;
+        sp.cos_a = cos(a);
+        sp.sin_a = sin(a);
+    }
+    sp.total_area_q = m->total_area_q;
+    ctx->uploaded = true;
+    return CCFD_OK;
+}
+
+static void fill_residual_launch(ccfd_ctx* ctx, ResidualLaunch& L) {
+    memset(&L, 0, sizeof(L));
+    L.mesh = ctx->mesh;
+    L.phys = ctx->phys;
+    L.order = ctx->params.spatial_order;
+    L.limiter = ctx->params.limiter;
+    L.flux_id = ctx->params.flux;
+    L.ns = ctx->params.eqn == CCFD_NAVIER_STOKES;
+    L.prim = ctx->prim;
+    L.grad = ctx->grad;
+    L.flux = ctx->flux;
+    L.ghost_pface = ctx->ghost_pface;
+    L.flags = ctx->flags;
+}
+
+static int check_flags(ccfd_ctx* ctx) {
+    unsigned f = 0;
+    CK(cudaMemcpyAsync(&f, ctx->flags, sizeof(unsigned), cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    if (f) CK(cudaMemsetAsync(ctx->flags, 0, sizeof(unsigned), ctx->stream));
+    return status_from_flags(f);
+}
+
+extern "C" int ccfd_set_state(ccfd_ctx* ctx, const double* state, int kind) {
+    if (!ctx || !state || !ctx->uploaded) return CCFD_ERR_ARG;
+    CK(cudaSetDevice(ctx->device));
+    const long N = ctx->N;
+    std::vector<double4> prim(N), cons(N);
+    double gam1 = ctx->phys.gam1, gam1q = ctx->phys.gam1q;
+    for (long d = 0; d < N; ++d) {
+        const double* s = &state[4 * ctx->cell_of_dev[d]];
+        double pv[4], cv[4];
+        if (kind == CCFD_CONSERVATIVE) {
+            memcpy(cv, s, sizeof(cv));
+            ccfd_host_cons_prim(gam1, cv, pv);
+        } else {
+            memcpy(pv, s, sizeof(pv));
+            ccfd_host_prim_cons(gam1q, pv, cv);
+        }
+        prim[d] = make_double4(pv[0], pv[1], pv[2], pv[3]);
+        cons[d] = make_double4(cv[0], cv[1], cv[2], cv[3]);
+    }
+    CK(cudaMemcpyAsync(ctx->prim, prim.data(), sizeof(double4) * N, cudaMemcpyHostToDevice, ctx->stream));
+    CK(cudaMemcpyAsync(ctx->cons0, cons.data(), sizeof(double4) * N, cudaMemcpyHostToDevice, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    return CCFD_OK;
+}
+
+extern "C" int ccfd_get_state(ccfd_ctx* ctx, double* state, int kind) {
+    if (!ctx || !state || !ctx->uploaded) return CCFD_ERR_ARG;
+    CK(cudaSetDevice(ctx->device));
+    const long N = ctx->N;
+    std::vector<double4> h(N);
+    CK(cudaMemcpyAsync(h.data(), kind == CCFD_CONSERVATIVE ? ctx->cons0 : ctx->prim, sizeof(double4) * N,
+                       cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    for (long d = 0; d < N; ++d) {
+        double* s = &state[4 * ctx->cell_of_dev[d]];
+        s[0] = h[d].x; s[1] = h[d].y; s[2] = h[d].z; s[3] = h[d].w;
+    }
+    return CCFD_OK;
+}
+
+extern "C" int ccfd_set_time(ccfd_ctx* ctx, double t) {
+    if (!ctx || !ctx->uploaded) return CCFD_ERR_ARG;
+    CK(cudaSetDevice(ctx->device));
+    CK(cudaMemcpyAsync(ctx->h_ctrl, ctx->ctrl, sizeof(Ctrl), cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    Ctrl& c = *ctx->h_ctrl;
+    c.t = t;
+    c.print_time = (floor(t / ctx->params.io_time_interval) + 1) * ctx->params.io_time_interval;
+    c.done = c.finished = c.converged = c.max_iter_hit = 0;
+    c.flags = 0;
+    CK(cudaMemcpyAsync(ctx->ctrl, ctx->h_ctrl, sizeof(Ctrl), cudaMemcpyHostToDevice, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    return CCFD_OK;
+}
+
+extern "C" int ccfd_get_time(ccfd_ctx* ctx, double* t) {
+    if (!ctx || !t || !ctx->uploaded) return CCFD_ERR_ARG;
+    CK(cudaSetDevice(ctx->device));
+    CK(cudaMemcpyAsync(ctx->h_ctrl, ctx->ctrl, sizeof(Ctrl), cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    *t = ctx->h_ctrl->t;
+    return CCFD_OK;
+}
+
+// Residual of the current state into ctx->u_t (device); no host copies.
+int ccfd_residual_device(ccfd_ctx* ctx, double time) {
+    ResidualLaunch L;
+    fill_residual_launch(ctx, L);
+    L.ctrl = nullptr;
+    L.tfix = time;
+    L.update_mode = 0;
+    L.u_t = ctx->u_t;
+    L.res_partial = ctx->res_partial;
+    launch_residual(L, ctx->stream);
+    CK(cudaGetLastError());
+    return CCFD_OK;
+}
+
+extern "C" int ccfd_residual(ccfd_ctx* ctx, double time, double* u_t_out, double* grad_out) {
+    if (!ctx || !ctx->uploaded) return CCFD_ERR_ARG;
+    CK(cudaSetDevice(ctx->device));
+    int st = ccfd_residual_device(ctx, time);
+    if (st) return st;
+    const long N = ctx->N;
+    if (u_t_out) {
+        std::vector<double4> h(N);
+        CK(cudaMemcpyAsync(h.data(), ctx->u_t, sizeof(double4) * N, cudaMemcpyDeviceToHost, ctx->stream));
+        CK(cudaStreamSynchronize(ctx->stream));
+        for (long d = 0; d < N; ++d) {
+            double* s = &u_t_out[4 * ctx->cell_of_dev[d]];
+            s[0] = h[d].x; s[1] = h[d].y; s[2] = h[d].z; s[3] = h[d].w;
+        }
+    }
+    if (grad_out) {
+        std::vector<double4> h(2 * N);
+        CK(cudaMemcpyAsync(h.data(), ctx->grad, sizeof(double4) * 2 * N, cudaMemcpyDeviceToHost, ctx->stream));
+        CK(cudaStreamSynchronize(ctx->stream));
+        for (long d = 0; d < N; ++d) {
+            double* s = &grad_out[8 * ctx->cell_of_dev[d]];
+            s[0] = h[2 * d].x; s[1] = h[2 * d].y; s[2] = h[2 * d].z; s[3] = h[2 * d].w;
+            s[4] = h[2 * d + 1].x; s[5] = h[2 * d + 1].y; s[6] = h[2 * d + 1].z; s[7] = h[2 * d + 1].w;
+        }
+    }
+    return check_flags(ctx);
+}
+
+extern "C" int ccfd_global_residual(ccfd_ctx* ctx, double res[4]) {
+    if (!ctx || !res || !ctx->uploaded) return CCFD_ERR_ARG;
+    CK(cudaSetDevice(ctx->device));
+    std::vector<double> h(4 * (size_t)ctx->nb_cells);
+    CK(cudaMemcpyAsync(h.data(), ctx->res_partial, sizeof(double) * h.size(), cudaMemcpyDeviceToHost,
+                       ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    double s[4] = {0, 0, 0, 0};
+    for (int b = 0; b < ctx->nb_cells; ++b)
+        for (int v = 0; v < 4; ++v) s[v] += h[4 * b + v];
+    for (int v = 0; v < 4; ++v) res[v] = sqrt(s[v] * ctx->total_area_q);
+    return CCFD_OK;
+}
+
+extern "C" int ccfd_time_step(ccfd_ctx* ctx, double* dt_out) {
+    if (!ctx || !dt_out || !ctx->uploaded) return CCFD_ERR_ARG;
+    CK(cudaSetDevice(ctx->device));
+    launch_dt(ctx->mesh, ctx->phys, nullptr, ctx->sp, ctx->prim, ctx->dt_partial, ctx->dt_bad, ctx->stream);
+    CK(cudaGetLastError());
+    std::vector<double2> part(ctx->nb_cells);
+    std::vector<int> bad(ctx->nb_cells);
+    CK(cudaMemcpyAsync(part.data(), ctx->dt_partial, sizeof(double2) * part.size(), cudaMemcpyDeviceToHost,
+                       ctx->stream));
+    CK(cudaMemcpyAsync(bad.data(), ctx->dt_bad, sizeof(int) * bad.size(), cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaMemcpyAsync(ctx->h_ctrl, ctx->ctrl, sizeof(Ctrl), cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    double a = 1e150, b = 1e150;
+    for (int i = 0; i < ctx->nb_cells; ++i) {
+        if (bad[i]) return CCFD_ERR_DT;
+        a = fmin(a, part[i].x);
+        b = fmin(b, part[i].y);
+    }
+    double dt = ctx->sp.ts1d ? a : fmin(a, b);
+    const Ctrl& c = *ctx->h_ctrl;
+    double t = c.t, pT = c.print_time, sT = c.stop_time;
+    if ((t + dt > pT) || (t + dt > sT)) dt = fmin(pT, sT) - t;
+    else if ((t + 1.5 * dt > pT) || (t + 1.5 * dt > sT)) dt = 0.5 * (fmin(pT, sT) - t);
+    *dt_out = dt;
+    return CCFD_OK;
+}
+
+// record one explicit time step into the stream (graph capture)
+static void record_step(ccfd_ctx* ctx) {
+    const StepParams& sp = ctx->sp;
+    launch_dt(ctx->mesh, ctx->phys, ctx->ctrl, sp, ctx->prim, ctx->dt_partial, ctx->dt_bad, ctx->stream);
+    launch_step_begin(ctx->ctrl, sp, ctx->dt_partial, ctx->dt_bad, ctx->nb_cells, ctx->stream);
+    for (int s = 1; s <= sp.nrk; ++s) {
+        ResidualLaunch L;
+        fill_residual_launch(ctx, L);
+        L.ctrl = ctx->ctrl;
+        L.a_time = sp.rk[s - 1];
+        L.update_mode = 1;
+        L.cons0 = ctx->cons0;
+        L.prim_out = ctx->prim;
+        L.u_t = (s == sp.nrk) ? ctx->u_t : nullptr;
+        L.rk = sp.rk[s];
+        L.last_stage = s == sp.nrk;
+        L.res_partial = (s == sp.nrk) ? ctx->res_partial : nullptr;
+        launch_residual(L, ctx->stream);
+    }
+    launch_step_end(ctx->ctrl, sp, ctx->res_partial, ctx->nb_cells, ctx->wall_ghost, ctx->wall_nl,
+                    ctx->ghost_pface, ctx->stream);
+}
+
+static int build_graph(ccfd_ctx* ctx, int steps, cudaGraphExec_t* exec) {
+    cudaGraph_t g;
+    CK(cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
+    for (int i = 0; i < steps; ++i) record_step(ctx);
+    cudaError_t e = cudaStreamEndCapture(ctx->stream, &g);
+    if (e != cudaSuccess) {
+        ctx->last_cuda_error = (int)e;
+        return CCFD_ERR_CUDA;
+    }
+    e = cudaGraphInstantiate(exec, g, 0);
+    cudaGraphDestroy(g);
+    if (e != cudaSuccess) {
+        ctx->last_cuda_error = (int)e;
+        return CCFD_ERR_CUDA;
+    }
+    return CCFD_OK;
+}
+
+static void fill_report(ccfd_ctx* ctx, ccfd_report* r) {
+    const Ctrl& c = *ctx->h_ctrl;
+    memset(r, 0, sizeof(*r));
+    r->t = c.t;
+    r->dt = c.dt;
+    r->iterations = c.iter;
+    for (int v = 0; v < 6; ++v) r->residual[v] = c.res[v];
+    for (int v = 0; v < 4; ++v) r->first_residual[v] = c.res_first[v];
+    r->cl = c.cl;
+    r->cd = c.cd;
+    r->converged = c.converged;
+    r->finished = c.finished;
+    r->newton_iterations = ctx->newton_total;
+    r->gmres_iterations = ctx->gmres_total;
+    r->status = status_from_flags(c.flags);
+}
+
+extern "C" int ccfd_run_explicit(ccfd_ctx* ctx, long nsteps, ccfd_report* report) {
+    if (!ctx || !ctx->uploaded) return CCFD_ERR_ARG;
+    if (ctx->params.implicit) return ccfd_run_implicit(ctx, nsteps, report);
+    CK(cudaSetDevice(ctx->device));
+    int st;
+    const int kMany = 16;
+    if (!ctx->graph_one && (st = build_graph(ctx, 1, &ctx->graph_one))) return st;
+    if (!ctx->graph_many && (st = build_graph(ctx, kMany, &ctx->graph_many))) return st;
+    // read the control block, set the step budget of this call
+    CK(cudaMemcpyAsync(ctx->h_ctrl, ctx->ctrl, sizeof(Ctrl), cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    Ctrl& c = *ctx->h_ctrl;
+    const long long big = (1LL << 62);
+    long long stop_at = nsteps > 0 ? c.iter + nsteps : big;
+    c.stop_at = stop_at;
+    CK(cudaMemcpyAsync(&ctx->ctrl->stop_at, &c.stop_at, sizeof(long long), cudaMemcpyHostToDevice,
+                       ctx->stream));
+    while (!c.done && c.iter < stop_at) {
+        long long remaining = stop_at - c.iter;
+        if (remaining >= kMany) {
+            for (int rep = 0; rep < 4 && remaining >= (long long)kMany * (rep + 1); ++rep)
+                CK(cudaGraphLaunch(ctx->graph_many, ctx->stream));
+        } else {
+            CK(cudaGraphLaunch(ctx->graph_one, ctx->stream));
+        }
+        CK(cudaMemcpyAsync(ctx->h_ctrl, ctx->ctrl, sizeof(Ctrl), cudaMemcpyDeviceToHost, ctx->stream));
+        CK(cudaStreamSynchronize(ctx->stream));
+    }
+    unsigned f = 0;
+    CK(cudaMemcpyAsync(&f, ctx->flags, sizeof(unsigned), cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    if (report) fill_report(ctx, report);
+    int s1 = status_from_flags(c.flags | f);
+    if (s1) return s1;
+    return CCFD_OK;
+}
+
+extern "C" int ccfd_clcd(ccfd_ctx* ctx, double* cl, double* cd) {
+    if (!ctx || !ctx->uploaded || !cl || !cd) return CCFD_ERR_ARG;
+    CK(cudaSetDevice(ctx->device));
+    if (!ctx->params.calc_wing || ctx->n_wall == 0) return CCFD_ERR_ARG;
+    std::vector<double> pf(ctx->B + 1);
+    std::vector<int> wl(ctx->n_wall);
+    std::vector<double> wnl(3 * ctx->n_wall);
+    CK(cudaMemcpyAsync(pf.data(), ctx->ghost_pface, sizeof(double) * pf.size(), cudaMemcpyDeviceToHost,
+                       ctx->stream));
+    CK(cudaMemcpyAsync(wl.data(), ctx->wall_ghost, sizeof(int) * wl.size(), cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaMemcpyAsync(wnl.data(), ctx->wall_nl, sizeof(double) * wnl.size(), cudaMemcpyDeviceToHost,
+                       ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    double l = 0.0, d = 0.0;
+    for (int k = 0; k < ctx->n_wall; ++k) {
+        double p0 = pf[wl[k]];
+        l += wnl[3 * k + 1] * p0 * wnl[3 * k + 2];
+        d += wnl[3 * k] * p0 * wnl[3 * k + 2];
+    }
+    l *= ctx->sp.q_inf_lq;
+    d *= ctx->sp.q_inf_lq;
+    *cl = l * ctx->sp.cos_a - d * ctx->sp.sin_a;
+    *cd = d * ctx->sp.cos_a + l * ctx->sp.sin_a;
+    return CCFD_OK;
+}

@@ -1,0 +1,51 @@
+// Device context of one solver instance (one mesh, one state) on one GPU.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <vector>
+
+#include "ccfd_b200.h"
+#include "solver.cuh"
+
+struct ccfd_ctx {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    ccfd_params params;
+    ccfd::Phys phys;
+    ccfd::StepParams sp;
+    ccfd::DevMesh mesh;
+    ccfd_exact exact;
+    double rk[6];
+    double total_area_q = 0.0;
+    long N = 0, F = 0, B = 0;
+    bool uploaded = false;
+    int last_cuda_error = 0;
+    size_t device_bytes = 0;
+    std::vector<void*> allocs;
+    std::vector<int> cell_of_dev;  // device cell -> reference cell
+    std::vector<int> dev_of_cell;  // reference cell -> device cell
+    // state and scratch
+    double4* prim = nullptr;
+    double4* cons0 = nullptr;
+    double4* grad = nullptr;
+    double4* flux = nullptr;
+    double4* u_t = nullptr;
+    double* ghost_pface = nullptr;
+    unsigned* flags = nullptr;
+    ccfd::Ctrl* ctrl = nullptr;
+    ccfd::Ctrl* h_ctrl = nullptr;
+    double2* dt_partial = nullptr;
+    int* dt_bad = nullptr;
+    double* res_partial = nullptr;
+    int nb_cells = 0;
+    int* wall_ghost = nullptr;
+    double* wall_nl = nullptr;
+    int n_wall = 0;
+    cudaGraphExec_t graph_one = nullptr, graph_many = nullptr;
+    long newton_total = 0, gmres_total = 0;
+    void* implicit_state = nullptr;  // owned by the implicit solver
+};
+
+// device-side residual of the current state into ctx->u_t (abi.cu)
+int ccfd_residual_device(ccfd_ctx* ctx, double time);

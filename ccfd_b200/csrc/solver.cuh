@@ -1,0 +1,68 @@
+// Device data layout and kernel declarations of the residual-and-update path.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "physics.cuh"
+
+namespace ccfd {
+
+// Mesh in device memory, uploaded once (32-bit indices; AoS records of 32 B
+// so that every gather of a cell / face record is one 32-byte sector).
+struct DevMesh {
+    int N, F, B, H;
+    const int* hs_off;        // [N+1] CSR offsets of the per-cell half-sides
+    const int* hs_nb;         // [H] neighbour cell, or -1-g for ghost g
+    const int* hs_fs;         // [H] face index f (cell owns f) or ~f
+    const double4* hs_gw;     // [H] (GP.x, GP.y, w.x, w.y)
+    const double4* cell_geo;  // [N] (area, 1/area, sx, sy)
+    const double* venk_eps2;  // [N] Venkatakrishnan epsilon^2
+    const int2* face_c;       // [F] (owner, neighbour or -1-g)
+    const double4* face_gp;   // [F] (owner GP.x, GP.y, neighbour GP.x, GP.y)
+    const double4* face_nl;   // [F] (n.x, n.y, len, 0)
+    const double4* face_bb;   // [F] (baryBaryVec.x, .y, baryBaryDist, 0)
+    const int* ghost_bc;      // [B] BC table index
+    const double4* ghost_gn;  // [B] (ghost bary.x, .y, n.x, n.y)
+    const double2* ghost_mid; // [B] face midpoint (exact-solution point)
+};
+
+// Time-loop control block in device memory.  The time step, simulation time,
+// output clamps and stop tests of timeDisc (src/timeDiscretization.c:
+// 595-731) run on the device so that many steps are replayed as one CUDA
+// graph without host round trips.
+struct Ctrl {
+    double t, dt, print_time, stop_time;
+    double io_time_interval;
+    long long iter, print_iter, io_iter_interval, max_iter, stop_at;
+    int active;      // this step runs
+    int done;        // no further steps (finished / converged / error / maxIter)
+    int finished;    // stopTime reached
+    int converged;   // stationary abort criterion met
+    int max_iter_hit;
+    unsigned flags;  // DevFlag bits
+    double res[6];
+    double res_first[4];
+    int have_first;
+    double cl, cd;
+    double visc_dominates;
+};
+
+// Run parameters of the explicit integrator (kernel argument).
+struct StepParams {
+    double cfl, dfl, gam_pr_max;
+    double rk[6];
+    int nrk;
+    int ts1d;
+    int visc;             // mu > 1e-10
+    int stationary;
+    int abort_variable;
+    double abort_residual, cl_abort, cd_abort, rel_abort;
+    int abort_on_cl, abort_on_cd;
+    int calc_wing;
+    int n_wall;           // wall faces in CL/CD summation order
+    double q_inf_lq, cos_a, sin_a;
+    double total_area_q;
+};
+
+}  // namespace ccfd

@@ -1,0 +1,276 @@
+/*
+ * ccfd_b200 -- B200-native residual-and-update path of the 2-D finite-volume
+ * Euler / Navier-Stokes solver ccfd (hheinzer/ccfd), behind a C ABI.
+ *
+ * The reference has no plugin layer: its hot path is a set of global-state C
+ * functions.  Each entry point below names the reference function or global it
+ * replaces (paths relative to the reference project root).  Everything here is
+ * plain C: pointers, sizes and status codes, no CUDA or torch types.  All
+ * arrays passed in are owned by the caller and copied; nothing is retained.
+ *
+ * Threading: a context is used by one host thread at a time; distinct
+ * contexts are independent (the reference is single-instance and global).
+ * Errors: every call returns a status (0 = CCFD_OK).  The reference prints a
+ * message and calls exit(1) instead; ccfd_strerror() gives the message and the
+ * C driver (ccfd_run) maps a non-zero status to the same exit(1).
+ */
+#ifndef CCFD_B200_H
+#define CCFD_B200_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---------------------------------------------------------------- status */
+enum ccfd_status {
+	CCFD_OK = 0,
+	CCFD_ERR_ARG = 1,          /* invalid argument / call order            */
+	CCFD_ERR_CUDA = 2,         /* CUDA runtime failure                     */
+	CCFD_ERR_NOMEM = 3,        /* host or device allocation failed         */
+	CCFD_ERR_DT = 4,           /* non-finite time step, timeDiscretization.c:260-263,283-286,302-305 */
+	CCFD_ERR_NEWTON = 5,       /* Newton not converged, timeDiscretization.c:544-549 */
+	CCFD_ERR_SINGULAR = 6,     /* singular LU-SGS diagonal block, linearSolver.c:245-249 */
+	CCFD_ERR_VACUUM = 7,       /* vacuum in exact Riemann solver, exactRiemann.c:77-90 */
+	CCFD_ERR_TIMEOUT = 8,      /* bounded device wait gave up              */
+	CCFD_ERR_INI = 9,          /* missing / invalid .ini key, readInTools.c:180-184 */
+	CCFD_ERR_MESH = 10,        /* mesh read / connectivity error, mesh.c   */
+	CCFD_ERR_STATE = 11,       /* non-finite state or residual             */
+	CCFD_ERR_BUDGET = 12,      /* request exceeds the device-memory budget */
+	CCFD_ERR_UNSUPPORTED = 13, /* option not built (e.g. periodic BC)      */
+	CCFD_ERR_NOT_CONVERGED = 14, /* maxIter reached, timeDiscretization.c:737-750 */
+	CCFD_ERR_GMRES = 15          /* GMRES breakdown (zero Hessenberg pivot)  */
+};
+
+/* enumerations: numbering identical to the reference's src/main.h */
+enum ccfd_flux {               /* src/main.h:76-88 */
+	CCFD_FLUX_GODUNOV = 1, CCFD_FLUX_ROE, CCFD_FLUX_HLL, CCFD_FLUX_HLLE,
+	CCFD_FLUX_HLLC, CCFD_FLUX_LXF, CCFD_FLUX_STEGER_WARMING,
+	CCFD_FLUX_CENTRAL, CCFD_FLUX_AUSMD, CCFD_FLUX_AUSMDV, CCFD_FLUX_VANLEER
+};
+enum ccfd_limiter {            /* src/main.h:93-96 */
+	CCFD_LIM_BARTH_JESPERSEN = 1, CCFD_LIM_VENKATAKRISHNAN = 2
+};
+enum ccfd_bc_type {            /* src/main.h:44-53; BC code = type*100 + id */
+	CCFD_BC_SLIPWALL = 1, CCFD_BC_WALL, CCFD_BC_INFLOW, CCFD_BC_OUTFLOW,
+	CCFD_BC_CHARACTERISTIC, CCFD_BC_EXACTSOL, CCFD_BC_PERIODIC,
+	CCFD_BC_PRESSURE_OUT
+};
+enum ccfd_eqn { CCFD_EULER = 0, CCFD_NAVIER_STOKES = 1 }; /* -Deuler / -Dnavierstokes */
+enum ccfd_precision {
+	CCFD_FP64 = 0,   /* every operation in FP64, as the reference          */
+	CCFD_MIXED = 1   /* FP32 face fluxes / sweeps / Krylov basis, FP64
+			    accumulation, state, FD difference, Newton update  */
+};
+enum ccfd_state_kind { CCFD_PRIMITIVE = 0, CCFD_CONSERVATIVE = 1 };
+
+/* ------------------------------------------------------------ parameters */
+/* Replaces the globals set by initEquation (src/equation.c:40-124), initFV
+ * (src/finiteVolume.c:30-65), initTimeDisc (src/timeDiscretization.c:69-240),
+ * initLinearSolver (src/linearSolver.c:68-107) and initAnalyze
+ * (src/analyze.c:199-280). */
+typedef struct ccfd_params {
+	int eqn;               /* enum ccfd_eqn                                 */
+	int flux;              /* enum ccfd_flux (fluxFunction)                 */
+	int spatial_order;     /* 1 or 2 (spatialOrder)                         */
+	int limiter;           /* enum ccfd_limiter (limiter)                   */
+	double venk_k;         /* venk_k                                        */
+	double gamma, R, mu, Pr;
+	int time_order;        /* timeOrder 1..3                                */
+	int n_rk_stages;       /* nRKstages 1..5                                */
+	double cfl, dfl;
+	int time_step_1d;      /* timeStep1D                                    */
+	int stationary;        /* stationary                                    */
+	double t_end;          /* tEnd                                          */
+	long max_iter;         /* maxIter                                       */
+	double io_time_interval; /* IOtimeInterval (clamps dt, timeDiscretization.c:317-321) */
+	long io_iter_interval;   /* IOiterInterval                              */
+	double abort_residual; /* abortResidual (absolute, like the reference)  */
+	int abort_variable;    /* 0-based (abortVariable - 1)                   */
+	double cl_abort_residual, cd_abort_residual;
+	int implicit;          /* implicit                                      */
+	int precond;           /* precond (LU-SGS)                              */
+	int n_kdim;            /* nKdim                                         */
+	int n_newton_iter;     /* nNewtonIter                                   */
+	double eps_newton;     /* epsNewton (not squared)                       */
+	double eps_gmres;      /* epsGMRES                                      */
+	double gamma_ew;       /* gammaEW                                       */
+	int calc_wing;         /* calcWing                                      */
+	int wall_id;           /* wall_id (BC code of the wing surface)         */
+	double ref_length;     /* referenceLength                               */
+	int precision;         /* enum ccfd_precision                           */
+	double rel_abort_residual; /* >0: stop when res/res_first <= this (extension) */
+} ccfd_params;
+
+/* one boundary condition, src/boundary.h:19-46, parsed by initBoundary
+ * (src/boundary.c:29-137) */
+typedef struct ccfd_bc {
+	int type;              /* enum ccfd_bc_type                             */
+	int id;                /* sub id (code % 100)                           */
+	int exact_func;        /* BCexactFunc for EXACTSOL                      */
+	int is_adiabatic;      /* adiabaticWall (parsed, unused like the reference) */
+	double pvar[4];        /* rho, vx, vy, p (inflow / characteristic / pressure) */
+	double connection[2];  /* periodic offset (periodic BCs are not built)  */
+} ccfd_bc;
+
+/* exact-function / initial-condition data used on the device by EXACTSOL
+ * ghost states (src/exactFunction.c:35-183) */
+typedef struct ccfd_exact {
+	double ref_state[2][4];  /* refState[0..1] (1-D Riemann; [0] also sets
+				    q_inf of the wing coefficients)           */
+	double rp1d_interface;   /* RP_1D_interface                             */
+	double alpha;            /* angle of attack in degrees (global alpha of
+				    src/initialCondition.c:161)               */
+	double x_min, x_max, y_min, y_max, dx_ref;
+} ccfd_exact;
+
+/* ------------------------------------------------------------------ mesh */
+/* Host view of a mesh in the reference's element / side order, as built by
+ * createMesh (src/mesh.c:1405-1844).  Index conventions:
+ *   cells       0..n_cells-1 in elem[] order (triangles then quadrilaterals)
+ *   faces       0..n_faces-1 in side[] order; the owner is side[f]
+ *   half-sides  per cell, CSR in the order of the cell's side list
+ *               (elem->firstSide ... nextElemSide), the order of every
+ *               per-cell sum of the reference
+ *   ghosts      0..n_bc-1 in BCside[] order; a neighbour index < 0 encodes
+ *               ghost b as -1-b
+ */
+typedef struct ccfd_mesh {
+	long n_cells, n_faces, n_bc, n_half_sides, n_nodes;
+	int *cell_type;        /* [N] 3 or 4                                    */
+	int *cell_domain;      /* [N] physical group (IC domain)                */
+	double *cell_bary;     /* [N][2]                                        */
+	double *cell_geo;      /* [N][4] area, 1/area, sx, sy                   */
+	long *hs_offset;       /* [N+1]                                         */
+	long *hs_face;         /* [H] face of the half-side                     */
+	int *hs_sign;          /* [H] +1: cell owns the face, -1: neighbour     */
+	long *hs_nb;           /* [H] neighbour cell or -1-ghost                */
+	double *hs_gp;         /* [H][2] bary -> face midpoint (side->GP)       */
+	double *hs_w;          /* [H][2] least-squares weights (side->w)        */
+	long *face_cells;      /* [F][2] owner cell, neighbour cell or -1-ghost */
+	long *face_hs;         /* [F][2] owner half-side, neighbour half-side or -1 */
+	double *face_n;        /* [F][2] unit normal, outward of the owner      */
+	double *face_len;      /* [F]                                           */
+	double *face_bb;       /* [F][3] owner side baryBaryVec x, y, baryBaryDist */
+	double *ghost_gp;      /* [B][2] ghost side GP (face midpoint - ghost bary) */
+	long *bc_face;         /* [B] face of the ghost                          */
+	int *bc_index;         /* [B] index into the BC table                   */
+	double *bc_ghost_bary; /* [B][2] mirrored ghost barycentre              */
+	double *bc_x;          /* [B][2] face midpoint, side->GP + elem->bary   */
+	double total_area_q, dx_ref, x_min, x_max, y_min, y_max;
+} ccfd_mesh;
+
+/* A complete case: parameters, boundary table, mesh and initial state, as
+ * the reference's init sequence (src/main.c:101-118) produces them. */
+typedef struct ccfd_case {
+	ccfd_params params;
+	int n_bc_table;
+	ccfd_bc bc_table[20];  /* NBC = 20, src/main.h:103                      */
+	ccfd_exact exact;
+	ccfd_mesh mesh;
+	double *prim0;         /* [N][4] initial primitive state                */
+	char file_name[256];   /* fileName                                      */
+	int output_format;     /* outputFormat                                  */
+	int ic_type, exact_func;
+} ccfd_case;
+
+/* -------------------------------------------------------- host-side API */
+/* Read a .ini parameter file with the reference's parser semantics
+ * (src/readInTools.c:38-405: case-insensitive keys, values filtered to
+ * [alnum _ . , -], keys consumed in read order) and build the full case
+ * exactly as initOutput..setInitialCondition do, including the Cartesian
+ * generator (src/mesh.c:385-486) or the gmsh 2/4 reader (src/mesh.c:498-992)
+ * and createMesh (src/mesh.c:1405-1844).  Replaces main()'s init sequence. */
+int ccfd_case_load(const char *ini_path, ccfd_case **out);
+/* Same, from .ini text held in memory; relative mesh paths resolve against
+ * base_dir (may be NULL). */
+int ccfd_case_load_text(const char *ini_text, const char *base_dir, ccfd_case **out);
+/* Build the mesh part of a case from raw elements (what a mesh reader
+ * returns): nodes [n_nodes][2], triangles [n_tri][4] (3 nodes + domain),
+ * quads [n_quad][5] (4 nodes + domain), BC edges [n_edge][3] (2 nodes + code).
+ * Node indices are 0-based.  Replaces createMesh (src/mesh.c:1405-1844). */
+int ccfd_mesh_build(const double *nodes, long n_nodes,
+		    const long *tria, long n_tria, const long *quad, long n_quad,
+		    const long *bc_edge, long n_bc_edge,
+		    const ccfd_bc *bc_table, int n_bc_table, ccfd_mesh *out);
+void ccfd_mesh_free(ccfd_mesh *m);
+void ccfd_case_free(ccfd_case *c);
+/* Venkatakrishnan epsilon^2 per cell, (K sqrt(A))^3, src/finiteVolume.c:47-52 */
+void ccfd_venk_eps2(const ccfd_mesh *m, double venk_k, double *eps2_out);
+/* Write a gmsh 2.2 ASCII mesh (the format src/mesh.c:498-742 reads). */
+int ccfd_write_gmsh2(const char *path, const double *nodes, long n_nodes,
+		     const long *tria, long n_tria, const long *quad, long n_quad,
+		     const long *bc_edge, long n_bc_edge);
+/* Read a gmsh 2.2 / 4.1 ASCII mesh into raw arrays (caller frees with free()). */
+int ccfd_read_gmsh(const char *path, double **nodes, long *n_nodes,
+		   long **tria, long *n_tria, long **quad, long *n_quad,
+		   long **bc_edge, long *n_bc_edge);
+const char *ccfd_strerror(int status);
+
+/* ------------------------------------------------------ device context */
+typedef struct ccfd_ctx ccfd_ctx;
+
+/* Run report of an explicit or implicit run (the quantities timeDisc prints,
+ * src/timeDiscretization.c:559-777). */
+typedef struct ccfd_report {
+	double t;              /* simulation time reached                       */
+	double dt;             /* last time step                                */
+	long iterations;       /* time steps taken                              */
+	double residual[6];    /* resIter: L2 residual of RHO, MX, MY, E; CL, CD rates */
+	double cl, cd;         /* wing coefficients (calcWing)                  */
+	int converged;         /* stationary: abort criterion met               */
+	int finished;          /* transient: tEnd reached                       */
+	long newton_iterations, gmres_iterations;
+	double first_residual[4]; /* resIter of the first step (relative stop)  */
+	int status;            /* device error status                          */
+} ccfd_report;
+
+/* Create a context on the current CUDA device.  Replaces the init* globals. */
+int ccfd_create(const ccfd_params *params, ccfd_ctx **out);
+void ccfd_destroy(ccfd_ctx *ctx);
+/* Upload mesh connectivity / geometry once (mesh.c output -> device SoA),
+ * boundary table and exact-function data.  Optionally reorders cells and
+ * faces for locality (reorder = 1: reverse Cuthill-McKee); results are
+ * independent of the ordering. */
+int ccfd_upload_case(ccfd_ctx *ctx, const ccfd_mesh *mesh, const ccfd_bc *bc,
+		     int n_bc, const ccfd_exact *exact, int reorder);
+/* State in reference cell order, [N][4], primitive or conservative.  Setting
+ * primitives also sets cVar = primCons(pVar) like setInitialCondition
+ * (src/initialCondition.c:346-350); setting conservatives sets
+ * pVar = consPrim(cVar). */
+int ccfd_set_state(ccfd_ctx *ctx, const double *state, int kind);
+int ccfd_get_state(ccfd_ctx *ctx, double *state, int kind);
+/* Set / get the simulation time t (src/timeDiscretization.c:31). */
+int ccfd_set_time(ccfd_ctx *ctx, double t);
+int ccfd_get_time(ccfd_ctx *ctx, double *t);
+/* Drop-in for fvTimeDerivative(time) (src/finiteVolume.c:78-121): evaluates
+ * R(U) from the current primitive state; u_t_out ([N][4], reference order)
+ * may be NULL to keep the result on the device.  grad_out ([N][8]: u_x[4],
+ * u_y[4]) may be NULL. */
+int ccfd_residual(ccfd_ctx *ctx, double time, double *u_t_out, double *grad_out);
+/* Drop-in for calcTimeStep (src/timeDiscretization.c:249-329). */
+int ccfd_time_step(ccfd_ctx *ctx, double *dt_out);
+/* Explicit time stepping: up to nsteps iterations of the loop in timeDisc
+ * (src/timeDiscretization.c:595-731) with explicitTimeStepEuler / RK
+ * (:337-401), calcTimeStep and globalResidual (src/analyze.c:521-539) on the
+ * device, captured as CUDA graphs.  nsteps <= 0 runs until tEnd, convergence
+ * or maxIter. */
+int ccfd_run_explicit(ccfd_ctx *ctx, long nsteps, ccfd_report *report);
+/* Implicit backward-Euler stepping: implicitTimeStep
+ * (src/timeDiscretization.c:412-552) with GMRES_M (src/linearSolver.c:
+ * 385-510), matrixVector (:343-373) and, if params.precond, the LU-SGS
+ * preconditioner (buildMatrix :186-252, calcDinv :136-179, LUSGS :261-333)
+ * on block-sparse storage. */
+int ccfd_run_implicit(ccfd_ctx *ctx, long nsteps, ccfd_report *report);
+/* Drop-in for globalResidual on the last residual (src/analyze.c:521-539). */
+int ccfd_global_residual(ccfd_ctx *ctx, double res[4]);
+/* Lift / drag of the wall with BC code params.wall_id: the sums of calcCoef
+ * (src/analyze.c:292-387) over the reconstructed wall-face pressures of the
+ * last residual, with q_inf from exact.ref_state[0] and exact.alpha. */
+int ccfd_clcd(ccfd_ctx *ctx, double *cl, double *cd);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

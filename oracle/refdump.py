@@ -1,0 +1,82 @@
+"""Reader and runner for the reference-oracle driver (TEST INFRASTRUCTURE ONLY).
+
+The oracle driver (``oracle/ref_driver.c``) links the reference ccfd sources
+unmodified and writes a small binary dump:  magic ``CCFDDMP1`` followed by
+records ``char name[32]; int32 type (0 f64, 1 i64); int32 pad; int64 count;
+data``.  Only tests, ``__graft_entry__.smoke()`` and the CPU-baseline leg of
+``bench.py`` use this module, as the checker or the timed reference -- never as
+the product path.
+"""
+from __future__ import annotations
+
+import os
+import subprocess
+import tempfile
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+REF_DIR = os.path.join(_HERE, "_ref")
+
+
+def ref_binary(eqn: str = "euler", fast: bool = False) -> str:
+    """Path of the compiled reference driver for an equation system."""
+    name = f"ccfd_ref_{eqn}" + ("_fast" if fast else "")
+    return os.path.join(REF_DIR, name)
+
+
+def have_ref(eqn: str = "euler", fast: bool = False) -> bool:
+    return os.access(ref_binary(eqn, fast), os.X_OK)
+
+
+def read_dump(path: str) -> dict:
+    out = {}
+    with open(path, "rb") as f:
+        if f.read(8) != b"CCFDDMP1":
+            raise ValueError(f"{path}: not an oracle dump")
+        while True:
+            name = f.read(32)
+            if len(name) < 32:
+                break
+            hdr = np.frombuffer(f.read(8), dtype=np.int32)
+            cnt = int(np.frombuffer(f.read(8), dtype=np.int64)[0])
+            dt = np.float64 if hdr[0] == 0 else np.int64
+            data = np.frombuffer(f.read(8 * cnt), dtype=dt).copy()
+            out[name.rstrip(b"\0").decode()] = data
+    return out
+
+
+def run_ref(ini_text: str, mode: str, *args, eqn: str = "euler",
+            fast: bool = False, state: np.ndarray | None = None,
+            threads: int | None = None, workdir: str | None = None,
+            timeout: float = 3600.0) -> dict:
+    """Run the reference driver on an .ini text in a scratch directory.
+
+    ``state`` (N x 4 primitive states in reference cell order) replaces the
+    initial condition.  Returns the parsed dump.
+    """
+    exe = ref_binary(eqn, fast)
+    if not os.access(exe, os.X_OK):
+        raise FileNotFoundError(exe)
+    with tempfile.TemporaryDirectory(dir=workdir) as tmp:
+        ini = os.path.join(tmp, "case.ini")
+        with open(ini, "w") as f:
+            f.write(ini_text)
+        dump = os.path.join(tmp, "out.dump")
+        argv = [exe, ini, dump, mode] + [str(a) for a in args]
+        if state is not None:
+            sp = os.path.join(tmp, "state.bin")
+            np.ascontiguousarray(state, dtype=np.float64).tofile(sp)
+            if len(args) == 0:
+                argv.append("0")
+            argv.append(sp)
+        env = dict(os.environ)
+        if threads is not None:
+            env["OMP_NUM_THREADS"] = str(threads)
+        env.setdefault("OMP_NUM_THREADS", "1")
+        r = subprocess.run(argv, cwd=tmp, env=env, capture_output=True,
+                           text=True, timeout=timeout)
+        if r.returncode != 0:
+            raise RuntimeError(f"reference driver failed ({r.returncode}):\n"
+                               f"{r.stdout[-3000:]}\n{r.stderr[-3000:]}")
+        return read_dump(dump)
