@@ -1,0 +1,306 @@
+"""Benchmark of the residual-and-update path (one JSON line on rank 0).
+
+Workload (one "step" = one explicit time step): double Mach reflection on a
+jittered triangle mesh, 1000 x 250 quads split into 500,000 triangles, HLLC
+flux, second order with the Venkatakrishnan limiter (K = 5), 3-stage RK,
+CFL 0.8, FP64.  Metric unit: cell-updates/s = cells x RK stages x steps / s.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Under torchrun each rank runs an independent replica on its own GPU (the path
+does not shard: replicas only, weak scaling); time is the max over ranks of
+the device time measured with CUDA events on the solver's stream.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "served solves/s & p50/p99 vs plain GPU loop @1e-8 res; cell-updates/s vs HBM"
+UNIT = "cell-updates/s"
+NX, NY = 1000, 250
+L2_BYTES = 126 * 1024 * 1024
+
+
+def _peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            p = json.load(f)
+        return float(p["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks / throttle reasons sampled during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.Q}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self) -> dict:
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                smax = float(f[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def algorithmic_bytes_per_stage(m: dict, venk: bool) -> int:
+    """Compulsory HBM traffic of one residual evaluation + RK stage update of
+    the two-pass (gradient -> face) scheme, each array touched once: per cell
+    primitive state read by both passes (2 x 32 B), 1/area (8), limited
+    gradients written and read (2 x 64), stage-start conservative state read
+    (32), updated primitive state written (32), Venkatakrishnan eps^2 (8); per
+    half-side neighbour index (4), least-squares weights (16), face-midpoint
+    offset (16); per face two cell indices (8), normal (16), length (8)."""
+    n, h, f = m["n_cells"], m["n_half_sides"], m["n_faces"]
+    per_cell = 32 + 32 + 8 + 128 + 32 + 32 + (8 if venk else 0)
+    return n * per_cell + h * (4 + 16 + 16) + f * (8 + 16 + 8)
+
+
+def make_case(tmpdir: str):
+    import ccfd_b200 as cc
+    from ccfd_b200 import meshgen
+    path = os.path.join(tmpdir, "dmr.msh")
+    meshgen.dmr_mesh(NX, NY).write_gmsh(path)
+    ini = meshgen.dmr_ini("dmr")
+    return cc.CaseData.from_text(ini, tmpdir), ini, path
+
+
+def cpu_reference_sample(ini: str, mesh_path: str, steps: int, threads: int):
+    """Time the reference (compiled from its sources, oracle/_ref) on the
+    host cores: returns (cell-updates/s, seconds per step, threads)."""
+    from oracle import refdump
+    d = refdump.run_ref(ini, "run", steps, fast=True, threads=threads,
+                        files={"dmr.msh": mesh_path}, timeout=1800)
+    n = int(d["counts"][0]) if "counts" in d else None
+    wall = d["step_wall"]
+    return wall, d
+
+
+def run_reference_arm(args, rank: int, world: int) -> None:
+    if rank != 0:
+        return
+    from oracle import refdump
+    threads = os.cpu_count() or 1
+    with tempfile.TemporaryDirectory() as tmp:
+        case, ini, path = make_case(tmp)
+        n = case.n_cells
+        if refdump.have_ref("euler", fast=True):
+            kind = "reference"
+            wall, _ = cpu_reference_sample(ini, path, args.warmup + args.steps, threads)
+            t = wall[args.warmup + args.steps - 1] - (wall[args.warmup - 1] if args.warmup else 0.0)
+            cores = threads
+        else:
+            from oracle import restated
+            kind = "port"
+            cores = 1
+            t0 = time.perf_counter()
+            restated.run_explicit(case, nsteps=args.warmup + args.steps)
+            t = (time.perf_counter() - t0) * args.steps / (args.warmup + args.steps)
+    value = n * 3 * args.steps / t
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT,
+            "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": 1e3 * t / args.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": f"double Mach reflection, {n} jittered triangles "
+                                   f"({NX}x{NY} quads split), HLLC, Venkatakrishnan K=5, RK3, CFL 0.8"},
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": kind,
+                             "sample": f"{args.warmup} warm-up + {args.steps} timed RK3 steps of the "
+                                       "full 500k-cell workload (reference's own time loop, "
+                                       "omp_get_wtime per step)"},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def main() -> int:
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--e2e-steps", type=int, default=20)
+    ap.add_argument("--cpu-steps", type=int, default=3)
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
+    ap.add_argument("--nx", type=int, default=NX)
+    ap.add_argument("--ny", type=int, default=NY)
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+    global NX, NY
+    NX, NY = args.nx, args.ny
+
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    import torch
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    if args.impl == "reference":
+        run_reference_arm(args, rank, world)
+        if dist is not None:
+            dist.destroy_process_group()
+        return 0
+
+    torch.cuda.set_device(local)
+    import ccfd_b200 as cc
+    cc.set_device(local)
+    hbm_peak, peak_src = _peaks()
+    with tempfile.TemporaryDirectory() as tmp:
+        case, ini, mesh_path = make_case(tmp)
+        m = case.mesh()
+        n = m["n_cells"]
+        nrk = 3
+        s = cc.Solver(case, reorder=True)
+        s.set_profiling(True)
+        s.run(args.warmup)
+        s.profile(reset=True)
+        torch.cuda.synchronize()
+        if dist is not None:
+            dist.barrier()
+        clocks = ClockSampler(local)
+        clocks.start()
+        rep = s.run(args.steps)
+        torch.cuda.synchronize()
+        if dist is not None:
+            dist.barrier()
+        clk = clocks.stop()
+        res_ms, res_cnt = s.profile(reset=True)
+        t_ms = torch.tensor([rep["device_ms"]], device="cuda", dtype=torch.float64)
+        if dist is not None:
+            dist.all_reduce(t_ms, op=dist.ReduceOp.MAX)
+        t_ms = float(t_ms.item())
+        steps_done = rep["iterations"] - args.warmup
+        value = world * n * nrk * steps_done / (t_ms / 1e3)
+        s.set_profiling(False)
+
+        # end to end through the public API with host buffers: every step
+        # uploads the state from pinned host memory and reads it back
+        host = torch.empty((n, 4), dtype=torch.float64, pin_memory=True).numpy()
+        host[:] = s.get_state()
+        if dist is not None:
+            dist.barrier()
+        t0 = time.perf_counter()
+        for _ in range(args.e2e_steps):
+            s.set_state(host)
+            s.run(1)
+            host[:] = s.get_state()
+        t_e2e = time.perf_counter() - t0
+        te = torch.tensor([t_e2e], device="cuda", dtype=torch.float64)
+        if dist is not None:
+            dist.all_reduce(te, op=dist.ReduceOp.MAX)
+        e2e_value = world * n * nrk * args.e2e_steps / float(te.item())
+        s.close()
+
+        bytes_stage = algorithmic_bytes_per_stage(m, venk=True)
+        avg_res_ms = res_ms / max(res_cnt, 1)
+        achieved = bytes_stage / (avg_res_ms / 1e3) / 1e9
+
+        cpu = None
+        if rank == 0 and world == 1 and not args.no_cpu:
+            from oracle import refdump
+            threads = os.cpu_count() or 1
+            if refdump.have_ref("euler", fast=True):
+                wall, _ = cpu_reference_sample(ini, mesh_path, args.cpu_steps, threads)
+                t_cpu = wall[-1] - wall[0] if len(wall) > 1 else wall[-1]
+                st_cpu = len(wall) - 1 if len(wall) > 1 else 1
+                cpu = {"value": n * nrk * st_cpu / t_cpu, "unit": UNIT, "cores": threads,
+                       "kind": "reference",
+                       "sample": f"{args.cpu_steps} RK3 steps of the same 500k-cell workload "
+                                 "(first step untimed), reference compiled from its sources "
+                                 "(-O3 -march=x86-64-v3, OpenMP)"}
+            else:
+                from oracle import restated
+                t0 = time.perf_counter()
+                restated.residual(case, case.prim0(), 0.0)
+                t_cpu = time.perf_counter() - t0
+                cpu = {"value": n / t_cpu, "unit": UNIT, "cores": 1, "kind": "port",
+                       "sample": "one residual evaluation of the 500k-cell workload (C restatement)"}
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": t_ms / max(steps_done, 1), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {
+                "workload": f"double Mach reflection, {n} jittered triangles ({NX}x{NY} quads "
+                            "split, seed 20260001), HLLC, Venkatakrishnan K=5, RK3 (timeOrder 2), "
+                            "CFL 0.8, FP64",
+                "cells": n, "faces": m["n_faces"], "rk_stages": nrk,
+                "parallelism": f"replicas x{world}",
+                "l2": "inputs larger than L2 (working set > 126 MB), no flush",
+            },
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm_peak,
+                         "unit": "GB/s", "frac": achieved / hbm_peak, "traffic": None,
+                         "kernel": "residual evaluation + RK stage (gradient/limiter, face flux, "
+                                   "update kernels)",
+                         "bytes_per_launch": bytes_stage, "avg_ms": avg_res_ms,
+                         "peak_source": peak_src},
+            "e2e": {"value": e2e_value, "unit": UNIT,
+                    "h2d_bytes_per_step": 2 * n * 4 * 8, "d2h_bytes_per_step": n * 4 * 8},
+            "gpu_launches": int(steps_done * (2 + 3 * nrk + 1)),
+            "clocks": clk,
+            "cpu_baseline": cpu,
+        }
+        print(json.dumps(line), flush=True)
+    if dist is not None:
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -23,7 +23,7 @@ import numpy as np
 
 from . import _native as N
 
-__all__ = ["CaseData", "Solver", "CcfdError", "mesh_arrays", "PRIMITIVE", "CONSERVATIVE"]
+__all__ = ["CaseData", "Solver", "set_device", "CcfdError", "mesh_arrays", "PRIMITIVE", "CONSERVATIVE"]
 
 PRIMITIVE, CONSERVATIVE = N.PRIMITIVE, N.CONSERVATIVE
 
@@ -141,6 +141,11 @@ class CaseData:
         return self.c.file_name.decode()
 
 
+def set_device(device: int) -> None:
+    """Bind the calling thread's next contexts to a CUDA device."""
+    _check(N.lib.ccfd_set_device(int(device)), "ccfd_set_device")
+
+
 class Solver:
     """One case resident on the current CUDA device."""
 
@@ -210,6 +215,16 @@ class Solver:
         _check(fn(self._ctx, int(nsteps), C.byref(rep)), "ccfd_run")
         return report_dict(rep)
 
+    def set_profiling(self, on: bool) -> None:
+        _check(N.lib.ccfd_set_profiling(self._ctx, int(on)), "ccfd_set_profiling")
+
+    def profile(self, reset: bool = True):
+        """(accumulated residual-evaluation device ms, count) inside step graphs."""
+        ms, cnt = C.c_double(), C.c_long()
+        _check(N.lib.ccfd_get_profile(self._ctx, C.byref(ms), C.byref(cnt), int(reset)),
+               "ccfd_get_profile")
+        return ms.value, cnt.value
+
     def clcd(self):
         cl, cd = C.c_double(), C.c_double()
         _check(N.lib.ccfd_clcd(self._ctx, C.byref(cl), C.byref(cd)), "ccfd_clcd")
@@ -221,4 +236,5 @@ def report_dict(rep: N.Report) -> dict:
             "residual": list(rep.residual), "cl": rep.cl, "cd": rep.cd,
             "converged": bool(rep.converged), "finished": bool(rep.finished),
             "newton_iterations": rep.newton_iterations, "gmres_iterations": rep.gmres_iterations,
-            "first_residual": list(rep.first_residual), "status": rep.status}
+            "first_residual": list(rep.first_residual), "status": rep.status,
+            "device_ms": rep.device_ms}

@@ -70,7 +70,7 @@ class Report(C.Structure):
                 ("residual", c_double * 6), ("cl", c_double), ("cd", c_double),
                 ("converged", c_int), ("finished", c_int), ("newton_iterations", c_long),
                 ("gmres_iterations", c_long), ("first_residual", c_double * 4),
-                ("status", c_int)]
+                ("status", c_int), ("device_ms", c_double)]
 
 
 def _load():
@@ -91,6 +91,7 @@ def _load():
         "ccfd_read_gmsh": (c_int, [C.c_char_p, P(P(c_double)), P(c_long), P(P(c_long)),
                                    P(c_long), P(P(c_long)), P(c_long), P(P(c_long)), P(c_long)]),
         "ccfd_strerror": (C.c_char_p, [c_int]),
+        "ccfd_set_device": (c_int, [c_int]),
         "ccfd_create": (c_int, [P(Params), P(C.c_void_p)]),
         "ccfd_destroy": (None, [C.c_void_p]),
         "ccfd_upload_case": (c_int, [C.c_void_p, P(Mesh), P(BC), c_int, P(Exact), c_int]),
@@ -104,6 +105,8 @@ def _load():
         "ccfd_run_implicit": (c_int, [C.c_void_p, c_long, P(Report)]),
         "ccfd_global_residual": (c_int, [C.c_void_p, P(c_double)]),
         "ccfd_clcd": (c_int, [C.c_void_p, P(c_double), P(c_double)]),
+        "ccfd_set_profiling": (c_int, [C.c_void_p, c_int]),
+        "ccfd_get_profile": (c_int, [C.c_void_p, P(c_double), P(c_long), c_int]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)

@@ -57,14 +57,26 @@ static int dupload(ccfd_ctx* ctx, T** p, const std::vector<T>& h) {
     return CCFD_OK;
 }
 
-static void free_device(ccfd_ctx* ctx) {
+static void drop_graphs(ccfd_ctx* ctx) {
     if (ctx->graph_many) cudaGraphExecDestroy(ctx->graph_many);
     if (ctx->graph_one) cudaGraphExecDestroy(ctx->graph_one);
     ctx->graph_many = ctx->graph_one = nullptr;
+    for (cudaEvent_t e : ctx->prof_ev_many) cudaEventDestroy(e);
+    for (cudaEvent_t e : ctx->prof_ev_one) cudaEventDestroy(e);
+    ctx->prof_ev_many.clear();
+    ctx->prof_ev_one.clear();
+}
+
+static void free_device(ccfd_ctx* ctx) {
+    drop_graphs(ctx);
     for (void* p : ctx->allocs) cudaFree(p);
     ctx->allocs.clear();
     ctx->device_bytes = 0;
     ctx->uploaded = false;
+}
+
+extern "C" int ccfd_set_device(int device) {
+    return cudaSetDevice(device) == cudaSuccess ? CCFD_OK : CCFD_ERR_CUDA;
 }
 
 extern "C" int ccfd_create(const ccfd_params* params, ccfd_ctx** out) {
@@ -94,6 +106,12 @@ extern "C" int ccfd_create(const ccfd_params* params, ccfd_ctx** out) {
         return CCFD_ERR_CUDA;
     }
     memset(ctx->h_ctrl, 0, sizeof(Ctrl));
+    if (cudaEventCreate(&ctx->ev_run0) != cudaSuccess || cudaEventCreate(&ctx->ev_run1) != cudaSuccess) {
+        cudaFreeHost(ctx->h_ctrl);
+        cudaStreamDestroy(ctx->stream);
+        delete ctx;
+        return CCFD_ERR_CUDA;
+    }
     // RK coefficient tables, src/timeDiscretization.c:94-169
     double* rk = ctx->rk;
     for (int i = 0; i < 6; ++i) rk[i] = 0.0;
@@ -119,6 +137,8 @@ extern "C" void ccfd_destroy(ccfd_ctx* ctx) {
     if (!ctx) return;
     cudaStreamSynchronize(ctx->stream);
     free_device(ctx);
+    if (ctx->ev_run0) cudaEventDestroy(ctx->ev_run0);
+    if (ctx->ev_run1) cudaEventDestroy(ctx->ev_run1);
     if (ctx->h_ctrl) cudaFreeHost(ctx->h_ctrl);
     cudaStreamDestroy(ctx->stream);
     delete ctx;
@@ -547,8 +567,9 @@ extern "C" int ccfd_time_step(ccfd_ctx* ctx, double* dt_out) {
     return CCFD_OK;
 }
 
-// record one explicit time step into the stream (graph capture)
-static void record_step(ccfd_ctx* ctx) {
+// record one explicit time step into the stream (graph capture); with
+// profiling, each residual evaluation is bracketed by two event-record nodes
+static void record_step(ccfd_ctx* ctx, std::vector<cudaEvent_t>* ev) {
     const StepParams& sp = ctx->sp;
     launch_dt(ctx->mesh, ctx->phys, ctx->ctrl, sp, ctx->prim, ctx->dt_partial, ctx->dt_bad, ctx->stream);
     launch_step_begin(ctx->ctrl, sp, ctx->dt_partial, ctx->dt_bad, ctx->nb_cells, ctx->stream);
@@ -564,16 +585,26 @@ static void record_step(ccfd_ctx* ctx) {
         L.rk = sp.rk[s];
         L.last_stage = s == sp.nrk;
         L.res_partial = (s == sp.nrk) ? ctx->res_partial : nullptr;
+        cudaEvent_t e0 = nullptr, e1 = nullptr;
+        if (ev) {
+            cudaEventCreate(&e0);
+            cudaEventCreate(&e1);
+            ev->push_back(e0);
+            ev->push_back(e1);
+            cudaEventRecordWithFlags(e0, ctx->stream, cudaEventRecordExternal);
+        }
         launch_residual(L, ctx->stream);
+        if (ev) cudaEventRecordWithFlags(e1, ctx->stream, cudaEventRecordExternal);
     }
     launch_step_end(ctx->ctrl, sp, ctx->res_partial, ctx->nb_cells, ctx->wall_ghost, ctx->wall_nl,
                     ctx->ghost_pface, ctx->stream);
 }
 
-static int build_graph(ccfd_ctx* ctx, int steps, cudaGraphExec_t* exec) {
+static int build_graph(ccfd_ctx* ctx, int steps, cudaGraphExec_t* exec,
+                       std::vector<cudaEvent_t>* ev) {
     cudaGraph_t g;
     CK(cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
-    for (int i = 0; i < steps; ++i) record_step(ctx);
+    for (int i = 0; i < steps; ++i) record_step(ctx, ev);
     cudaError_t e = cudaStreamEndCapture(ctx->stream, &g);
     if (e != cudaSuccess) {
         ctx->last_cuda_error = (int)e;
@@ -605,14 +636,53 @@ static void fill_report(ccfd_ctx* ctx, ccfd_report* r) {
     r->status = status_from_flags(c.flags);
 }
 
+// accumulate the residual-evaluation times of the last graph launch (only
+// active stages: an inactive stage is a pair of back-to-back events)
+static int collect_profile(ccfd_ctx* ctx, const std::vector<cudaEvent_t>& ev) {
+    for (size_t i = 0; i + 1 < ev.size(); i += 2) {
+        float ms = 0.0f;
+        CK(cudaEventElapsedTime(&ms, ev[i], ev[i + 1]));
+        ctx->prof_ms += ms;
+        ctx->prof_count += 1;
+    }
+    return CCFD_OK;
+}
+
+extern "C" int ccfd_set_profiling(ccfd_ctx* ctx, int on) {
+    if (!ctx) return CCFD_ERR_ARG;
+    if ((bool)on != ctx->profiling) {
+        CK(cudaSetDevice(ctx->device));
+        drop_graphs(ctx);
+        ctx->profiling = on != 0;
+    }
+    ctx->prof_ms = 0.0;
+    ctx->prof_count = 0;
+    return CCFD_OK;
+}
+
+extern "C" int ccfd_get_profile(ccfd_ctx* ctx, double* residual_ms, long* residual_count, int reset) {
+    if (!ctx || !residual_ms || !residual_count) return CCFD_ERR_ARG;
+    *residual_ms = ctx->prof_ms;
+    *residual_count = ctx->prof_count;
+    if (reset) {
+        ctx->prof_ms = 0.0;
+        ctx->prof_count = 0;
+    }
+    return CCFD_OK;
+}
+
 extern "C" int ccfd_run_explicit(ccfd_ctx* ctx, long nsteps, ccfd_report* report) {
     if (!ctx || !ctx->uploaded) return CCFD_ERR_ARG;
     if (ctx->params.implicit) return ccfd_run_implicit(ctx, nsteps, report);
     CK(cudaSetDevice(ctx->device));
     int st;
     const int kMany = 16;
-    if (!ctx->graph_one && (st = build_graph(ctx, 1, &ctx->graph_one))) return st;
-    if (!ctx->graph_many && (st = build_graph(ctx, kMany, &ctx->graph_many))) return st;
+    const bool prof = ctx->profiling;
+    if (!ctx->graph_one && (st = build_graph(ctx, 1, &ctx->graph_one, prof ? &ctx->prof_ev_one : nullptr)))
+        return st;
+    if (!ctx->graph_many &&
+        (st = build_graph(ctx, kMany, &ctx->graph_many, prof ? &ctx->prof_ev_many : nullptr)))
+        return st;
     // read the control block, set the step budget of this call
     CK(cudaMemcpyAsync(ctx->h_ctrl, ctx->ctrl, sizeof(Ctrl), cudaMemcpyDeviceToHost, ctx->stream));
     CK(cudaStreamSynchronize(ctx->stream));
@@ -622,21 +692,36 @@ extern "C" int ccfd_run_explicit(ccfd_ctx* ctx, long nsteps, ccfd_report* report
     c.stop_at = stop_at;
     CK(cudaMemcpyAsync(&ctx->ctrl->stop_at, &c.stop_at, sizeof(long long), cudaMemcpyHostToDevice,
                        ctx->stream));
+    CK(cudaEventRecord(ctx->ev_run0, ctx->stream));
     while (!c.done && c.iter < stop_at) {
         long long remaining = stop_at - c.iter;
+        const std::vector<cudaEvent_t>* used = nullptr;
         if (remaining >= kMany) {
-            for (int rep = 0; rep < 4 && remaining >= (long long)kMany * (rep + 1); ++rep)
+            // with profiling, one graph per host round trip so every event
+            // pair is read before the graph records it again
+            int reps = prof ? 1 : 4;
+            for (int rep = 0; rep < reps && remaining >= (long long)kMany * (rep + 1); ++rep)
                 CK(cudaGraphLaunch(ctx->graph_many, ctx->stream));
+            used = &ctx->prof_ev_many;
         } else {
             CK(cudaGraphLaunch(ctx->graph_one, ctx->stream));
+            used = &ctx->prof_ev_one;
         }
         CK(cudaMemcpyAsync(ctx->h_ctrl, ctx->ctrl, sizeof(Ctrl), cudaMemcpyDeviceToHost, ctx->stream));
         CK(cudaStreamSynchronize(ctx->stream));
+        if (prof && (st = collect_profile(ctx, *used))) return st;
     }
+    CK(cudaEventRecord(ctx->ev_run1, ctx->stream));
+    CK(cudaEventSynchronize(ctx->ev_run1));
+    float run_ms = 0.0f;
+    CK(cudaEventElapsedTime(&run_ms, ctx->ev_run0, ctx->ev_run1));
     unsigned f = 0;
     CK(cudaMemcpyAsync(&f, ctx->flags, sizeof(unsigned), cudaMemcpyDeviceToHost, ctx->stream));
     CK(cudaStreamSynchronize(ctx->stream));
-    if (report) fill_report(ctx, report);
+    if (report) {
+        fill_report(ctx, report);
+        report->device_ms = run_ms;
+    }
     int s1 = status_from_flags(c.flags | f);
     if (s1) return s1;
     return CCFD_OK;

@@ -44,6 +44,12 @@ struct ccfd_ctx {
     int n_wall = 0;
     cudaGraphExec_t graph_one = nullptr, graph_many = nullptr;
     long newton_total = 0, gmres_total = 0;
+    // profiling: event pairs around each residual evaluation in the graphs
+    bool profiling = false;
+    std::vector<cudaEvent_t> prof_ev_many, prof_ev_one;
+    double prof_ms = 0.0;
+    long prof_count = 0;
+    cudaEvent_t ev_run0 = nullptr, ev_run1 = nullptr;
     void* implicit_state = nullptr;  // owned by the implicit solver
 };
 

@@ -224,8 +224,14 @@ typedef struct ccfd_report {
 	long newton_iterations, gmres_iterations;
 	double first_residual[4]; /* resIter of the first step (relative stop)  */
 	int status;            /* device error status                          */
+	double device_ms;      /* device time of the call (CUDA events on the
+				  context's stream, first launch to last)      */
 } ccfd_report;
 
+/* Select the CUDA device for the calling host thread (cudaSetDevice); the
+ * next ccfd_create binds its context to it.  No counterpart in the reference
+ * (single-process CPU code). */
+int ccfd_set_device(int device);
 /* Create a context on the current CUDA device.  Replaces the init* globals. */
 int ccfd_create(const ccfd_params *params, ccfd_ctx **out);
 void ccfd_destroy(ccfd_ctx *ctx);
@@ -263,6 +269,15 @@ int ccfd_run_explicit(ccfd_ctx *ctx, long nsteps, ccfd_report *report);
  * preconditioner (buildMatrix :186-252, calcDinv :136-179, LUSGS :261-333)
  * on block-sparse storage. */
 int ccfd_run_implicit(ccfd_ctx *ctx, long nsteps, ccfd_report *report);
+/* Profiling of the residual evaluations inside the timed step graphs: with
+ * profiling on, every residual evaluation of a step (gradient, face flux and
+ * update kernels of one Runge-Kutta stage) is bracketed by CUDA events on the
+ * context's stream; ccfd_get_profile returns the accumulated device time and
+ * count since the last reset.  No counterpart in the reference (its timer is
+ * the wall clock around the time loop, src/timeDiscretization.c:583,734). */
+int ccfd_set_profiling(ccfd_ctx *ctx, int on);
+int ccfd_get_profile(ccfd_ctx *ctx, double *residual_ms, long *residual_count,
+		     int reset);
 /* Drop-in for globalResidual on the last residual (src/analyze.c:521-539). */
 int ccfd_global_residual(ccfd_ctx *ctx, double res[4]);
 /* Lift / drag of the wall with BC code params.wall_id: the sums of calcCoef

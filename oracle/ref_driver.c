@@ -289,6 +289,7 @@ int main(int argc, char *argv[])
 		calcTimeStep(printTime, &dt, &visc);
 		double resIter[NVAR + 2] = {0.0};
 		double *hist = malloc(sizeof(double) * 8 * (maxIter + 2));
+		double *wall = malloc(sizeof(double) * (maxIter + 2));
 		long iter, nhist = 0;
 		bool converged = false;
 		double tStart = omp_get_wtime();
@@ -315,6 +316,7 @@ int main(int argc, char *argv[])
 				resIter[4] = fabs(resIter[4] - wing.cl) / firstElem->dt;
 				resIter[5] = fabs(resIter[5] - wing.cd) / firstElem->dt;
 			}
+			wall[nhist] = omp_get_wtime() - tStart;
 			double *h = &hist[8 * nhist++];
 			h[0] = t; h[1] = dt;
 			for (int v = 0; v < 6; ++v)
@@ -344,6 +346,7 @@ int main(int argc, char *argv[])
 		double tEnd = omp_get_wtime();
 		dump_state();
 		dump_f64("history", hist, 8 * nhist);
+		dump_f64("step_wall", wall, nhist);
 		double info[8] = {t, (double)nhist, tEnd - tStart,
 				  (double)omp_get_max_threads(), converged ? 1.0 : 0.0,
 				  isImplicit ? (double)nNewtonIterGlobal : 0.0,
@@ -355,6 +358,7 @@ int main(int argc, char *argv[])
 			dump_f64("clcd", clcd, 2);
 		}
 		free(hist);
+		free(wall);
 	} else {
 		fprintf(stderr, "ccfd_ref: unknown mode %s\n", mode);
 		return 2;

@@ -49,16 +49,20 @@ def read_dump(path: str) -> dict:
 def run_ref(ini_text: str, mode: str, *args, eqn: str = "euler",
             fast: bool = False, state: np.ndarray | None = None,
             threads: int | None = None, workdir: str | None = None,
-            timeout: float = 3600.0) -> dict:
+            files: dict | None = None, timeout: float = 3600.0) -> dict:
     """Run the reference driver on an .ini text in a scratch directory.
 
     ``state`` (N x 4 primitive states in reference cell order) replaces the
-    initial condition.  Returns the parsed dump.
+    initial condition.  ``files`` maps names to paths linked into the scratch
+    directory (the reference's parser drops '/' from values, so a mesh file
+    must sit in its working directory).  Returns the parsed dump.
     """
     exe = ref_binary(eqn, fast)
     if not os.access(exe, os.X_OK):
         raise FileNotFoundError(exe)
     with tempfile.TemporaryDirectory(dir=workdir) as tmp:
+        for name, src in (files or {}).items():
+            os.symlink(os.path.abspath(src), os.path.join(tmp, name))
         ini = os.path.join(tmp, "case.ini")
         with open(ini, "w") as f:
             f.write(ini_text)

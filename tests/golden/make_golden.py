@@ -1,0 +1,88 @@
+"""Generate the committed golden fixtures of the parity tests.
+
+Run in a checkout that has the reference project (default ../reference path
+given by --ref) and the compiled reference oracle (``make -C oracle``):
+
+    python tests/golden/make_golden.py --ref /path/to/ccfd
+
+Outputs (small, committed):
+  sod_check.json    the reference's own regression suite (check/*.ini with
+                    check/targetOutput/*.csv): per case the .ini text and the
+                    golden x, density, velocity columns at t = 0.25
+  ref_small.npz     outputs of the compiled reference (oracle/_ref) on small
+                    synthetic cases: residuals at seeded random states for
+                    every flux function and limiter, every boundary type,
+                    Navier-Stokes, and short explicit runs
+The synthetic cases themselves are described by CASES below and rebuilt by
+the tests from the same generators and seeds.
+"""
+from __future__ import annotations
+
+import argparse
+import glob
+import json
+import os
+import sys
+import tempfile
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+sys.path.insert(0, ROOT)
+
+from tests.golden import cases as CASES  # noqa: E402
+from oracle import refdump  # noqa: E402
+
+
+def sod_check(ref: str) -> dict:
+    out = {}
+    for ini in sorted(glob.glob(os.path.join(ref, "check", "*.ini"))):
+        name = os.path.basename(ini)[:-4]
+        tgt = sorted(glob.glob(os.path.join(ref, "check", "targetOutput", f"{name}_*")))[-1]
+        data = np.genfromtxt(tgt, skip_header=1, delimiter=",")[:, 0:3]
+        with open(ini) as f:
+            text = f.read()
+        out[name] = {"ini": text, "target": os.path.basename(tgt),
+                     "x": data[:, 0].tolist(), "rho": data[:, 1].tolist(),
+                     "u": data[:, 2].tolist()}
+    return out
+
+
+def ref_small() -> dict:
+    arrays = {}
+    with tempfile.TemporaryDirectory() as tmp:
+        for key, spec in CASES.residual_cases().items():
+            ini, files = CASES.materialise(spec, tmp)
+            prim = CASES.random_state(spec, tmp)
+            d = refdump.run_ref(ini, "residual", spec["time"], state=prim, eqn=spec["eqn"],
+                                files=files)
+            arrays[f"{key}/u_t"] = d["u_t"]
+            arrays[f"{key}/u_x"] = d["u_x"]
+            arrays[f"{key}/u_y"] = d["u_y"]
+            arrays[f"{key}/prim"] = prim.ravel()
+        for key, spec in CASES.run_cases().items():
+            ini, files = CASES.materialise(spec, tmp)
+            d = refdump.run_ref(ini, "run", spec["steps"], eqn=spec["eqn"], files=files)
+            arrays[f"{key}/pvar"] = d["pvar"]
+            arrays[f"{key}/info"] = d["run_info"]
+            arrays[f"{key}/history"] = d["history"]
+    return arrays
+
+
+def main() -> int:
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--ref", default="/root/reference")
+    a = ap.parse_args()
+    if not refdump.have_ref("euler") or not refdump.have_ref("navierstokes"):
+        print("compiled reference missing: run `make -C oracle` first", file=sys.stderr)
+        return 1
+    with open(os.path.join(HERE, "sod_check.json"), "w") as f:
+        json.dump(sod_check(a.ref), f)
+    np.savez_compressed(os.path.join(HERE, "ref_small.npz"), **ref_small())
+    print("wrote sod_check.json, ref_small.npz")
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,110 @@
+"""Host layer: library loading / exported C ABI, .ini semantics, mesh errors."""
+import ctypes as C
+import os
+import re
+
+import numpy as np
+import pytest
+
+import ccfd_b200 as cc
+from ccfd_b200 import _native as N
+from ccfd_b200 import meshgen
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def test_library_exports_every_declared_symbol():
+    with open(os.path.join(ROOT, "include", "ccfd_b200.h")) as f:
+        hdr = f.read()
+    hdr = re.sub(r"/\*.*?\*/", "", hdr, flags=re.S)
+    names = set(re.findall(r"\b(ccfd_[a-z0-9_]+)\s*\(", hdr))
+    assert len(names) > 20
+    lib = C.CDLL(N.LIB_PATH)
+    missing = [n for n in sorted(names) if not hasattr(lib, n)]
+    assert not missing, missing
+
+
+def test_strerror_covers_statuses():
+    for s in range(0, 16):
+        assert N.lib.ccfd_strerror(s).decode() != "unknown status"
+
+
+SOD = """meshType = 1
+nElemsX = 10
+nElemsY = 2
+X0 = (/0.0, 0.0/)
+Xmax = (/1.0, 0.1/)
+nBCsegments = (/1, 1, 1, 1/)
+meshBCtype = 101 ! bottom
+MeshBCType = 401
+meshbctype = 101
+meshBCtype = 401
+icType = 2
+exactFunc = 5
+StateLeft = (/1.0, 0.0, 0.0, 1.0/)
+StateRight = (/0.125, 0.0, 0.0, 0.1/)
+nBC = 2
+BCtype = 101
+BCtype = 401
+FluxFunction = 3
+fileName = t
+tEnd = 0.1
+IOtimeInterval = 0.1
+IOiterInterval = 10
+"""
+
+
+def test_ini_semantics_defaults_and_case_insensitive_keys():
+    case = cc.CaseData.from_text(SOD)
+    p = case.params
+    # defaults of the reference (src/*.c getX(..., "default"))
+    assert p.gamma == 1.4 and p.cfl == 0.9 and p.spatial_order == 1
+    assert p.n_rk_stages == 1 and p.time_order == 1 and p.stationary == 1
+    assert p.flux == 3 and p.max_iter == 100000
+    assert case.n_cells == 20
+    prim = case.prim0()
+    x = case.mesh()["cell_bary"][:, 0]
+    assert np.all(prim[x <= 0.5, 0] == 1.0) and np.all(prim[x > 0.5, 0] == 0.125)
+
+
+def test_ini_missing_mandatory_key_is_an_error():
+    bad = SOD.replace("FluxFunction    = 3", "").replace("FluxFunction = 3", "")
+    with pytest.raises(cc.CcfdError) as e:
+        cc.CaseData.from_text(bad)
+    assert e.value.status == 9
+
+
+def test_ini_repeated_keys_are_consumed_in_order():
+    txt = SOD.replace("meshBCtype = 101 ! bottom", "meshBCtype = 401 ! bottom")
+    case = cc.CaseData.from_text(txt)
+    m = case.mesh()
+    codes = np.array([case.c.bc_table[i].type * 100 + case.c.bc_table[i].id for i in m["bc_index"]])
+    # bottom (first 10 BC edges) now outflow
+    assert (codes == 401).sum() == 10 + 2 + 2
+
+
+def test_undefined_bc_code_is_a_mesh_error():
+    bad = SOD.replace("BCtype = 401", "BCtype = 501\nrho=1\nmach=0.1\nalpha=0\npressure=1")
+    with pytest.raises(cc.CcfdError) as e:
+        cc.CaseData.from_text(bad)
+    assert e.value.status == 10
+
+
+def test_mesh_build_rejects_inconsistent_boundary(tmp_path):
+    m = meshgen.dmr_mesh(4, 2)
+    m.bc = m.bc[:-1]  # drop one boundary edge: odd side count
+    path = m.write_gmsh(str(tmp_path / "dmr.msh"))
+    with pytest.raises(cc.CcfdError) as e:
+        cc.CaseData.from_text(meshgen.dmr_ini("dmr"), str(tmp_path))
+    assert e.value.status == 10
+
+
+def test_gmsh_roundtrip(tmp_path):
+    m = meshgen.dmr_mesh(6, 3)
+    m.write_gmsh(str(tmp_path / "a.msh"))
+    case = cc.CaseData.from_text(meshgen.dmr_ini("a"), str(tmp_path))
+    assert case.n_cells == 36
+    mm = case.mesh()
+    assert mm["n_bc"] == 18 and mm["n_faces"] == (3 * 36 + 18) // 2
+    # cell areas sum to the domain area
+    assert abs(mm["cell_geo"][:, 0].sum() - 4.0) < 1e-12
