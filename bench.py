@@ -165,6 +165,7 @@ def run_reference_arm(args, rank: int, world: int) -> None:
 
 
 def main() -> int:
+    global NX, NY
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=200)
@@ -177,7 +178,6 @@ def main() -> int:
     ap.add_argument("--ny", type=int, default=NY)
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
-    global NX, NY
     NX, NY = args.nx, args.ny
 
     rank = int(os.environ.get("RANK", "0"))
