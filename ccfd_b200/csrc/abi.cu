@@ -569,7 +569,7 @@ extern "C" int ccfd_time_step(ccfd_ctx* ctx, double* dt_out) {
 
 // record one explicit time step into the stream (graph capture); with
 // profiling, each residual evaluation is bracketed by two event-record nodes
-static void record_step(ccfd_ctx* ctx, std::vector<cudaEvent_t>* ev) {
+static void record_step(ccfd_ctx* ctx, const std::vector<cudaEvent_t>* ev, size_t* ev_next) {
     const StepParams& sp = ctx->sp;
     launch_dt(ctx->mesh, ctx->phys, ctx->ctrl, sp, ctx->prim, ctx->dt_partial, ctx->dt_bad, ctx->stream);
     launch_step_begin(ctx->ctrl, sp, ctx->dt_partial, ctx->dt_bad, ctx->nb_cells, ctx->stream);
@@ -587,10 +587,8 @@ static void record_step(ccfd_ctx* ctx, std::vector<cudaEvent_t>* ev) {
         L.res_partial = (s == sp.nrk) ? ctx->res_partial : nullptr;
         cudaEvent_t e0 = nullptr, e1 = nullptr;
         if (ev) {
-            cudaEventCreate(&e0);
-            cudaEventCreate(&e1);
-            ev->push_back(e0);
-            ev->push_back(e1);
+            e0 = (*ev)[(*ev_next)++];
+            e1 = (*ev)[(*ev_next)++];
             cudaEventRecordWithFlags(e0, ctx->stream, cudaEventRecordExternal);
         }
         launch_residual(L, ctx->stream);
@@ -603,8 +601,18 @@ static void record_step(ccfd_ctx* ctx, std::vector<cudaEvent_t>* ev) {
 static int build_graph(ccfd_ctx* ctx, int steps, cudaGraphExec_t* exec,
                        std::vector<cudaEvent_t>* ev) {
     cudaGraph_t g;
+    if (ev) {
+        // events are created before the capture begins
+        size_t need = (size_t)steps * ctx->sp.nrk * 2;
+        while (ev->size() < need) {
+            cudaEvent_t e;
+            CK(cudaEventCreate(&e));
+            ev->push_back(e);
+        }
+    }
+    size_t ev_next = 0;
     CK(cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
-    for (int i = 0; i < steps; ++i) record_step(ctx, ev);
+    for (int i = 0; i < steps; ++i) record_step(ctx, ev, &ev_next);
     cudaError_t e = cudaStreamEndCapture(ctx->stream, &g);
     if (e != cudaSuccess) {
         ctx->last_cuda_error = (int)e;
