@@ -10,19 +10,19 @@
 
 #include "ccfd_b200.h"
 #include "ccfd_ctx.cuh"
-#include "kernels.cuh"
-#include "reorder.h"
 #include "host/ccfd_host.h"
+#include "kernels.cuh"
+#include "tiles.h"
 
 using namespace ccfd;
 
-#define CK(x)                                   \
-    do {                                        \
-        cudaError_t e_ = (x);                   \
-        if (e_ != cudaSuccess) {                \
-            ctx->last_cuda_error = (int)e_;     \
-            return CCFD_ERR_CUDA;               \
-        }                                       \
+#define CK(x)                               \
+    do {                                    \
+        cudaError_t e_ = (x);               \
+        if (e_ != cudaSuccess) {            \
+            ctx->last_cuda_error = (int)e_; \
+            return CCFD_ERR_CUDA;           \
+        }                                   \
     } while (0)
 
 static int status_from_flags(unsigned f) {
@@ -53,18 +53,27 @@ template <typename T>
 static int dupload(ccfd_ctx* ctx, T** p, const std::vector<T>& h) {
     int st = dalloc(ctx, p, h.size());
     if (st) return st;
-    if (!h.empty()) CK(cudaMemcpyAsync(*p, h.data(), h.size() * sizeof(T), cudaMemcpyHostToDevice, ctx->stream));
+    if (!h.empty())
+        CK(cudaMemcpyAsync(*p, h.data(), h.size() * sizeof(T), cudaMemcpyHostToDevice, ctx->stream));
     return CCFD_OK;
 }
 
+template <typename T>
+static int dupload_c(ccfd_ctx* ctx, const T** p, const std::vector<T>& h) {
+    T* q = nullptr;
+    int st = dupload(ctx, &q, h);
+    *p = q;
+    return st;
+}
+
 static void drop_graphs(ccfd_ctx* ctx) {
-    if (ctx->graph_many) cudaGraphExecDestroy(ctx->graph_many);
-    if (ctx->graph_one) cudaGraphExecDestroy(ctx->graph_one);
-    ctx->graph_many = ctx->graph_one = nullptr;
-    for (cudaEvent_t e : ctx->prof_ev_many) cudaEventDestroy(e);
-    for (cudaEvent_t e : ctx->prof_ev_one) cudaEventDestroy(e);
-    ctx->prof_ev_many.clear();
-    ctx->prof_ev_one.clear();
+    for (int a = 0; a < 2; ++a)
+        for (int b = 0; b < 2; ++b) {
+            if (ctx->graph[a][b]) cudaGraphExecDestroy(ctx->graph[a][b]);
+            ctx->graph[a][b] = nullptr;
+            for (cudaEvent_t e : ctx->prof_ev[a][b]) cudaEventDestroy(e);
+            ctx->prof_ev[a][b].clear();
+        }
 }
 
 static void free_device(ccfd_ctx* ctx) {
@@ -84,14 +93,14 @@ extern "C" int ccfd_create(const ccfd_params* params, ccfd_ctx** out) {
     *out = nullptr;
     const ccfd_params& p = *params;
     if (p.flux < 1 || p.flux > 11 || p.spatial_order < 1 || p.spatial_order > 2 ||
-        (p.spatial_order == 2 && p.limiter != 1 && p.limiter != 2) ||
-        p.time_order < 1 || p.time_order > 3 ||
+        (p.spatial_order == 2 && p.limiter != 1 && p.limiter != 2) || p.time_order < 1 ||
+        p.time_order > 3 ||
         (!(p.n_rk_stages == 1 && p.time_order == 1) && (p.n_rk_stages < 3 || p.n_rk_stages > 5)))
         return CCFD_ERR_ARG;
-    if (p.time_step_1d && p.mu > 1e-10) return CCFD_ERR_ARG; /* timeDiscretization.c:264-267 */
-    int dev = 0;
+    if (p.time_step_1d && p.mu > 1e-10 && p.eqn == CCFD_NAVIER_STOKES)
+        return CCFD_ERR_ARG; /* src/timeDiscretization.c:264-267 */
+    int dev = 0, ndev = 0;
     if (cudaGetDevice(&dev) != cudaSuccess) return CCFD_ERR_CUDA;
-    int ndev = 0;
     if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return CCFD_ERR_CUDA;
     ccfd_ctx* ctx = new ccfd_ctx();
     ctx->params = p;
@@ -100,18 +109,13 @@ extern "C" int ccfd_create(const ccfd_params* params, ccfd_ctx** out) {
         delete ctx;
         return CCFD_ERR_CUDA;
     }
-    if (cudaMallocHost((void**)&ctx->h_ctrl, sizeof(Ctrl)) != cudaSuccess) {
+    if (cudaMallocHost((void**)&ctx->h_ctrl, sizeof(Ctrl)) != cudaSuccess ||
+        cudaEventCreate(&ctx->ev_run0) != cudaSuccess || cudaEventCreate(&ctx->ev_run1) != cudaSuccess) {
         cudaStreamDestroy(ctx->stream);
         delete ctx;
         return CCFD_ERR_CUDA;
     }
     memset(ctx->h_ctrl, 0, sizeof(Ctrl));
-    if (cudaEventCreate(&ctx->ev_run0) != cudaSuccess || cudaEventCreate(&ctx->ev_run1) != cudaSuccess) {
-        cudaFreeHost(ctx->h_ctrl);
-        cudaStreamDestroy(ctx->stream);
-        delete ctx;
-        return CCFD_ERR_CUDA;
-    }
     // RK coefficient tables, src/timeDiscretization.c:94-169
     double* rk = ctx->rk;
     for (int i = 0; i < 6; ++i) rk[i] = 0.0;
@@ -119,9 +123,8 @@ extern "C" int ccfd_create(const ccfd_params* params, ccfd_ctx** out) {
         rk[1] = 1.0;
     } else {
         static const double t3[3][3] = {{0.1418, 0.4, 1.0}, {0.1918, 0.4929, 1.0}, {0.2884, 0.5010, 1.0}};
-        static const double t4[3][4] = {{0.0833, 0.2069, 0.4265, 1.0},
-                                        {0.1084, 0.2602, 0.5052, 1.0},
-                                        {0.1666, 0.3027, 0.5275, 1.0}};
+        static const double t4[3][4] = {
+            {0.0833, 0.2069, 0.4265, 1.0}, {0.1084, 0.2602, 0.5052, 1.0}, {0.1666, 0.3027, 0.5275, 1.0}};
         static const double t5[3][5] = {{0.0533, 0.1263, 0.2375, 0.4414, 1.0},
                                         {0.0695, 0.1602, 0.2898, 0.5060, 1.0},
                                         {0.1067, 0.1979, 0.3232, 0.5201, 1.0}};
@@ -129,6 +132,8 @@ extern "C" int ccfd_create(const ccfd_params* params, ccfd_ctx** out) {
         for (int s = 0; s < p.n_rk_stages; ++s)
             rk[s + 1] = p.n_rk_stages == 3 ? t3[o][s] : p.n_rk_stages == 4 ? t4[o][s] : t5[o][s];
     }
+    const char* tc = getenv("CCFD_TILE_CELLS");
+    if (tc) ctx->tile_cells = std::max(32, std::min(2048, atoi(tc)));
     *out = ctx;
     return CCFD_OK;
 }
@@ -179,114 +184,130 @@ extern "C" int ccfd_upload_case(ccfd_ctx* ctx, const ccfd_mesh* m, const ccfd_bc
     CK(cudaSetDevice(ctx->device));
     free_device(ctx);
     const ccfd_params& p = ctx->params;
-    const long N = m->n_cells, F = m->n_faces, B = m->n_bc, H = m->n_half_sides;
+    const long N = m->n_cells, F = m->n_faces, B = m->n_bc;
     ctx->N = N;
-    ctx->F = F;
     ctx->B = B;
 
-    // locality ordering of cells and faces (results do not depend on it:
-    // every per-cell and per-face operation keeps the reference's operand
-    // order; only the storage order changes)
-    std::vector<int> cperm, fperm;  // device index -> reference index
-    if (reorder) ccfd_rcm_order(m, cperm, fperm);
+    // cell order: Hilbert curve of the barycentres (or the reference order);
+    // results do not depend on it, only the storage order changes
+    std::vector<int> cperm;
+    if (reorder) ccfd_hilbert_order(m, cperm);
     else {
         cperm.resize(N);
-        fperm.resize(F);
         for (long i = 0; i < N; ++i) cperm[i] = (int)i;
-        for (long i = 0; i < F; ++i) fperm[i] = (int)i;
     }
-    ctx->cell_of_dev = cperm;
-    std::vector<int> cinv(N), finv(F);
+    std::vector<int> cinv(N);
     for (long i = 0; i < N; ++i) cinv[cperm[i]] = (int)i;
-    for (long i = 0; i < F; ++i) finv[fperm[i]] = (int)i;
+    ctx->cell_of_dev = cperm;
     ctx->dev_of_cell = cinv;
 
-    std::vector<int> hs_off(N + 1), hs_nb(H), hs_fs(H);
-    std::vector<double4> hs_gw(H), cell_geo(N);
-    std::vector<double> venk(N, 0.0);
-    std::vector<int> hmap(H);  // reference half-side -> device half-side
-    long k = 0;
+    // interior faces in the order of their owner's device index
+    std::vector<int> fint;
+    for (long f = 0; f < F; ++f)
+        if (m->face_cells[2 * f + 1] >= 0) fint.push_back((int)f);
+    std::stable_sort(fint.begin(), fint.end(), [&](int a, int b) {
+        return cinv[m->face_cells[2 * a]] < cinv[m->face_cells[2 * b]];
+    });
+    std::vector<int> fdev(F, -1);
+    for (size_t i = 0; i < fint.size(); ++i) fdev[fint[i]] = (int)i;
+    const long FI = (long)fint.size();
+    ctx->F = FI;
+
+    // per-cell CSR in device order
+    std::vector<int> hs_off(N + 1), hs_nb;
+    std::vector<double4> hs_gw, cell_geo(N);
+    std::vector<int> hs_dev_of_ref(m->n_half_sides);
+    hs_nb.reserve(m->n_half_sides);
+    hs_gw.reserve(m->n_half_sides);
     for (long d = 0; d < N; ++d) {
         long c = cperm[d];
-        hs_off[d] = (int)k;
-        for (long h = m->hs_offset[c]; h < m->hs_offset[c + 1]; ++h, ++k) {
+        hs_off[d] = (int)hs_nb.size();
+        for (long h = m->hs_offset[c]; h < m->hs_offset[c + 1]; ++h) {
             long nb = m->hs_nb[h];
-            hs_nb[k] = nb >= 0 ? cinv[nb] : (int)nb;
-            int fd = finv[m->hs_face[h]];
-            hs_fs[k] = m->hs_sign[h] > 0 ? fd : ~fd;
-            hs_gw[k] = make_double4(m->hs_gp[2 * h], m->hs_gp[2 * h + 1], m->hs_w[2 * h], m->hs_w[2 * h + 1]);
-            hmap[h] = (int)k;
+            hs_dev_of_ref[h] = (int)hs_nb.size();
+            hs_nb.push_back(nb >= 0 ? cinv[nb] : (int)nb);
+            hs_gw.push_back(make_double4(m->hs_gp[2 * h], m->hs_gp[2 * h + 1], m->hs_w[2 * h], m->hs_w[2 * h + 1]));
         }
         cell_geo[d] = make_double4(m->cell_geo[4 * c], m->cell_geo[4 * c + 1], m->cell_geo[4 * c + 2],
                                    m->cell_geo[4 * c + 3]);
     }
-    hs_off[N] = (int)k;
+    hs_off[N] = (int)hs_nb.size();
+    std::vector<double> venk(N, 0.0);
     if (p.spatial_order == 2 && p.limiter == 2) {
         std::vector<double> e2(N);
         ccfd_venk_eps2(m, p.venk_k, e2.data());
         for (long d = 0; d < N; ++d) venk[d] = e2[cperm[d]];
     }
-    std::vector<int2> face_c(F);
-    std::vector<double4> face_gp(F), face_nl(F), face_bb(F);
-    for (long fd = 0; fd < F; ++fd) {
-        long f = fperm[fd];
-        long c0 = m->face_cells[2 * f], c1 = m->face_cells[2 * f + 1];
-        face_c[fd] = make_int2(cinv[c0], c1 >= 0 ? cinv[c1] : (int)c1);
-        long h0 = m->face_hs[2 * f], h1 = m->face_hs[2 * f + 1];
-        double g1x = 0.0, g1y = 0.0;
-        if (h1 >= 0) {
-            g1x = m->hs_gp[2 * h1];
-            g1y = m->hs_gp[2 * h1 + 1];
-        }
-        face_gp[fd] = make_double4(m->hs_gp[2 * h0], m->hs_gp[2 * h0 + 1], g1x, g1y);
-        face_nl[fd] = make_double4(m->face_n[2 * f], m->face_n[2 * f + 1], m->face_len[f], 0.0);
-        face_bb[fd] = make_double4(m->face_bb[3 * f], m->face_bb[3 * f + 1], m->face_bb[3 * f + 2], 0.0);
+    std::vector<double4> face_nl(FI + 1), face_bb(FI + 1);
+    for (long i = 0; i < FI; ++i) {
+        long f = fint[i];
+        face_nl[i] = make_double4(m->face_n[2 * f], m->face_n[2 * f + 1], m->face_len[f], 0.0);
+        face_bb[i] = make_double4(m->face_bb[3 * f], m->face_bb[3 * f + 1], m->face_bb[3 * f + 2], 0.0);
     }
-    std::vector<int> ghost_bc(B + 1);
-    std::vector<double4> ghost_gn(B + 1);
-    std::vector<double2> ghost_mid(B + 1);
+    // ghosts (BCside order)
+    std::vector<int> g_cell(B + 1), g_hs(B + 1), g_bc(B + 1);
+    std::vector<double4> g_gn(B + 1), g_ml(B + 1), g_bb(B + 1);
     for (long g = 0; g < B; ++g) {
         long f = m->bc_face[g];
-        ghost_bc[g] = m->bc_index[g];
-        ghost_gn[g] = make_double4(m->bc_ghost_bary[2 * g], m->bc_ghost_bary[2 * g + 1], m->face_n[2 * f],
-                                   m->face_n[2 * f + 1]);
-        ghost_mid[g] = make_double2(m->bc_x[2 * g], m->bc_x[2 * g + 1]);
+        g_cell[g] = cinv[m->face_cells[2 * f]];
+        g_hs[g] = hs_dev_of_ref[m->face_hs[2 * f]];
+        g_bc[g] = m->bc_index[g];
+        g_gn[g] = make_double4(m->bc_ghost_bary[2 * g], m->bc_ghost_bary[2 * g + 1], m->face_n[2 * f],
+                               m->face_n[2 * f + 1]);
+        g_ml[g] = make_double4(m->bc_x[2 * g], m->bc_x[2 * g + 1], m->face_len[f], 0.0);
+        g_bb[g] = make_double4(m->face_bb[3 * f], m->face_bb[3 * f + 1], m->face_bb[3 * f + 2], 0.0);
+    }
+    // tiles of the fused stage kernel
+    TileSet ts;
+    ccfd_build_tiles(m, cperm, cinv, fdev, ctx->tile_cells, ts);
+    if (ts.max_e >= 32768 || ts.max_hs >= 32768) return CCFD_ERR_ARG;
+    std::vector<int4> counts(ts.n_tiles);
+    std::vector<int> gl_off(ts.n_tiles + 1, 0);
+    for (int t = 0; t < ts.n_tiles; ++t) {
+        counts[t] = make_int4(ts.counts[4 * t], ts.counts[4 * t + 1], ts.counts[4 * t + 2], ts.counts[4 * t + 3]);
+        gl_off[t + 1] = gl_off[t] + ts.counts[4 * t + 1] + 1;
     }
 
     int st;
-    int *d_hs_off, *d_hs_nb, *d_hs_fs, *d_ghost_bc;
-    double4 *d_hs_gw, *d_cell_geo, *d_face_gp, *d_face_nl, *d_face_bb, *d_ghost_gn;
-    double* d_venk;
-    int2* d_face_c;
-    double2* d_ghost_mid;
-    if ((st = dupload(ctx, &d_hs_off, hs_off)) || (st = dupload(ctx, &d_hs_nb, hs_nb)) ||
-        (st = dupload(ctx, &d_hs_fs, hs_fs)) || (st = dupload(ctx, &d_hs_gw, hs_gw)) ||
-        (st = dupload(ctx, &d_cell_geo, cell_geo)) || (st = dupload(ctx, &d_venk, venk)) ||
-        (st = dupload(ctx, &d_face_c, face_c)) || (st = dupload(ctx, &d_face_gp, face_gp)) ||
-        (st = dupload(ctx, &d_face_nl, face_nl)) || (st = dupload(ctx, &d_face_bb, face_bb)) ||
-        (st = dupload(ctx, &d_ghost_bc, ghost_bc)) || (st = dupload(ctx, &d_ghost_gn, ghost_gn)) ||
-        (st = dupload(ctx, &d_ghost_mid, ghost_mid))) {
+    DevMesh& dm = ctx->mesh;
+    memset(&dm, 0, sizeof(dm));
+    TileDev& td = ctx->tiles;
+    memset(&td, 0, sizeof(td));
+    GhostDev& gd = ctx->ghosts;
+    memset(&gd, 0, sizeof(gd));
+    std::vector<short> hs_nbl(ts.hs_nbl.begin(), ts.hs_nbl.end()), hs_loc(ts.hs_loc.begin(), ts.hs_loc.end());
+    if ((st = dupload_c(ctx, &dm.hs_off, hs_off)) || (st = dupload_c(ctx, &dm.hs_nb, hs_nb)) ||
+        (st = dupload_c(ctx, &dm.hs_gw, hs_gw)) || (st = dupload_c(ctx, &dm.cell_geo, cell_geo)) ||
+        (st = dupload_c(ctx, &dm.venk_eps2, venk)) || (st = dupload_c(ctx, &dm.face_nl, face_nl)) ||
+        (st = dupload_c(ctx, &dm.face_bb, face_bb)) || (st = dupload_c(ctx, &gd.cell, g_cell)) ||
+        (st = dupload_c(ctx, &gd.hs, g_hs)) || (st = dupload_c(ctx, &gd.bc, g_bc)) ||
+        (st = dupload_c(ctx, &gd.gn, g_gn)) || (st = dupload_c(ctx, &gd.ml, g_ml)) ||
+        (st = dupload_c(ctx, &gd.bb, g_bb)) || (st = dupload_c(ctx, &td.e_off, ts.e_off)) ||
+        (st = dupload_c(ctx, &td.counts, counts)) || (st = dupload_c(ctx, &td.e_ref, ts.e_ref)) ||
+        (st = dupload_c(ctx, &td.hs_off, ts.hs_off)) || (st = dupload_c(ctx, &td.hs_nbl, hs_nbl)) ||
+        (st = dupload_c(ctx, &td.gl_off, gl_off)) || (st = dupload_c(ctx, &td.hs_loc, hs_loc)) ||
+        (st = dupload_c(ctx, &td.f_off, ts.f_off)) || (st = dupload_c(ctx, &td.f_id, ts.f_id)) ||
+        (st = dupload_c(ctx, &td.f_lr, ts.f_lr)) || (st = dupload_c(ctx, &td.f_hs, ts.f_hs)) ||
+        (st = dupload_c(ctx, &td.u_code, ts.u_code))) {
         free_device(ctx);
         return st;
     }
-    DevMesh& dm = ctx->mesh;
     dm.N = (int)N;
-    dm.F = (int)F;
+    dm.F = (int)FI;
     dm.B = (int)B;
-    dm.H = (int)H;
-    dm.hs_off = d_hs_off;
-    dm.hs_nb = d_hs_nb;
-    dm.hs_fs = d_hs_fs;
-    dm.hs_gw = d_hs_gw;
-    dm.cell_geo = d_cell_geo;
-    dm.venk_eps2 = d_venk;
-    dm.face_c = d_face_c;
-    dm.face_gp = d_face_gp;
-    dm.face_nl = d_face_nl;
-    dm.face_bb = d_face_bb;
-    dm.ghost_bc = d_ghost_bc;
-    dm.ghost_gn = d_ghost_gn;
-    dm.ghost_mid = d_ghost_mid;
+    dm.H = hs_off[N];
+    td.n_tiles = ts.n_tiles;
+    td.max_e = ts.max_e;
+    td.max_g = ts.max_g;
+    td.max_hs = ts.max_hs;
+    td.max_f = ts.max_f;
+    td.smem_bytes = 32 * ts.max_e + 64 * ts.max_g + 16 * (ts.max_hs + (ts.max_hs & 1)) + 32 * ts.max_f;
+    int smem_max = 0;
+    CK(cudaDeviceGetAttribute(&smem_max, cudaDevAttrMaxSharedMemoryPerBlockOptin, ctx->device));
+    if (td.smem_bytes > smem_max) {
+        free_device(ctx);
+        return CCFD_ERR_ARG;
+    }
 
     // physics constants (src/equation.c:572-578)
     Phys& P = ctx->phys;
@@ -334,19 +355,22 @@ extern "C" int ccfd_upload_case(ccfd_ctx* ctx, const ccfd_mesh* m, const ccfd_bc
 
     // state and scratch
     ctx->nb_cells = (int)((N + 255) / 256);
-    if ((st = dalloc(ctx, &ctx->prim, N)) || (st = dalloc(ctx, &ctx->cons0, N)) ||
-        (st = dalloc(ctx, &ctx->grad, 2 * N)) || (st = dalloc(ctx, &ctx->flux, F)) ||
-        (st = dalloc(ctx, &ctx->u_t, N)) || (st = dalloc(ctx, &ctx->ghost_pface, B + 1)) ||
+    ctx->nb_part = std::max(ctx->nb_cells, ts.n_tiles);
+    if ((st = dalloc(ctx, &ctx->prim_buf[0], N)) || (st = dalloc(ctx, &ctx->prim_buf[1], N)) ||
+        (st = dalloc(ctx, &ctx->cons0, N)) || (st = dalloc(ctx, &ctx->u_t, N)) ||
+        (st = dalloc(ctx, &ctx->grad, 2 * N)) || (st = dalloc(ctx, &ctx->ghost_prim, B + 1)) ||
+        (st = dalloc(ctx, &ctx->bc_flux, B + 1)) || (st = dalloc(ctx, &ctx->ghost_pface, B + 1)) ||
         (st = dalloc(ctx, &ctx->flags, 1)) || (st = dalloc(ctx, &ctx->ctrl, 1)) ||
-        (st = dalloc(ctx, &ctx->dt_partial, ctx->nb_cells)) ||
-        (st = dalloc(ctx, &ctx->dt_bad, ctx->nb_cells)) ||
-        (st = dalloc(ctx, &ctx->res_partial, 4 * (size_t)ctx->nb_cells))) {
+        (st = dalloc(ctx, &ctx->dt_partial, ctx->nb_part)) || (st = dalloc(ctx, &ctx->dt_bad, ctx->nb_part)) ||
+        (st = dalloc(ctx, &ctx->res_partial, 4 * (size_t)ctx->nb_part))) {
         free_device(ctx);
         return st;
     }
+    ctx->cur = 0;
     CK(cudaMemsetAsync(ctx->flags, 0, sizeof(unsigned), ctx->stream));
     CK(cudaMemsetAsync(ctx->ghost_pface, 0, sizeof(double) * (B + 1), ctx->stream));
     CK(cudaMemsetAsync(ctx->grad, 0, sizeof(double4) * 2 * N, ctx->stream));
+    CK(cudaMemsetAsync(ctx->res_partial, 0, sizeof(double) * 4 * ctx->nb_part, ctx->stream));
 
     // control block: t = 0, printTime / printIter of initTimeDisc
     // (src/timeDiscretization.c:238-239)
@@ -397,17 +421,19 @@ extern "C" int ccfd_upload_case(ccfd_ctx* ctx, const ccfd_mesh* m, const ccfd_bc
     return CCFD_OK;
 }
 
-static void fill_residual_launch(ccfd_ctx* ctx, ResidualLaunch& L) {
+static void fill_stage(ccfd_ctx* ctx, StageLaunch& L) {
     memset(&L, 0, sizeof(L));
     L.mesh = ctx->mesh;
+    L.tiles = ctx->tiles;
+    L.ghosts = ctx->ghosts;
     L.phys = ctx->phys;
+    L.sp = ctx->sp;
     L.order = ctx->params.spatial_order;
     L.limiter = ctx->params.limiter;
     L.flux_id = ctx->params.flux;
     L.ns = ctx->params.eqn == CCFD_NAVIER_STOKES;
-    L.prim = ctx->prim;
-    L.grad = ctx->grad;
-    L.flux = ctx->flux;
+    L.ghost_prim = ctx->ghost_prim;
+    L.bc_flux = ctx->bc_flux;
     L.ghost_pface = ctx->ghost_pface;
     L.flags = ctx->flags;
 }
@@ -419,6 +445,8 @@ static int check_flags(ccfd_ctx* ctx) {
     if (f) CK(cudaMemsetAsync(ctx->flags, 0, sizeof(unsigned), ctx->stream));
     return status_from_flags(f);
 }
+
+static double4* cur_prim(ccfd_ctx* ctx) { return ctx->prim_buf[ctx->cur]; }
 
 extern "C" int ccfd_set_state(ccfd_ctx* ctx, const double* state, int kind) {
     if (!ctx || !state || !ctx->uploaded) return CCFD_ERR_ARG;
@@ -439,7 +467,7 @@ extern "C" int ccfd_set_state(ccfd_ctx* ctx, const double* state, int kind) {
         prim[d] = make_double4(pv[0], pv[1], pv[2], pv[3]);
         cons[d] = make_double4(cv[0], cv[1], cv[2], cv[3]);
     }
-    CK(cudaMemcpyAsync(ctx->prim, prim.data(), sizeof(double4) * N, cudaMemcpyHostToDevice, ctx->stream));
+    CK(cudaMemcpyAsync(cur_prim(ctx), prim.data(), sizeof(double4) * N, cudaMemcpyHostToDevice, ctx->stream));
     CK(cudaMemcpyAsync(ctx->cons0, cons.data(), sizeof(double4) * N, cudaMemcpyHostToDevice, ctx->stream));
     CK(cudaStreamSynchronize(ctx->stream));
     return CCFD_OK;
@@ -450,7 +478,7 @@ extern "C" int ccfd_get_state(ccfd_ctx* ctx, double* state, int kind) {
     CK(cudaSetDevice(ctx->device));
     const long N = ctx->N;
     std::vector<double4> h(N);
-    CK(cudaMemcpyAsync(h.data(), kind == CCFD_CONSERVATIVE ? ctx->cons0 : ctx->prim, sizeof(double4) * N,
+    CK(cudaMemcpyAsync(h.data(), kind == CCFD_CONSERVATIVE ? ctx->cons0 : cur_prim(ctx), sizeof(double4) * N,
                        cudaMemcpyDeviceToHost, ctx->stream));
     CK(cudaStreamSynchronize(ctx->stream));
     for (long d = 0; d < N; ++d) {
@@ -486,14 +514,16 @@ extern "C" int ccfd_get_time(ccfd_ctx* ctx, double* t) {
 
 // Residual of the current state into ctx->u_t (device); no host copies.
 int ccfd_residual_device(ccfd_ctx* ctx, double time) {
-    ResidualLaunch L;
-    fill_residual_launch(ctx, L);
+    StageLaunch L;
+    fill_stage(ctx, L);
     L.ctrl = nullptr;
     L.tfix = time;
-    L.update_mode = 0;
+    L.mode = 0;
+    L.prim_in = cur_prim(ctx);
     L.u_t = ctx->u_t;
+    L.grad_out = ctx->params.spatial_order == 2 ? ctx->grad : nullptr;
     L.res_partial = ctx->res_partial;
-    launch_residual(L, ctx->stream);
+    launch_stage(L, ctx->stream);
     CK(cudaGetLastError());
     return CCFD_OK;
 }
@@ -529,12 +559,12 @@ extern "C" int ccfd_residual(ccfd_ctx* ctx, double time, double* u_t_out, double
 extern "C" int ccfd_global_residual(ccfd_ctx* ctx, double res[4]) {
     if (!ctx || !res || !ctx->uploaded) return CCFD_ERR_ARG;
     CK(cudaSetDevice(ctx->device));
-    std::vector<double> h(4 * (size_t)ctx->nb_cells);
+    std::vector<double> h(4 * (size_t)ctx->tiles.n_tiles);
     CK(cudaMemcpyAsync(h.data(), ctx->res_partial, sizeof(double) * h.size(), cudaMemcpyDeviceToHost,
                        ctx->stream));
     CK(cudaStreamSynchronize(ctx->stream));
     double s[4] = {0, 0, 0, 0};
-    for (int b = 0; b < ctx->nb_cells; ++b)
+    for (int b = 0; b < ctx->tiles.n_tiles; ++b)
         for (int v = 0; v < 4; ++v) s[v] += h[4 * b + v];
     for (int v = 0; v < 4; ++v) res[v] = sqrt(s[v] * ctx->total_area_q);
     return CCFD_OK;
@@ -543,7 +573,7 @@ extern "C" int ccfd_global_residual(ccfd_ctx* ctx, double res[4]) {
 extern "C" int ccfd_time_step(ccfd_ctx* ctx, double* dt_out) {
     if (!ctx || !dt_out || !ctx->uploaded) return CCFD_ERR_ARG;
     CK(cudaSetDevice(ctx->device));
-    launch_dt(ctx->mesh, ctx->phys, nullptr, ctx->sp, ctx->prim, ctx->dt_partial, ctx->dt_bad, ctx->stream);
+    launch_dt(ctx->mesh, ctx->phys, nullptr, ctx->sp, cur_prim(ctx), ctx->dt_partial, ctx->dt_bad, ctx->stream);
     CK(cudaGetLastError());
     std::vector<double2> part(ctx->nb_cells);
     std::vector<int> bad(ctx->nb_cells);
@@ -567,39 +597,36 @@ extern "C" int ccfd_time_step(ccfd_ctx* ctx, double* dt_out) {
     return CCFD_OK;
 }
 
-// record one explicit time step into the stream (graph capture); with
-// profiling, each residual evaluation is bracketed by two event-record nodes
-static void record_step(ccfd_ctx* ctx, const std::vector<cudaEvent_t>* ev, size_t* ev_next) {
+// Record one explicit time step starting from primitive buffer `par` into
+// the stream (graph capture); returns the parity after the step.  With
+// profiling, each stage is bracketed by two event-record nodes.
+static int record_step(ccfd_ctx* ctx, int par, const std::vector<cudaEvent_t>* ev, size_t* ev_next) {
     const StepParams& sp = ctx->sp;
-    launch_dt(ctx->mesh, ctx->phys, ctx->ctrl, sp, ctx->prim, ctx->dt_partial, ctx->dt_bad, ctx->stream);
-    launch_step_begin(ctx->ctrl, sp, ctx->dt_partial, ctx->dt_bad, ctx->nb_cells, ctx->stream);
     for (int s = 1; s <= sp.nrk; ++s) {
-        ResidualLaunch L;
-        fill_residual_launch(ctx, L);
+        StageLaunch L;
+        fill_stage(ctx, L);
         L.ctrl = ctx->ctrl;
         L.a_time = sp.rk[s - 1];
-        L.update_mode = 1;
+        L.mode = 1;
+        L.prim_in = ctx->prim_buf[par];
+        L.prim_out = ctx->prim_buf[par ^ 1];
         L.cons0 = ctx->cons0;
-        L.prim_out = ctx->prim;
-        L.u_t = (s == sp.nrk) ? ctx->u_t : nullptr;
         L.rk = sp.rk[s];
         L.last_stage = s == sp.nrk;
-        L.res_partial = (s == sp.nrk) ? ctx->res_partial : nullptr;
-        cudaEvent_t e0 = nullptr, e1 = nullptr;
-        if (ev) {
-            e0 = (*ev)[(*ev_next)++];
-            e1 = (*ev)[(*ev_next)++];
-            cudaEventRecordWithFlags(e0, ctx->stream, cudaEventRecordExternal);
-        }
-        launch_residual(L, ctx->stream);
-        if (ev) cudaEventRecordWithFlags(e1, ctx->stream, cudaEventRecordExternal);
+        L.res_partial = L.last_stage ? ctx->res_partial : nullptr;
+        L.dt_partial = L.last_stage ? ctx->dt_partial : nullptr;
+        L.dt_bad = ctx->dt_bad;
+        if (ev) cudaEventRecordWithFlags((*ev)[(*ev_next)++], ctx->stream, cudaEventRecordExternal);
+        launch_stage(L, ctx->stream);
+        if (ev) cudaEventRecordWithFlags((*ev)[(*ev_next)++], ctx->stream, cudaEventRecordExternal);
+        par ^= 1;
     }
-    launch_step_end(ctx->ctrl, sp, ctx->res_partial, ctx->nb_cells, ctx->wall_ghost, ctx->wall_nl,
-                    ctx->ghost_pface, ctx->stream);
+    launch_step_end(ctx->ctrl, sp, ctx->res_partial, ctx->dt_partial, ctx->dt_bad, ctx->tiles.n_tiles,
+                    ctx->wall_ghost, ctx->wall_nl, ctx->ghost_pface, ctx->stream);
+    return par;
 }
 
-static int build_graph(ccfd_ctx* ctx, int steps, cudaGraphExec_t* exec,
-                       std::vector<cudaEvent_t>* ev) {
+static int build_graph(ccfd_ctx* ctx, int par, int steps, cudaGraphExec_t* exec, std::vector<cudaEvent_t>* ev) {
     cudaGraph_t g;
     if (ev) {
         // events are created before the capture begins
@@ -612,7 +639,7 @@ static int build_graph(ccfd_ctx* ctx, int steps, cudaGraphExec_t* exec,
     }
     size_t ev_next = 0;
     CK(cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
-    for (int i = 0; i < steps; ++i) record_step(ctx, ev, &ev_next);
+    for (int i = 0; i < steps; ++i) par = record_step(ctx, par, ev, &ev_next);
     cudaError_t e = cudaStreamEndCapture(ctx->stream, &g);
     if (e != cudaSuccess) {
         ctx->last_cuda_error = (int)e;
@@ -644,12 +671,12 @@ static void fill_report(ccfd_ctx* ctx, ccfd_report* r) {
     r->status = status_from_flags(c.flags);
 }
 
-// accumulate the residual-evaluation times of the last graph launch (only
-// active stages: an inactive stage is a pair of back-to-back events)
-static int collect_profile(ccfd_ctx* ctx, const std::vector<cudaEvent_t>& ev) {
-    for (size_t i = 0; i + 1 < ev.size(); i += 2) {
+// accumulate the stage times of the steps that ran (their event pairs come
+// first in the graph)
+static int collect_profile(ccfd_ctx* ctx, const std::vector<cudaEvent_t>& ev, size_t pairs) {
+    for (size_t i = 0; i < pairs && 2 * i + 1 < ev.size(); ++i) {
         float ms = 0.0f;
-        CK(cudaEventElapsedTime(&ms, ev[i], ev[i + 1]));
+        CK(cudaEventElapsedTime(&ms, ev[2 * i], ev[2 * i + 1]));
         ctx->prof_ms += ms;
         ctx->prof_count += 1;
     }
@@ -686,11 +713,7 @@ extern "C" int ccfd_run_explicit(ccfd_ctx* ctx, long nsteps, ccfd_report* report
     int st;
     const int kMany = 16;
     const bool prof = ctx->profiling;
-    if (!ctx->graph_one && (st = build_graph(ctx, 1, &ctx->graph_one, prof ? &ctx->prof_ev_one : nullptr)))
-        return st;
-    if (!ctx->graph_many &&
-        (st = build_graph(ctx, kMany, &ctx->graph_many, prof ? &ctx->prof_ev_many : nullptr)))
-        return st;
+    const int nrk = ctx->sp.nrk;
     // read the control block, set the step budget of this call
     CK(cudaMemcpyAsync(ctx->h_ctrl, ctx->ctrl, sizeof(Ctrl), cudaMemcpyDeviceToHost, ctx->stream));
     CK(cudaStreamSynchronize(ctx->stream));
@@ -698,26 +721,31 @@ extern "C" int ccfd_run_explicit(ccfd_ctx* ctx, long nsteps, ccfd_report* report
     const long long big = (1LL << 62);
     long long stop_at = nsteps > 0 ? c.iter + nsteps : big;
     c.stop_at = stop_at;
-    CK(cudaMemcpyAsync(&ctx->ctrl->stop_at, &c.stop_at, sizeof(long long), cudaMemcpyHostToDevice,
-                       ctx->stream));
+    CK(cudaMemcpyAsync(&ctx->ctrl->stop_at, &c.stop_at, sizeof(long long), cudaMemcpyHostToDevice, ctx->stream));
     CK(cudaEventRecord(ctx->ev_run0, ctx->stream));
+    // dt of the current state for the first step; later steps get theirs
+    // from the last stage of the step before
+    launch_dt(ctx->mesh, ctx->phys, ctx->ctrl, ctx->sp, cur_prim(ctx), ctx->dt_partial, ctx->dt_bad, ctx->stream);
+    launch_step_begin(ctx->ctrl, ctx->sp, ctx->dt_partial, ctx->dt_bad, ctx->nb_cells, ctx->stream);
+    CK(cudaGetLastError());
     while (!c.done && c.iter < stop_at) {
         long long remaining = stop_at - c.iter;
-        const std::vector<cudaEvent_t>* used = nullptr;
-        if (remaining >= kMany) {
-            // with profiling, one graph per host round trip so every event
-            // pair is read before the graph records it again
-            int reps = prof ? 1 : 4;
-            for (int rep = 0; rep < reps && remaining >= (long long)kMany * (rep + 1); ++rep)
-                CK(cudaGraphLaunch(ctx->graph_many, ctx->stream));
-            used = &ctx->prof_ev_many;
-        } else {
-            CK(cudaGraphLaunch(ctx->graph_one, ctx->stream));
-            used = &ctx->prof_ev_one;
-        }
+        int which = remaining >= kMany ? 1 : 0;
+        int steps = which ? kMany : 1;
+        int par = ctx->cur;
+        if (!ctx->graph[par][which] &&
+            (st = build_graph(ctx, par, steps, &ctx->graph[par][which], prof ? &ctx->prof_ev[par][which] : nullptr)))
+            return st;
+        long long iter0 = c.iter;
+        CK(cudaGraphLaunch(ctx->graph[par][which], ctx->stream));
         CK(cudaMemcpyAsync(ctx->h_ctrl, ctx->ctrl, sizeof(Ctrl), cudaMemcpyDeviceToHost, ctx->stream));
         CK(cudaStreamSynchronize(ctx->stream));
-        if (prof && (st = collect_profile(ctx, *used))) return st;
+        // steps after a stop inside the graph do not run: the state is in
+        // the buffer the last executed stage wrote
+        long long ran = c.iter - iter0;
+        if ((ran * nrk) & 1) ctx->cur ^= 1;
+        if (prof && (st = collect_profile(ctx, ctx->prof_ev[par][which], (size_t)ran * nrk))) return st;
+        if (ran == 0) break;  // error in the first stage of the graph
     }
     CK(cudaEventRecord(ctx->ev_run1, ctx->stream));
     CK(cudaEventSynchronize(ctx->ev_run1));
@@ -730,9 +758,7 @@ extern "C" int ccfd_run_explicit(ccfd_ctx* ctx, long nsteps, ccfd_report* report
         fill_report(ctx, report);
         report->device_ms = run_ms;
     }
-    int s1 = status_from_flags(c.flags | f);
-    if (s1) return s1;
-    return CCFD_OK;
+    return status_from_flags(c.flags | f);
 }
 
 extern "C" int ccfd_clcd(ccfd_ctx* ctx, double* cl, double* cd) {
@@ -742,11 +768,9 @@ extern "C" int ccfd_clcd(ccfd_ctx* ctx, double* cl, double* cd) {
     std::vector<double> pf(ctx->B + 1);
     std::vector<int> wl(ctx->n_wall);
     std::vector<double> wnl(3 * ctx->n_wall);
-    CK(cudaMemcpyAsync(pf.data(), ctx->ghost_pface, sizeof(double) * pf.size(), cudaMemcpyDeviceToHost,
-                       ctx->stream));
+    CK(cudaMemcpyAsync(pf.data(), ctx->ghost_pface, sizeof(double) * pf.size(), cudaMemcpyDeviceToHost, ctx->stream));
     CK(cudaMemcpyAsync(wl.data(), ctx->wall_ghost, sizeof(int) * wl.size(), cudaMemcpyDeviceToHost, ctx->stream));
-    CK(cudaMemcpyAsync(wnl.data(), ctx->wall_nl, sizeof(double) * wnl.size(), cudaMemcpyDeviceToHost,
-                       ctx->stream));
+    CK(cudaMemcpyAsync(wnl.data(), ctx->wall_nl, sizeof(double) * wnl.size(), cudaMemcpyDeviceToHost, ctx->stream));
     CK(cudaStreamSynchronize(ctx->stream));
     double l = 0.0, d = 0.0;
     for (int k = 0; k < ctx->n_wall; ++k) {

@@ -6,6 +6,7 @@
 #include <vector>
 
 #include "ccfd_b200.h"
+#include "kernels.cuh"
 #include "solver.cuh"
 
 struct ccfd_ctx {
@@ -15,6 +16,9 @@ struct ccfd_ctx {
     ccfd::Phys phys;
     ccfd::StepParams sp;
     ccfd::DevMesh mesh;
+    ccfd::TileDev tiles;
+    ccfd::GhostDev ghosts;
+    int tile_cells = 256;
     ccfd_exact exact;
     double rk[6];
     double total_area_q = 0.0;
@@ -25,12 +29,15 @@ struct ccfd_ctx {
     std::vector<void*> allocs;
     std::vector<int> cell_of_dev;  // device cell -> reference cell
     std::vector<int> dev_of_cell;  // reference cell -> device cell
-    // state and scratch
-    double4* prim = nullptr;
+    // state (primitive state ping-pong: a stage reads one buffer and writes
+    // the other, because neighbouring tiles still read the old state)
+    double4* prim_buf[2] = {nullptr, nullptr};
+    int cur = 0;
     double4* cons0 = nullptr;
-    double4* grad = nullptr;
-    double4* flux = nullptr;
     double4* u_t = nullptr;
+    double4* grad = nullptr;
+    double4* ghost_prim = nullptr;
+    double4* bc_flux = nullptr;
     double* ghost_pface = nullptr;
     unsigned* flags = nullptr;
     ccfd::Ctrl* ctrl = nullptr;
@@ -39,14 +46,16 @@ struct ccfd_ctx {
     int* dt_bad = nullptr;
     double* res_partial = nullptr;
     int nb_cells = 0;
+    int nb_part = 0;  // partial-array length: max(cell blocks, tiles)
     int* wall_ghost = nullptr;
     double* wall_nl = nullptr;
     int n_wall = 0;
-    cudaGraphExec_t graph_one = nullptr, graph_many = nullptr;
+    // step graphs per start buffer parity: [parity][0: one step, 1: many]
+    cudaGraphExec_t graph[2][2] = {{nullptr, nullptr}, {nullptr, nullptr}};
+    std::vector<cudaEvent_t> prof_ev[2][2];
     long newton_total = 0, gmres_total = 0;
     // profiling: event pairs around each residual evaluation in the graphs
     bool profiling = false;
-    std::vector<cudaEvent_t> prof_ev_many, prof_ev_one;
     double prof_ms = 0.0;
     long prof_count = 0;
     cudaEvent_t ev_run0 = nullptr, ev_run1 = nullptr;

@@ -1,38 +1,74 @@
-// Host-side launch interface of the explicit-path kernels.
+// Host-side launch interface of the residual-and-update kernels.
 #pragma once
 
 #include "solver.cuh"
 
 namespace ccfd {
 
-// One residual evaluation R(U) (optionally fused with a Runge-Kutta stage).
-struct ResidualLaunch {
+// Tiles of the fused stage kernel in device memory (see tiles.h).
+struct TileDev {
+    int n_tiles;
+    int smem_bytes;
+    int max_e, max_g, max_hs, max_f;
+    const int* e_off;     // [n_tiles + 1]
+    const int4* counts;   // [n_tiles] (nT, nG, nE cells, nE)
+    const int* e_ref;     // staged entries: device cell or -1-g
+    const int* hs_off;    // [n_tiles + 1] into hs_nbl
+    const short* hs_nbl;  // local E index of the neighbour of each gradient half-side
+    const int* gl_off;    // [n_tiles + 1] into hs_loc
+    const short* hs_loc;  // local half-side start per gradient cell (nG + 1 per tile)
+    const int* f_off;     // [n_tiles + 1]
+    const int* f_id;      // device interior face id
+    const int* f_lr;      // packed local cell indices
+    const int* f_hs;      // packed local half-side indices
+    const int* u_code;    // [H] per device half-side: 2 * local face + neighbour flag, or -1-g
+};
+
+// Per-ghost data of the boundary kernel (device order of ghosts = BCside order).
+struct GhostDev {
+    const int* cell;       // interior device cell
+    const int* hs;         // device half-side of the interior side
+    const int* bc;         // BC table index
+    const double4* gn;     // (ghost bary x, y, n.x, n.y)
+    const double4* ml;     // (face midpoint x, y, len, 0)
+    const double4* bb;     // (baryBaryVec x, y, baryBaryDist, 0) of the interior side
+};
+
+// One residual evaluation (optionally fused with a Runge-Kutta stage).
+struct StageLaunch {
     DevMesh mesh;
+    TileDev tiles;
+    GhostDev ghosts;
     Phys phys;
+    StepParams sp;
     const Ctrl* ctrl;      // device control block, or nullptr (fixed time)
     double tfix;           // time when ctrl == nullptr
     double a_time;         // stage time = t + a_time * dt
     int order, limiter, flux_id, ns;
-    const double4* prim;   // [N] input primitive state
-    double4* grad;         // [2N] limited gradients (scratch)
-    double4* flux;         // [F] face fluxes (scratch)
+    int mode;              // 0: residual u_t only; 1: RK stage
+    const double4* prim_in;
+    double4* prim_out;     // RK: updated primitive state
+    double4* cons0;        // RK: stage-start conservative state (updated in place at the last stage)
+    double4* ghost_prim;   // [B] ghost states at the mirrored barycentres
+    double4* bc_flux;      // [B] boundary face fluxes
     double* ghost_pface;   // [B] interior face pressure at boundary faces
-    unsigned* flags;       // device error bits
-    int update_mode;       // 0: write u_t only; 1: RK stage
-    double4* cons0;        // [N] stage-start conservative state (RK)
-    double4* prim_out;     // [N] updated primitive state (RK)
-    double4* u_t;          // [N] residual output (may be nullptr in RK mode)
-    double rk;             // RK coefficient of this stage
+    double4* u_t;          // [N] residual (mode 0, or RK last stage), may be nullptr
+    double4* grad_out;     // [2N] limited gradients (mode 0 only), may be nullptr
+    double rk;
     int last_stage;
-    double* res_partial;   // [4 * nblocks] residual partial sums or nullptr
+    double* res_partial;   // [4 * n_tiles] or nullptr
+    double2* dt_partial;   // [n_tiles] (last RK stage) or nullptr
+    int* dt_bad;           // [n_tiles]
+    unsigned* flags;
 };
 
-void launch_residual(const ResidualLaunch& L, cudaStream_t st);
+void launch_stage(const StageLaunch& L, cudaStream_t st);
 void launch_dt(const DevMesh& m, const Phys& P, const Ctrl* ctrl, const StepParams& sp,
                const double4* prim, double2* partial, int* bad_partial, cudaStream_t st);
 void launch_step_begin(Ctrl* ctrl, const StepParams& sp, const double2* partial,
                        const int* bad_partial, int nb, cudaStream_t st);
-void launch_step_end(Ctrl* ctrl, const StepParams& sp, const double* res_partial, int nb,
+void launch_step_end(Ctrl* ctrl, const StepParams& sp, const double* res_partial,
+                     const double2* dt_partial, const int* dt_bad, int nb,
                      const int* wall_ghost, const double* wall_nl, const double* ghost_pface,
                      cudaStream_t st);
 

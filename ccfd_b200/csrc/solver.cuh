@@ -8,23 +8,17 @@
 
 namespace ccfd {
 
-// Mesh in device memory, uploaded once (32-bit indices; AoS records of 32 B
-// so that every gather of a cell / face record is one 32-byte sector).
+// Mesh in device memory, uploaded once: cells in Hilbert order, 32-bit
+// indices, 32-byte records so that every gather of a record is one sector.
 struct DevMesh {
-    int N, F, B, H;
+    int N, F, B, H;           // cells, interior faces, ghosts, half-sides
     const int* hs_off;        // [N+1] CSR offsets of the per-cell half-sides
     const int* hs_nb;         // [H] neighbour cell, or -1-g for ghost g
-    const int* hs_fs;         // [H] face index f (cell owns f) or ~f
     const double4* hs_gw;     // [H] (GP.x, GP.y, w.x, w.y)
     const double4* cell_geo;  // [N] (area, 1/area, sx, sy)
     const double* venk_eps2;  // [N] Venkatakrishnan epsilon^2
-    const int2* face_c;       // [F] (owner, neighbour or -1-g)
-    const double4* face_gp;   // [F] (owner GP.x, GP.y, neighbour GP.x, GP.y)
-    const double4* face_nl;   // [F] (n.x, n.y, len, 0)
+    const double4* face_nl;   // [F] (n.x, n.y, len, 0) of interior faces
     const double4* face_bb;   // [F] (baryBaryVec.x, .y, baryBaryDist, 0)
-    const int* ghost_bc;      // [B] BC table index
-    const double4* ghost_gn;  // [B] (ghost bary.x, .y, n.x, n.y)
-    const double2* ghost_mid; // [B] face midpoint (exact-solution point)
 };
 
 // Time-loop control block in device memory.  The time step, simulation time,
