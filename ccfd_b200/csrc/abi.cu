@@ -336,6 +336,11 @@ extern "C" int ccfd_upload_case(ccfd_ctx* ctx, const ccfd_mesh* m, const ccfd_bc
     P.ex.dx_ref = ex->dx_ref;
     ctx->total_area_q = m->total_area_q;
     ctx->exact = *ex;
+    if ((st = dalloc(ctx, &ctx->phys_g, 1))) {
+        free_device(ctx);
+        return st;
+    }
+    CK(cudaMemcpyAsync(ctx->phys_g, &ctx->phys, sizeof(Phys), cudaMemcpyHostToDevice, ctx->stream));
 
     // wing surface list for CL / CD
     std::vector<int> wl;
@@ -358,8 +363,8 @@ extern "C" int ccfd_upload_case(ccfd_ctx* ctx, const ccfd_mesh* m, const ccfd_bc
     ctx->nb_part = std::max(ctx->nb_cells, ts.n_tiles);
     if ((st = dalloc(ctx, &ctx->prim_buf[0], N)) || (st = dalloc(ctx, &ctx->prim_buf[1], N)) ||
         (st = dalloc(ctx, &ctx->cons0, N)) || (st = dalloc(ctx, &ctx->u_t, N)) ||
-        (st = dalloc(ctx, &ctx->grad, 2 * N)) || (st = dalloc(ctx, &ctx->ghost_prim, B + 1)) ||
-        (st = dalloc(ctx, &ctx->bc_flux, B + 1)) || (st = dalloc(ctx, &ctx->ghost_pface, B + 1)) ||
+        (st = dalloc(ctx, &ctx->grad, 2 * N)) || (st = dalloc(ctx, &ctx->ticket, 1)) ||
+        (st = dalloc(ctx, &ctx->ghost_pface, B + 1)) ||
         (st = dalloc(ctx, &ctx->flags, 1)) || (st = dalloc(ctx, &ctx->ctrl, 1)) ||
         (st = dalloc(ctx, &ctx->dt_partial, ctx->nb_part)) || (st = dalloc(ctx, &ctx->dt_bad, ctx->nb_part)) ||
         (st = dalloc(ctx, &ctx->res_partial, 4 * (size_t)ctx->nb_part))) {
@@ -368,6 +373,7 @@ extern "C" int ccfd_upload_case(ccfd_ctx* ctx, const ccfd_mesh* m, const ccfd_bc
     }
     ctx->cur = 0;
     CK(cudaMemsetAsync(ctx->flags, 0, sizeof(unsigned), ctx->stream));
+    CK(cudaMemsetAsync(ctx->ticket, 0, sizeof(unsigned), ctx->stream));
     CK(cudaMemsetAsync(ctx->ghost_pface, 0, sizeof(double) * (B + 1), ctx->stream));
     CK(cudaMemsetAsync(ctx->grad, 0, sizeof(double4) * 2 * N, ctx->stream));
     CK(cudaMemsetAsync(ctx->res_partial, 0, sizeof(double) * 4 * ctx->nb_part, ctx->stream));
@@ -427,15 +433,17 @@ static void fill_stage(ccfd_ctx* ctx, StageLaunch& L) {
     L.tiles = ctx->tiles;
     L.ghosts = ctx->ghosts;
     L.phys = ctx->phys;
+    L.phys_g = ctx->phys_g;
     L.sp = ctx->sp;
     L.order = ctx->params.spatial_order;
     L.limiter = ctx->params.limiter;
     L.flux_id = ctx->params.flux;
     L.ns = ctx->params.eqn == CCFD_NAVIER_STOKES;
-    L.ghost_prim = ctx->ghost_prim;
-    L.bc_flux = ctx->bc_flux;
     L.ghost_pface = ctx->ghost_pface;
     L.flags = ctx->flags;
+    L.ticket = ctx->ticket;
+    L.wall_ghost = ctx->wall_ghost;
+    L.wall_nl = ctx->wall_nl;
 }
 
 static int check_flags(ccfd_ctx* ctx) {
@@ -621,8 +629,6 @@ static int record_step(ccfd_ctx* ctx, int par, const std::vector<cudaEvent_t>* e
         if (ev) cudaEventRecordWithFlags((*ev)[(*ev_next)++], ctx->stream, cudaEventRecordExternal);
         par ^= 1;
     }
-    launch_step_end(ctx->ctrl, sp, ctx->res_partial, ctx->dt_partial, ctx->dt_bad, ctx->tiles.n_tiles,
-                    ctx->wall_ghost, ctx->wall_nl, ctx->ghost_pface, ctx->stream);
     return par;
 }
 

@@ -36,8 +36,8 @@ struct ccfd_ctx {
     double4* cons0 = nullptr;
     double4* u_t = nullptr;
     double4* grad = nullptr;
-    double4* ghost_prim = nullptr;
-    double4* bc_flux = nullptr;
+    unsigned* ticket = nullptr;
+    ccfd::Phys* phys_g = nullptr;
     double* ghost_pface = nullptr;
     unsigned* flags = nullptr;
     ccfd::Ctrl* ctrl = nullptr;

@@ -40,6 +40,7 @@ struct StageLaunch {
     TileDev tiles;
     GhostDev ghosts;
     Phys phys;
+    const Phys* phys_g;    // the same constants in global memory (boundary code)
     StepParams sp;
     const Ctrl* ctrl;      // device control block, or nullptr (fixed time)
     double tfix;           // time when ctrl == nullptr
@@ -49,8 +50,6 @@ struct StageLaunch {
     const double4* prim_in;
     double4* prim_out;     // RK: updated primitive state
     double4* cons0;        // RK: stage-start conservative state (updated in place at the last stage)
-    double4* ghost_prim;   // [B] ghost states at the mirrored barycentres
-    double4* bc_flux;      // [B] boundary face fluxes
     double* ghost_pface;   // [B] interior face pressure at boundary faces
     double4* u_t;          // [N] residual (mode 0, or RK last stage), may be nullptr
     double4* grad_out;     // [2N] limited gradients (mode 0 only), may be nullptr
@@ -60,6 +59,9 @@ struct StageLaunch {
     double2* dt_partial;   // [n_tiles] (last RK stage) or nullptr
     int* dt_bad;           // [n_tiles]
     unsigned* flags;
+    unsigned* ticket;      // CTA completion counter of the last stage (zero between launches)
+    const int* wall_ghost; // wing surface ghosts in calcCoef summation order
+    const double* wall_nl; // their (n.x, n.y, len)
 };
 
 void launch_stage(const StageLaunch& L, cudaStream_t st);
@@ -67,9 +69,5 @@ void launch_dt(const DevMesh& m, const Phys& P, const Ctrl* ctrl, const StepPara
                const double4* prim, double2* partial, int* bad_partial, cudaStream_t st);
 void launch_step_begin(Ctrl* ctrl, const StepParams& sp, const double2* partial,
                        const int* bad_partial, int nb, cudaStream_t st);
-void launch_step_end(Ctrl* ctrl, const StepParams& sp, const double* res_partial,
-                     const double2* dt_partial, const int* dt_bad, int nb,
-                     const int* wall_ghost, const double* wall_nl, const double* ghost_pface,
-                     cudaStream_t st);
 
 }  // namespace ccfd

@@ -1,23 +1,25 @@
 // Kernels of the residual-and-update path.
 //
-//   k_bnd    per ghost (boundary face), small: ghost state at the mirrored
-//            barycentre (setBCatBarys, src/boundary.c:320-331), limited
-//            gradient of the interior cell, ghost state at the face
-//            (setBCatSides, :300-314) and the boundary-face flux
 //   k_stage  per tile (one CTA), fused: stage the primitive states of the
-//            tile and two neighbour rings in shared memory; least-squares
+//            tile, two neighbour rings and the adjacent ghost cells (ghost
+//            states at the mirrored barycentres, setBCatBarys, src/boundary.c:
+//            320-331) in shared memory; least-squares
 //            gradients with Barth-Jespersen / Venkatakrishnan limiting for the
 //            tile and ring 1 (spatialReconstruction, src/reconstruction.c:
 //            198-314); limited linear reconstruction, convective and viscous
-//            flux of every interior face of the tile (fluxCalculation,
+//            flux of every face of the tile, ghost states at boundary faces
+//            (setBCatSides, src/boundary.c:300-314; fluxCalculation,
 //            src/fluxCalculation.c:882-998); per-cell sum of the face fluxes
 //            in the reference's side order, no atomics (src/finiteVolume.c:
 //            96-120); Runge-Kutta stage update with consPrim
 //            (src/timeDiscretization.c:362-398); at the last stage the local
-//            time step of the new state and the global-residual partial sums
-//   k_dt / k_step_begin / k_step_end   calcTimeStep (src/timeDiscretization.c:
-//            249-329), the per-step bookkeeping of timeDisc (:595-731) and the
-//            wing coefficients of calcCoef (src/analyze.c:292-387)
+//            time step of the new state and the global-residual partial sums;
+//            the CTA that finishes last reduces the partials in a fixed order
+//            and performs the end-of-step bookkeeping of timeDisc
+//            (src/timeDiscretization.c:595-731), the wing coefficients of
+//            calcCoef (src/analyze.c:292-387) and the next time step
+//   k_dt / k_step_begin   calcTimeStep (src/timeDiscretization.c:249-329)
+//            for the first step of a run
 //
 // Gradients and face fluxes live only in shared memory.  Floating-point
 // operations keep the reference's operand order; the library is compiled
@@ -146,81 +148,37 @@ __device__ __forceinline__ void face_flux(const Phys& P, double nx, double ny, d
     for (int v = 0; v < 4; ++v) F[v] *= len;
 }
 
-template <int NS>
-__device__ void bnd_flux_dispatch(int flux, const Phys& P, double nx, double ny, double len,
-                                  const double L[4], const double R[4], const double q0[4],
-                                  const double q1[4], const double g0x[4], const double g0y[4],
-                                  const double g1x[4], const double g1y[4], double4 bb,
-                                  double F[4], unsigned* flags) {
-#define CCFD_BF(ID) \
-    case ID: face_flux<ID, NS>(P, nx, ny, len, L, R, q0, q1, g0x, g0y, g1x, g1y, bb, F, flags); break;
-    switch (flux) {
-        CCFD_BF(1) CCFD_BF(2) CCFD_BF(3) CCFD_BF(4) CCFD_BF(5) CCFD_BF(6)
-        CCFD_BF(7) CCFD_BF(8) CCFD_BF(9) CCFD_BF(10) CCFD_BF(11)
-    }
-#undef CCFD_BF
-}
-
 // ghost state at the mirrored barycentre of ghost g from interior state q
-__device__ __forceinline__ void ghost_bary(const GhostDev& G, const Phys& P, int g, double time,
-                                           const double q[4], double out[4], unsigned* flags) {
-    double4 gn = G.gn[g];
+// (kept out of line: the boundary code is rare and heavy, the hot face code
+// should not carry its registers)
+__device__ __noinline__ double4 ghost_bary(const int* __restrict__ gbc, const double4* __restrict__ ggn,
+                                           const Phys* __restrict__ Pg, int g, double time, double4 qv,
+                                           unsigned* flags) {
+    const Phys& P = *Pg;
+    double4 gn = ggn[g];
     double x[2] = {gn.x, gn.y};
-    boundary_state(P, P.bc[G.bc[g]], gn.z, gn.w, time, q, out, x, flags);
+    double q[4] = {qv.x, qv.y, qv.z, qv.w}, out[4];
+    boundary_state(P, P.bc[gbc[g]], gn.z, gn.w, time, q, out, x, flags);
+    return make_double4(out[0], out[1], out[2], out[3]);
 }
 
-// one thread per ghost / boundary face
-template <int NS>
-__global__ void __launch_bounds__(128) k_bnd(StageLaunch L) {
-    int g = blockIdx.x * blockDim.x + threadIdx.x;
-    const DevMesh& m = L.mesh;
-    if (g >= m.B || inactive(L.ctrl)) return;
-    const Phys& P = L.phys;
-    double time = stage_time(L.ctrl, L.tfix, L.a_time);
-    int c = L.ghosts.cell[g];
-    double q0[4];
-    ld4(L.prim_in[c], q0);
-    double gb[4];
-    ghost_bary(L.ghosts, P, g, time, q0, gb, L.flags);
-    L.ghost_prim[g] = mk4(gb);
-    double ux[4] = {0, 0, 0, 0}, uy[4] = {0, 0, 0, 0};
-    double Lf[4];
-    if (L.order == 2) {
-        int h0 = m.hs_off[c], nh = m.hs_off[c + 1] - h0;
-        double eps2 = L.limiter == 2 ? m.venk_eps2[c] : 0.0;
-        auto nbr = [&](int k, double qn[4]) {
-            int nb = m.hs_nb[h0 + k];
-            if (nb >= 0) ld4(L.prim_in[nb], qn);
-            else ghost_bary(L.ghosts, P, -1 - nb, time, q0, qn, L.flags);
-        };
-        auto gw = [&](int k) { return m.hs_gw[h0 + k]; };
-        cell_gradient(L.limiter, q0, nh, eps2, nbr, gw, ux, uy);
-        double4 gp = m.hs_gw[L.ghosts.hs[g]];
-#pragma unroll
-        for (int v = 0; v < 4; ++v) Lf[v] = q0[v] + gp.x * ux[v] + gp.y * uy[v];
-    } else {
-#pragma unroll
-        for (int v = 0; v < 4; ++v) Lf[v] = q0[v];
-        // the ghost cell state is only set by the second-order
-        // reconstruction; it is zero otherwise (calloc'd ghost element)
-        gb[0] = gb[1] = gb[2] = gb[3] = 0.0;
-    }
-    double4 gn = L.ghosts.gn[g], ml = L.ghosts.ml[g];
-    double R[4];
-    double xm[2] = {ml.x, ml.y};
-    boundary_state(P, P.bc[L.ghosts.bc[g]], gn.z, gn.w, time, Lf, R, xm, L.flags);
-    if (L.ghost_pface) L.ghost_pface[g] = Lf[3];
-    double zero[4] = {0, 0, 0, 0}, F[4];
-    double4 bb = NS ? L.ghosts.bb[g] : make_double4(0, 0, 1, 0);
-    bnd_flux_dispatch<NS>(L.flux_id, P, gn.z, gn.w, ml.z, Lf, R, q0, gb, ux, uy, zero, zero, bb, F,
-                          L.flags);
-    L.bc_flux[g] = mk4(F);
+// ghost state at a boundary face from the reconstructed interior face state
+__device__ __noinline__ double4 ghost_face(const int* __restrict__ gbc, const double4* __restrict__ ggn,
+                                           const double4* __restrict__ gml, const Phys* __restrict__ Pg,
+                                           int g, double time, double4 Lv, unsigned* flags) {
+    const Phys& P = *Pg;
+    double4 gn = ggn[g], ml = gml[g];
+    double x[2] = {ml.x, ml.y};
+    double Lq[4] = {Lv.x, Lv.y, Lv.z, Lv.w}, R[4];
+    boundary_state(P, P.bc[gbc[g]], gn.z, gn.w, time, Lq, R, x, flags);
+    return make_double4(R[0], R[1], R[2], R[3]);
 }
 
 template <int NV>
 __device__ __forceinline__ void block_sum(double v[NV], double* out) {
     __shared__ double sh[NV][32];
     int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    __syncthreads();
 #pragma unroll
     for (int k = 0; k < NV; ++k)
 #pragma unroll
@@ -245,6 +203,7 @@ __device__ __forceinline__ void block_min2(double a, double b, int bad, double2*
     __shared__ double sa[32], sb[32];
     __shared__ int sbad[32];
     int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    __syncthreads();
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) {
         a = fmin(a, __shfl_down_sync(0xffffffffu, a, o));
@@ -289,178 +248,10 @@ __device__ __forceinline__ bool local_dt(const Phys& P, const StepParams& sp, co
     return ok;
 }
 
-// fused residual evaluation (+ RK stage) of one tile per CTA
-template <int FLUX, int ORDER, int NS>
-__global__ void __launch_bounds__(kThreads, 2) k_stage(StageLaunch L) {
-    extern __shared__ double4 smem[];
-    if (inactive(L.ctrl)) return;
-    const DevMesh& m = L.mesh;
-    const TileDev& T = L.tiles;
-    const Phys& P = L.phys;
-    const int t = blockIdx.x, tid = threadIdx.x;
-    const int4 cnt = T.counts[t];
-    const int nT = cnt.x, nG = cnt.y, nE = cnt.w;
-    const int e0 = T.e_off[t];
-    double4* ps = smem;                                   // [max_e] states
-    double4* gs = ps + T.max_e;                           // [2 max_g] gradients
-    double2* hgp = reinterpret_cast<double2*>(gs + 2 * T.max_g);  // [max_hs] GP
-    double4* fs = reinterpret_cast<double4*>(hgp + T.max_hs + (T.max_hs & 1));  // [max_f]
-
-    // A: stage the states of the tile, its rings and ghosts
-    for (int e = tid; e < nE; e += kThreads) {
-        int r = T.e_ref[e0 + e];
-        ps[e] = r >= 0 ? L.prim_in[r] : L.ghost_prim[-1 - r];
-    }
-    __syncthreads();
-
-    // B: limited gradients of the tile and ring-1 cells
-    const int hb = T.hs_off[t], gb = T.gl_off[t];
-    if (ORDER == 2) {
-        for (int i = tid; i < nG; i += kThreads) {
-            int d = T.e_ref[e0 + i];
-            int h0 = m.hs_off[d], nh = m.hs_off[d + 1] - h0;
-            int lo = T.hs_loc[gb + i];
-            double q[4], ux[4], uy[4];
-            ld4(ps[i], q);
-            double eps2 = L.limiter == 2 ? m.venk_eps2[d] : 0.0;
-            auto nbr = [&](int k, double qn[4]) { ld4(ps[T.hs_nbl[hb + lo + k]], qn); };
-            auto gw = [&](int k) {
-                double4 g = m.hs_gw[h0 + k];
-                hgp[lo + k] = make_double2(g.x, g.y);
-                return g;
-            };
-            cell_gradient(L.limiter, q, nh, eps2, nbr, gw, ux, uy);
-            gs[2 * i] = mk4(ux);
-            gs[2 * i + 1] = mk4(uy);
-        }
-        __syncthreads();
-    }
-
-    // C: interior face fluxes of the tile
-    const int f0 = T.f_off[t], nF = T.f_off[t + 1] - f0;
-    for (int j = tid; j < nF; j += kThreads) {
-        int fid = T.f_id[f0 + j];
-        int lr = T.f_lr[f0 + j];
-        int il = lr & 0xffff, ir = lr >> 16;
-        double q0[4], q1[4], Lf[4], Rf[4];
-        double g0x[4] = {0, 0, 0, 0}, g0y[4] = {0, 0, 0, 0}, g1x[4] = {0, 0, 0, 0}, g1y[4] = {0, 0, 0, 0};
-        ld4(ps[il], q0);
-        ld4(ps[ir], q1);
-        if (ORDER == 2) {
-            int hh = T.f_hs[f0 + j];
-            double2 gpl = hgp[hh & 0xffff], gpr = hgp[hh >> 16];
-            ld4(gs[2 * il], g0x);
-            ld4(gs[2 * il + 1], g0y);
-            ld4(gs[2 * ir], g1x);
-            ld4(gs[2 * ir + 1], g1y);
-#pragma unroll
-            for (int v = 0; v < 4; ++v) {
-                Lf[v] = q0[v] + gpl.x * g0x[v] + gpl.y * g0y[v];
-                Rf[v] = q1[v] + gpr.x * g1x[v] + gpr.y * g1y[v];
-            }
-        } else {
-#pragma unroll
-            for (int v = 0; v < 4; ++v) {
-                Lf[v] = q0[v];
-                Rf[v] = q1[v];
-            }
-        }
-        double4 nl = m.face_nl[fid];
-        double4 bb = NS ? m.face_bb[fid] : make_double4(0, 0, 1, 0);
-        double F[4];
-        face_flux<FLUX, NS>(P, nl.x, nl.y, nl.z, Lf, Rf, q0, q1, g0x, g0y, g1x, g1y, bb, F, L.flags);
-        fs[j] = mk4(F);
-    }
-    __syncthreads();
-
-    // D: per-cell flux sum in side order, update
-    double r[4] = {0, 0, 0, 0};
-    double dconv = 1e150, dvisc = 1e150;
-    int bad = 0;
-    const bool rk = L.mode == 1;
-    for (int i = tid; i < nT; i += kThreads) {
-        int d = T.e_ref[e0 + i];
-        int h0 = m.hs_off[d], h1 = m.hs_off[d + 1];
-        double s[4] = {0.0, 0.0, 0.0, 0.0};
-        for (int h = h0; h < h1; ++h) {
-            int code = T.u_code[h];
-            double F[4];
-            if (code >= 0) {
-                ld4(fs[code >> 1], F);
-                if (code & 1) {
-#pragma unroll
-                    for (int v = 0; v < 4; ++v) s[v] += -F[v];
-                } else {
-#pragma unroll
-                    for (int v = 0; v < 4; ++v) s[v] += F[v];
-                }
-            } else {
-                ld4(L.bc_flux[-1 - code], F);
-#pragma unroll
-                for (int v = 0; v < 4; ++v) s[v] += F[v];
-            }
-        }
-        double4 geo = m.cell_geo[d];
-        double ut[4];
-#pragma unroll
-        for (int v = 0; v < 4; ++v) ut[v] = (0.0 - s[v]) * geo.y;
-        if (L.u_t) L.u_t[d] = mk4(ut);
-        if (!rk && L.grad_out) {
-            L.grad_out[2 * d] = gs[2 * i];
-            L.grad_out[2 * d + 1] = gs[2 * i + 1];
-        }
-        if (rk) {
-            double c0[4], cn[4], pn[4];
-            ld4(L.cons0[d], c0);
-            double adt = L.rk * L.ctrl->dt;
-#pragma unroll
-            for (int v = 0; v < 4; ++v) cn[v] = c0[v] + adt * ut[v];
-            cons_prim(P.gam1, cn, pn);
-            L.prim_out[d] = mk4(pn);
-            if (L.last_stage) {
-                L.cons0[d] = mk4(cn);
-                double a, b;
-                if (!local_dt(P, L.sp, pn, geo, &a, &b)) bad = 1;
-                else {
-                    dconv = fmin(dconv, a);
-                    dvisc = fmin(dvisc, b);
-                }
-            }
-        }
-#pragma unroll
-        for (int v = 0; v < 4; ++v) r[v] += geo.x * ut[v] * ut[v];
-    }
-    if (L.res_partial) {
-        double out[4];
-        block_sum<4>(r, out);
-        if (tid == 0)
-#pragma unroll
-            for (int v = 0; v < 4; ++v) L.res_partial[4 * t + v] = out[v];
-    }
-    if (L.dt_partial) block_min2(dconv, dvisc, bad, &L.dt_partial[t], &L.dt_bad[t]);
-}
-
-// per-block minima of the convective and viscous time steps
-__global__ void __launch_bounds__(256) k_dt(DevMesh m, Phys P, const Ctrl* ctrl, StepParams sp,
-                                            const double4* __restrict__ prim,
-                                            double2* __restrict__ partial, int* bad_partial) {
-    int c = blockIdx.x * blockDim.x + threadIdx.x;
-    double dconv = 1e150, dvisc = 1e150;
-    int bad = 0;
-    if (c < m.N) {
-        double q[4];
-        ld4(prim[c], q);
-        if (!local_dt(P, sp, q, m.cell_geo[c], &dconv, &dvisc)) {
-            bad = 1;
-            dconv = dvisc = 1e150;
-        }
-    }
-    block_min2(dconv, dvisc, bad, &partial[blockIdx.x], &bad_partial[blockIdx.x]);
-}
-
 // global dt from the partial minima with the output / end-time clamp
 // (src/timeDiscretization.c:310-321)
-__device__ void finish_dt(Ctrl* ctrl, const StepParams& sp, double dtc, double dtv, int bad) {
+__device__ __forceinline__ void finish_dt(Ctrl* ctrl, const StepParams& sp, double dtc, double dtv,
+                                          int bad) {
     if (bad) {
         ctrl->flags |= FLAG_DT;
         ctrl->done = 1;
@@ -475,78 +266,35 @@ __device__ void finish_dt(Ctrl* ctrl, const StepParams& sp, double dtc, double d
     ctrl->dt = dt;
 }
 
-__device__ void reduce_min2(const double2* partial, const int* bad_partial, int nb, double* a_out,
-                            double* b_out, int* bad_out) {
-    __shared__ double sa[256], sb[256];
-    __shared__ int sbad[256];
-    int tid = threadIdx.x;
+// End of a step, executed by one whole block: global residual (fixed-order
+// reduction of the per-tile partials), wing coefficients, t += dt, the stop
+// tests of timeDisc (src/timeDiscretization.c:609-731) and the next dt.
+__device__ __forceinline__ void step_end_block(Ctrl* ctrl, const StepParams& sp, const double* res_partial,
+                               const double2* dt_partial, const int* dt_bad, int nb,
+                               const int* wall_ghost, const double* wall_nl,
+                               const double* ghost_pface) {
+    __shared__ double s_res[4];
+    __shared__ double2 s_dt;
+    __shared__ int s_bad;
+    const int tid = threadIdx.x;
+    double r[4] = {0.0, 0.0, 0.0, 0.0};
     double a = 1e150, b = 1e150;
     int bad = 0;
     for (int i = tid; i < nb; i += blockDim.x) {
-        a = fmin(a, partial[i].x);
-        b = fmin(b, partial[i].y);
-        bad |= bad_partial[i];
+#pragma unroll
+        for (int v = 0; v < 4; ++v) r[v] += __ldcg(&res_partial[4 * i + v]);
+        double2 d = __ldcg(&dt_partial[i]);
+        a = fmin(a, d.x);
+        b = fmin(b, d.y);
+        bad |= __ldcg(&dt_bad[i]);
     }
-    sa[tid] = a; sb[tid] = b; sbad[tid] = bad;
+    block_sum<4>(r, s_res);
+    block_min2(a, b, bad, &s_dt, &s_bad);
     __syncthreads();
-    for (int s = blockDim.x / 2; s > 0; s >>= 1) {
-        if (tid < s) {
-            sa[tid] = fmin(sa[tid], sa[tid + s]);
-            sb[tid] = fmin(sb[tid], sb[tid + s]);
-            sbad[tid] |= sbad[tid + s];
-        }
-        __syncthreads();
-    }
-    *a_out = sa[0];
-    *b_out = sb[0];
-    *bad_out = sbad[0];
-}
-
-// first step of a run: dt of the current state, whether the step runs
-__global__ void k_step_begin(Ctrl* ctrl, StepParams sp, const double2* __restrict__ partial,
-                             const int* __restrict__ bad_partial, int nb) {
-    double a, b;
-    int bad;
-    reduce_min2(partial, bad_partial, nb, &a, &b, &bad);
-    if (threadIdx.x != 0) return;
-    if (ctrl->done || ctrl->iter >= ctrl->stop_at) {
-        ctrl->active = 0;
-        return;
-    }
-    ctrl->active = 1;
-    finish_dt(ctrl, sp, a, b, bad);
-}
-
-// end of a step: global residual, wing coefficients, t += dt, the stop tests
-// of timeDisc (src/timeDiscretization.c:609-731) and the next step's dt
-__global__ void k_step_end(Ctrl* ctrl, StepParams sp, const double* __restrict__ res_partial,
-                           const double2* __restrict__ dt_partial, const int* __restrict__ dt_bad,
-                           int nb, const int* __restrict__ wall_ghost,
-                           const double* __restrict__ wall_nl,
-                           const double* __restrict__ ghost_pface) {
-    __shared__ double sh[4][256];
-    int tid = threadIdx.x;
-    if (!ctrl->active) return;
-    double r[4] = {0.0, 0.0, 0.0, 0.0};
-    for (int i = tid; i < nb; i += blockDim.x)
-#pragma unroll
-        for (int v = 0; v < 4; ++v) r[v] += res_partial[4 * i + v];
-#pragma unroll
-    for (int v = 0; v < 4; ++v) sh[v][tid] = r[v];
-    __syncthreads();
-    for (int s = blockDim.x / 2; s > 0; s >>= 1) {
-        if (tid < s)
-#pragma unroll
-            for (int v = 0; v < 4; ++v) sh[v][tid] += sh[v][tid + s];
-        __syncthreads();
-    }
-    double dta, dtb;
-    int dbad;
-    reduce_min2(dt_partial, dt_bad, nb, &dta, &dtb, &dbad);
     if (tid != 0) return;
     double res[6];
 #pragma unroll
-    for (int v = 0; v < 4; ++v) res[v] = sqrt(sh[v][0] * sp.total_area_q);
+    for (int v = 0; v < 4; ++v) res[v] = sqrt(s_res[v] * sp.total_area_q);
     res[4] = res[5] = 0.0;
     double dt = ctrl->dt;
     ctrl->t += dt;
@@ -556,7 +304,7 @@ __global__ void k_step_end(Ctrl* ctrl, StepParams sp, const double* __restrict__
         double cl_old = ctrl->cl, cd_old = ctrl->cd;
         double cl = 0.0, cd = 0.0;
         for (int k = 0; k < sp.n_wall; ++k) {
-            double p0 = ghost_pface[wall_ghost[k]];
+            double p0 = __ldcg(&ghost_pface[wall_ghost[k]]);
             double wnx = wall_nl[3 * k], wny = wall_nl[3 * k + 1], wl = wall_nl[3 * k + 2];
             cl += wny * p0 * wl;
             cd += wnx * p0 * wl;
@@ -616,9 +364,255 @@ __global__ void k_step_end(Ctrl* ctrl, StepParams sp, const double* __restrict__
         return;
     }
     if (iter >= ctrl->stop_at) return;
-    // next step: dt of the new state (computed by the last stage)
     ctrl->active = 1;
-    finish_dt(ctrl, sp, dta, dtb, dbad);
+    finish_dt(ctrl, sp, s_dt.x, s_dt.y, s_bad);
+}
+
+// fused residual evaluation (+ RK stage) of one tile per CTA
+template <int FLUX, int ORDER, int NS>
+#ifndef CCFD_STAGE_MIN_BLOCKS
+#define CCFD_STAGE_MIN_BLOCKS 3
+#endif
+__global__ void __launch_bounds__(kThreads, CCFD_STAGE_MIN_BLOCKS) k_stage(StageLaunch L) {
+    extern __shared__ double4 smem[];
+    if (inactive(L.ctrl)) return;
+    const DevMesh& m = L.mesh;
+    const TileDev& T = L.tiles;
+    const Phys& P = L.phys;
+    const int t = blockIdx.x, tid = threadIdx.x;
+    const int4 cnt = T.counts[t];
+    const int nT = cnt.x, nG = cnt.y, nEc = cnt.z, nE = cnt.w;
+    const int e0 = T.e_off[t];
+    const double time = stage_time(L.ctrl, L.tfix, L.a_time);
+    double4* ps = smem;                                   // [max_e] states
+    double4* gs = ps + T.max_e;                           // [2 max_g] gradients
+    double2* hgp = reinterpret_cast<double2*>(gs + 2 * T.max_g);  // [max_hs] GP
+    double4* fs = reinterpret_cast<double4*>(hgp + T.max_hs + (T.max_hs & 1));  // [max_f]
+
+    // A: stage the states of the tile and its rings; ghost cells get the
+    // boundary state at their mirrored barycentre (second order only: the
+    // reference sets ghost cell states in its second-order reconstruction
+    // and leaves them zero otherwise)
+    for (int e = tid; e < nEc; e += kThreads) ps[e] = L.prim_in[T.e_ref[e0 + e]];
+    for (int e = nEc + tid; e < nE; e += kThreads) {
+        int g = -1 - T.e_ref[e0 + e];
+        double gq[4] = {0.0, 0.0, 0.0, 0.0};
+        if (ORDER == 2) {
+            ld4(ghost_bary(L.ghosts.bc, L.ghosts.gn, L.phys_g, g, time,
+                           L.prim_in[L.ghosts.cell[g]], L.flags), gq);
+        }
+        ps[e] = mk4(gq);
+    }
+    __syncthreads();
+
+    // B: limited gradients of the tile and ring-1 cells
+    const int hb = T.hs_off[t], gb = T.gl_off[t];
+    if (ORDER == 2) {
+        for (int i = tid; i < nG; i += kThreads) {
+            int d = T.e_ref[e0 + i];
+            int h0 = m.hs_off[d], nh = m.hs_off[d + 1] - h0;
+            int lo = T.hs_loc[gb + i];
+            double q[4], ux[4], uy[4];
+            ld4(ps[i], q);
+            double eps2 = L.limiter == 2 ? m.venk_eps2[d] : 0.0;
+            auto nbr = [&](int k, double qn[4]) { ld4(ps[T.hs_nbl[hb + lo + k]], qn); };
+            auto gw = [&](int k) {
+                double4 g = m.hs_gw[h0 + k];
+                hgp[lo + k] = make_double2(g.x, g.y);
+                return g;
+            };
+            cell_gradient(L.limiter, q, nh, eps2, nbr, gw, ux, uy);
+            gs[2 * i] = mk4(ux);
+            gs[2 * i + 1] = mk4(uy);
+        }
+        __syncthreads();
+    }
+
+    // C: fluxes of the tile's faces (interior faces, then boundary faces)
+    const int f0 = T.f_off[t], nF = T.f_off[t + 1] - f0;
+    for (int j = tid; j < nF; j += kThreads) {
+        int fid = T.f_id[f0 + j];
+        int lr = T.f_lr[f0 + j];
+        int il = lr & 0xffff, ir = lr >> 16;
+        double q0[4], q1[4], Lf[4], Rf[4];
+        double g0x[4] = {0, 0, 0, 0}, g0y[4] = {0, 0, 0, 0}, g1x[4] = {0, 0, 0, 0}, g1y[4] = {0, 0, 0, 0};
+        ld4(ps[il], q0);
+        ld4(ps[ir], q1);
+        int hh = T.f_hs[f0 + j];
+        if (ORDER == 2) {
+            double2 gpl = hgp[hh & 0xffff];
+            ld4(gs[2 * il], g0x);
+            ld4(gs[2 * il + 1], g0y);
+#pragma unroll
+            for (int v = 0; v < 4; ++v) Lf[v] = q0[v] + gpl.x * g0x[v] + gpl.y * g0y[v];
+        } else {
+#pragma unroll
+            for (int v = 0; v < 4; ++v) Lf[v] = q0[v];
+        }
+        double nx, ny, len;
+        double4 bb = make_double4(0, 0, 1, 0);
+        if (fid >= 0) {
+            if (ORDER == 2) {
+                double2 gpr = hgp[hh >> 16];
+                ld4(gs[2 * ir], g1x);
+                ld4(gs[2 * ir + 1], g1y);
+#pragma unroll
+                for (int v = 0; v < 4; ++v) Rf[v] = q1[v] + gpr.x * g1x[v] + gpr.y * g1y[v];
+            } else {
+#pragma unroll
+                for (int v = 0; v < 4; ++v) Rf[v] = q1[v];
+            }
+            double4 nl = m.face_nl[fid];
+            nx = nl.x; ny = nl.y; len = nl.z;
+            if (NS) bb = m.face_bb[fid];
+        } else {
+            int g = -1 - fid;
+            ld4(ghost_face(L.ghosts.bc, L.ghosts.gn, L.ghosts.ml, L.phys_g, g, time, mk4(Lf),
+                           L.flags), Rf);
+            if (L.ghost_pface) L.ghost_pface[g] = Lf[3];
+            double4 gn = L.ghosts.gn[g];
+            nx = gn.z; ny = gn.w; len = L.ghosts.ml[g].z;
+            if (NS) bb = L.ghosts.bb[g];
+        }
+        double F[4];
+        face_flux<FLUX, NS>(P, nx, ny, len, Lf, Rf, q0, q1, g0x, g0y, g1x, g1y, bb, F, L.flags);
+        fs[j] = mk4(F);
+    }
+    __syncthreads();
+
+    // D: per-cell flux sum in side order, update
+    double r[4] = {0, 0, 0, 0};
+    double dconv = 1e150, dvisc = 1e150;
+    int bad = 0;
+    const bool rk = L.mode == 1;
+    for (int i = tid; i < nT; i += kThreads) {
+        int d = T.e_ref[e0 + i];
+        int h0 = m.hs_off[d], h1 = m.hs_off[d + 1];
+        double s[4] = {0.0, 0.0, 0.0, 0.0};
+        for (int h = h0; h < h1; ++h) {
+            int code = T.u_code[h];
+            double F[4];
+            ld4(fs[code >> 1], F);
+            if (code & 1) {
+#pragma unroll
+                for (int v = 0; v < 4; ++v) s[v] += -F[v];
+            } else {
+#pragma unroll
+                for (int v = 0; v < 4; ++v) s[v] += F[v];
+            }
+        }
+        double4 geo = m.cell_geo[d];
+        double ut[4];
+#pragma unroll
+        for (int v = 0; v < 4; ++v) ut[v] = (0.0 - s[v]) * geo.y;
+        if (L.u_t) L.u_t[d] = mk4(ut);
+        if (!rk && L.grad_out) {
+            L.grad_out[2 * d] = ORDER == 2 ? gs[2 * i] : make_double4(0, 0, 0, 0);
+            L.grad_out[2 * d + 1] = ORDER == 2 ? gs[2 * i + 1] : make_double4(0, 0, 0, 0);
+        }
+        if (rk) {
+            double c0[4], cn[4], pn[4];
+            ld4(L.cons0[d], c0);
+            double adt = L.rk * L.ctrl->dt;
+#pragma unroll
+            for (int v = 0; v < 4; ++v) cn[v] = c0[v] + adt * ut[v];
+            cons_prim(P.gam1, cn, pn);
+            L.prim_out[d] = mk4(pn);
+            if (L.last_stage) {
+                L.cons0[d] = mk4(cn);
+                double a, b;
+                if (!local_dt(P, L.sp, pn, geo, &a, &b)) bad = 1;
+                else {
+                    dconv = fmin(dconv, a);
+                    dvisc = fmin(dvisc, b);
+                }
+            }
+        }
+#pragma unroll
+        for (int v = 0; v < 4; ++v) r[v] += geo.x * ut[v] * ut[v];
+    }
+    if (L.res_partial) {
+        double out[4];
+        block_sum<4>(r, out);
+        if (tid == 0)
+#pragma unroll
+            for (int v = 0; v < 4; ++v) L.res_partial[4 * t + v] = out[v];
+    }
+    if (L.dt_partial) block_min2(dconv, dvisc, bad, &L.dt_partial[t], &L.dt_bad[t]);
+    if (rk && L.last_stage) {
+        // the CTA that finishes last closes the step
+        __shared__ int s_last;
+        __threadfence();
+        __syncthreads();
+        if (tid == 0) s_last = atomicAdd(L.ticket, 1u) == (unsigned)(T.n_tiles - 1);
+        __syncthreads();
+        if (s_last) {
+            __threadfence();
+            step_end_block(const_cast<Ctrl*>(L.ctrl), L.sp, L.res_partial, L.dt_partial, L.dt_bad,
+                           T.n_tiles, L.wall_ghost, L.wall_nl, L.ghost_pface);
+            if (tid == 0) *L.ticket = 0u;
+        }
+    }
+}
+
+// per-block minima of the convective and viscous time steps
+__global__ void __launch_bounds__(256) k_dt(DevMesh m, Phys P, const Ctrl* ctrl, StepParams sp,
+                                            const double4* __restrict__ prim,
+                                            double2* __restrict__ partial, int* bad_partial) {
+    int c = blockIdx.x * blockDim.x + threadIdx.x;
+    double dconv = 1e150, dvisc = 1e150;
+    int bad = 0;
+    if (c < m.N) {
+        double q[4];
+        ld4(prim[c], q);
+        if (!local_dt(P, sp, q, m.cell_geo[c], &dconv, &dvisc)) {
+            bad = 1;
+            dconv = dvisc = 1e150;
+        }
+    }
+    block_min2(dconv, dvisc, bad, &partial[blockIdx.x], &bad_partial[blockIdx.x]);
+}
+
+__device__ void reduce_min2(const double2* partial, const int* bad_partial, int nb, double* a_out,
+                            double* b_out, int* bad_out) {
+    __shared__ double sa[256], sb[256];
+    __shared__ int sbad[256];
+    int tid = threadIdx.x;
+    double a = 1e150, b = 1e150;
+    int bad = 0;
+    for (int i = tid; i < nb; i += blockDim.x) {
+        a = fmin(a, partial[i].x);
+        b = fmin(b, partial[i].y);
+        bad |= bad_partial[i];
+    }
+    sa[tid] = a; sb[tid] = b; sbad[tid] = bad;
+    __syncthreads();
+    for (int s = blockDim.x / 2; s > 0; s >>= 1) {
+        if (tid < s) {
+            sa[tid] = fmin(sa[tid], sa[tid + s]);
+            sb[tid] = fmin(sb[tid], sb[tid + s]);
+            sbad[tid] |= sbad[tid + s];
+        }
+        __syncthreads();
+    }
+    *a_out = sa[0];
+    *b_out = sb[0];
+    *bad_out = sbad[0];
+}
+
+// first step of a run: dt of the current state, whether the step runs
+__global__ void k_step_begin(Ctrl* ctrl, StepParams sp, const double2* __restrict__ partial,
+                             const int* __restrict__ bad_partial, int nb) {
+    double a, b;
+    int bad;
+    reduce_min2(partial, bad_partial, nb, &a, &b, &bad);
+    if (threadIdx.x != 0) return;
+    if (ctrl->done || ctrl->iter >= ctrl->stop_at) {
+        ctrl->active = 0;
+        return;
+    }
+    ctrl->active = 1;
+    finish_dt(ctrl, sp, a, b, bad);
 }
 
 // ------------------------------------------------------------ dispatchers
@@ -645,11 +639,6 @@ static void launch_flux(const StageLaunch& L, cudaStream_t st) {
 }
 
 void launch_stage(const StageLaunch& L, cudaStream_t st) {
-    if (L.mesh.B > 0) {
-        int nb = (L.mesh.B + 127) / 128;
-        if (L.ns) k_bnd<1><<<nb, 128, 0, st>>>(L);
-        else k_bnd<0><<<nb, 128, 0, st>>>(L);
-    }
 #define CCFD_FLUX_CASE(ID) \
     case ID: launch_flux<ID>(L, st); break;
     switch (L.flux_id) {
@@ -668,13 +657,6 @@ void launch_dt(const DevMesh& m, const Phys& P, const Ctrl* ctrl, const StepPara
 void launch_step_begin(Ctrl* ctrl, const StepParams& sp, const double2* partial,
                        const int* bad_partial, int nb, cudaStream_t st) {
     k_step_begin<<<1, 256, 0, st>>>(ctrl, sp, partial, bad_partial, nb);
-}
-
-void launch_step_end(Ctrl* ctrl, const StepParams& sp, const double* res_partial,
-                     const double2* dt_partial, const int* dt_bad, int nb, const int* wall_ghost,
-                     const double* wall_nl, const double* ghost_pface, cudaStream_t st) {
-    k_step_end<<<1, 256, 0, st>>>(ctrl, sp, res_partial, dt_partial, dt_bad, nb, wall_ghost,
-                                  wall_nl, ghost_pface);
 }
 
 }  // namespace ccfd

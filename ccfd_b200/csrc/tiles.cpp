@@ -130,45 +130,51 @@ void ccfd_build_tiles(const ccfd_mesh* m, const std::vector<int>& cperm, const s
             }
         }
         ts.hs_loc.push_back((int16_t)hs_local);
-        // interior faces touching tile cells, in first-encounter order
+        // faces touching tile cells in first-encounter order: interior
+        // faces first, then the tile's boundary faces
+        std::vector<int> bfaces;
         for (long d = d0; d < d1; ++d) {
             long c = cperm[d];
             for (long h = m->hs_offset[c]; h < m->hs_offset[c + 1]; ++h) {
-                if (m->hs_nb[h] < 0) continue;
                 long f = m->hs_face[h];
+                if (m->hs_nb[h] < 0) {
+                    bfaces.push_back((int)f);
+                    continue;
+                }
                 if (fmark[f] != t) {
                     fmark[f] = t;
                     faces.push_back((int)f);
                 }
             }
         }
-        std::vector<int> flocal_of;  // reference face -> local index (sparse via map)
+        const int nFi = (int)faces.size();
+        faces.insert(faces.end(), bfaces.begin(), bfaces.end());
+        const int blk = (int)ts.hs_loc.size() - (nG + 1);
         for (size_t j = 0; j < faces.size(); ++j) {
             long f = faces[j];
             long o = m->face_cells[2 * f], nbr = m->face_cells[2 * f + 1];
-            int il = loc[cinv[o]], ir = loc[cinv[nbr]];
-            // local half-side index = local start of the cell + position in
-            // its side list
-            int hl = ts.hs_loc[ts.hs_loc.size() - (nG + 1) + il] +
-                     (int)(m->face_hs[2 * f] - m->hs_offset[o]);
-            int hr = ts.hs_loc[ts.hs_loc.size() - (nG + 1) + ir] +
-                     (int)(m->face_hs[2 * f + 1] - m->hs_offset[nbr]);
-            ts.f_id.push_back(fdev[f]);
-            ts.f_lr.push_back(il | (ir << 16));
-            ts.f_hs.push_back(hl | (hr << 16));
-            fmark[f] = -3 - (int)j;  // remember the local index for the codes below
+            int il = loc[cinv[o]];
+            int hl = ts.hs_loc[blk + il] + (int)(m->face_hs[2 * f] - m->hs_offset[o]);
+            if ((int)j < nFi) {
+                int ir = loc[cinv[nbr]];
+                int hr = ts.hs_loc[blk + ir] + (int)(m->face_hs[2 * f + 1] - m->hs_offset[nbr]);
+                ts.f_id.push_back(fdev[f]);
+                ts.f_lr.push_back(il | (ir << 16));
+                ts.f_hs.push_back(hl | (hr << 16));
+            } else {
+                int g = (int)(-1 - nbr);
+                ts.f_id.push_back(-1 - g);
+                ts.f_lr.push_back(il | (gloc[g] << 16));
+                ts.f_hs.push_back(hl);
+            }
+            fmark[f] = -3 - (int)j;  // local index for the codes below
         }
         for (long d = d0; d < d1; ++d) {
             long c = cperm[d];
             long k = dh[d];
             for (long h = m->hs_offset[c]; h < m->hs_offset[c + 1]; ++h, ++k) {
-                long nb = m->hs_nb[h];
-                if (nb < 0) {
-                    ts.u_code[k] = (int)nb;  // -1 - ghost
-                } else {
-                    int j = -3 - fmark[m->hs_face[h]];
-                    ts.u_code[k] = 2 * j + (m->hs_sign[h] > 0 ? 0 : 1);
-                }
+                int j = -3 - fmark[m->hs_face[h]];
+                ts.u_code[k] = 2 * j + (m->hs_sign[h] > 0 ? 0 : 1);
             }
         }
         for (size_t j = 0; j < faces.size(); ++j) fmark[faces[j]] = t;

@@ -26,10 +26,11 @@ struct TileSet {
     std::vector<int16_t> hs_nbl; // per gradient-cell half-side: local E index of neighbour
     std::vector<int16_t> hs_loc; // per gradient cell: local start of its half-sides (nG + 1 per tile)
     std::vector<int> f_off;      // per tile offsets into the face arrays
-    std::vector<int> f_id;       // device id of an interior face
-    std::vector<int> f_lr;       // packed local grad-cell indices (owner | neighbour << 16)
+    std::vector<int> f_id;       // device id of an interior face, or -1-g for the boundary face of ghost g
+    std::vector<int> f_lr;       // packed local indices (owner | neighbour << 16); a boundary
+                                 // face's neighbour is the ghost's staged entry
     std::vector<int> f_hs;       // packed local half-side indices (owner | neighbour << 16)
-    std::vector<int> u_code;     // per tile cell half-side (device CSR order): local face * 2 + (neighbour ? 1 : 0), or -1-g
+    std::vector<int> u_code;     // per device half-side of a tile cell: 2 * local face + (neighbour ? 1 : 0)
     int max_e = 0, max_g = 0, max_hs = 0, max_f = 0;
 };
 
