@@ -78,6 +78,7 @@ static void drop_graphs(ccfd_ctx* ctx) {
 
 static void free_device(ccfd_ctx* ctx) {
     drop_graphs(ctx);
+    ccfd_implicit_free(ctx);
     for (void* p : ctx->allocs) cudaFree(p);
     ctx->allocs.clear();
     ctx->device_bytes = 0;
@@ -423,6 +424,10 @@ extern "C" int ccfd_upload_case(ccfd_ctx* ctx, const ccfd_mesh* m, const ccfd_bc
         sp.sin_a = sin(a);
     }
     sp.total_area_q = m->total_area_q;
+    if (p.implicit && (st = ccfd_implicit_setup(ctx, hs_off, hs_nb))) {
+        free_device(ctx);
+        return st;
+    }
     ctx->uploaded = true;
     return CCFD_OK;
 }
@@ -530,6 +535,20 @@ int ccfd_residual_device(ccfd_ctx* ctx, double time) {
     L.prim_in = cur_prim(ctx);
     L.u_t = ctx->u_t;
     L.grad_out = ctx->params.spatial_order == 2 ? ctx->grad : nullptr;
+    L.res_partial = ctx->res_partial;
+    launch_stage(L, ctx->stream);
+    CK(cudaGetLastError());
+    return CCFD_OK;
+}
+
+int ccfd_residual_of(ccfd_ctx* ctx, const double4* prim, double time, double4* ut) {
+    StageLaunch L;
+    fill_stage(ctx, L);
+    L.ctrl = nullptr;
+    L.tfix = time;
+    L.mode = 0;
+    L.prim_in = prim;
+    L.u_t = ut;
     L.res_partial = ctx->res_partial;
     launch_stage(L, ctx->stream);
     CK(cudaGetLastError());

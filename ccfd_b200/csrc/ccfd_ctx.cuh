@@ -64,3 +64,9 @@ struct ccfd_ctx {
 
 // device-side residual of the current state into ctx->u_t (abi.cu)
 int ccfd_residual_device(ccfd_ctx* ctx, double time);
+// residual of an arbitrary primitive state into ut (abi.cu)
+int ccfd_residual_of(ccfd_ctx* ctx, const double4* prim, double time, double4* ut);
+// implicit solver set-up / release (implicit.cu); the device buffers are
+// owned by the context's allocation list
+int ccfd_implicit_setup(ccfd_ctx* ctx, const std::vector<int>& hs_off, const std::vector<int>& hs_nb);
+void ccfd_implicit_free(ccfd_ctx* ctx);

@@ -270,7 +270,7 @@ __device__ __forceinline__ void finish_dt(Ctrl* ctrl, const StepParams& sp, doub
 // reduction of the per-tile partials), wing coefficients, t += dt, the stop
 // tests of timeDisc (src/timeDiscretization.c:609-731) and the next dt.
 __device__ __forceinline__ void step_end_block(Ctrl* ctrl, const StepParams& sp, const double* res_partial,
-                               const double2* dt_partial, const int* dt_bad, int nb,
+                               int nres, const double2* dt_partial, const int* dt_bad, int ndt,
                                const int* wall_ghost, const double* wall_nl,
                                const double* ghost_pface) {
     __shared__ double s_res[4];
@@ -280,9 +280,10 @@ __device__ __forceinline__ void step_end_block(Ctrl* ctrl, const StepParams& sp,
     double r[4] = {0.0, 0.0, 0.0, 0.0};
     double a = 1e150, b = 1e150;
     int bad = 0;
-    for (int i = tid; i < nb; i += blockDim.x) {
+    for (int i = tid; i < nres; i += blockDim.x)
 #pragma unroll
         for (int v = 0; v < 4; ++v) r[v] += __ldcg(&res_partial[4 * i + v]);
+    for (int i = tid; i < ndt; i += blockDim.x) {
         double2 d = __ldcg(&dt_partial[i]);
         a = fmin(a, d.x);
         b = fmin(b, d.y);
@@ -548,8 +549,8 @@ __global__ void __launch_bounds__(kThreads, CCFD_STAGE_MIN_BLOCKS) k_stage(Stage
         __syncthreads();
         if (s_last) {
             __threadfence();
-            step_end_block(const_cast<Ctrl*>(L.ctrl), L.sp, L.res_partial, L.dt_partial, L.dt_bad,
-                           T.n_tiles, L.wall_ghost, L.wall_nl, L.ghost_pface);
+            step_end_block(const_cast<Ctrl*>(L.ctrl), L.sp, L.res_partial, T.n_tiles, L.dt_partial,
+                           L.dt_bad, T.n_tiles, L.wall_ghost, L.wall_nl, L.ghost_pface);
             if (tid == 0) *L.ticket = 0u;
         }
     }
@@ -613,6 +614,24 @@ __global__ void k_step_begin(Ctrl* ctrl, StepParams sp, const double2* __restric
     }
     ctrl->active = 1;
     finish_dt(ctrl, sp, a, b, bad);
+}
+
+// end of an implicit step (the residual partials come from the last
+// residual evaluation, the dt partials from k_dt of the new state)
+__global__ void k_step_end_sep(Ctrl* ctrl, StepParams sp, const double* res_partial, int nres,
+                               const double2* dt_partial, const int* dt_bad, int ndt,
+                               const int* wall_ghost, const double* wall_nl,
+                               const double* ghost_pface) {
+    if (!ctrl->active) return;
+    step_end_block(ctrl, sp, res_partial, nres, dt_partial, dt_bad, ndt, wall_ghost, wall_nl,
+                   ghost_pface);
+}
+
+void imp_step_end_launch(Ctrl* ctrl, const StepParams& sp, const double* res_partial, int nres,
+                         const double2* dt_partial, const int* dt_bad, int ndt, const int* wall_ghost,
+                         const double* wall_nl, const double* ghost_pface, cudaStream_t st) {
+    k_step_end_sep<<<1, 256, 0, st>>>(ctrl, sp, res_partial, nres, dt_partial, dt_bad, ndt, wall_ghost,
+                                      wall_nl, ghost_pface);
 }
 
 // ------------------------------------------------------------ dispatchers

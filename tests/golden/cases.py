@@ -129,6 +129,23 @@ def run_cases() -> dict:
     }
 
 
+def implicit_cases() -> dict:
+    """Short implicit runs on a small NACA 0012 O-grid (32 x 12 quads), where
+    the reference's dense Jacobian ((4N)^2 doubles) is still affordable."""
+    def ini(ns=False, precond=True, cfl=20.0, kdim=10, steps=4):
+        s = meshgen.airfoil_ini("naca", mach=0.5, alpha=2.0, navier_stokes=ns, reynolds=500.0,
+                                flux=2, implicit=True, precond=precond, n_kdim=kdim, cfl=cfl,
+                                max_iter=steps)
+        return s
+    return {
+        "naca_euler_imp_pc": {"mesh": ("naca", 32, 12, 101), "ini": ini(), "eqn": "euler", "steps": 4},
+        "naca_euler_imp_nopc": {"mesh": ("naca", 32, 12, 101), "ini": ini(precond=False, kdim=20),
+                                "eqn": "euler", "steps": 4},
+        "naca_ns_imp_pc": {"mesh": ("naca", 32, 12), "ini": ini(ns=True, cfl=10.0), "eqn": "navierstokes",
+                           "steps": 3},
+    }
+
+
 def make_mesh(spec):
     kind = spec["mesh"]
     if kind is None:
@@ -136,7 +153,9 @@ def make_mesh(spec):
     if kind[0] == "dmr":
         return "dmr", meshgen.dmr_mesh(kind[1], kind[2])
     if kind[0] == "naca":
-        return "naca", meshgen.naca_ogrid(0.0, 0.0, 0.12, kind[1], kind[2], r_far=5.0, h0=1e-2)
+        wall = kind[3] if len(kind) > 3 else 201
+        return "naca", meshgen.naca_ogrid(0.0, 0.0, 0.12, kind[1], kind[2], r_far=5.0, h0=1e-2,
+                                          wall_code=wall)
     raise ValueError(kind)
 
 

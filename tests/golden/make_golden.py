@@ -67,6 +67,13 @@ def ref_small() -> dict:
             arrays[f"{key}/pvar"] = d["pvar"]
             arrays[f"{key}/info"] = d["run_info"]
             arrays[f"{key}/history"] = d["history"]
+        for key, spec in CASES.implicit_cases().items():
+            ini, files = CASES.materialise(spec, tmp)
+            d = refdump.run_ref(ini, "coef", spec["steps"], eqn=spec["eqn"], files=files)
+            arrays[f"{key}/pvar"] = d["pvar"]
+            arrays[f"{key}/info"] = d["run_info"]
+            arrays[f"{key}/history"] = d["history"]
+            arrays[f"{key}/clcd"] = d["clcd"]
     return arrays
 
 

@@ -1,0 +1,38 @@
+"""Implicit path (Newton / matrix-free GMRES / LU-SGS) against the compiled
+reference on a small NACA 0012 O-grid, where the reference's dense Jacobian
+is affordable.  Tolerance: 1e-8 relative on the state and on CL / CD after
+the same number of implicit steps (the Krylov, Jacobian and 4x4-inverse
+arithmetic is reordered, so the iterates agree to rounding, not bitwise)."""
+import tempfile
+
+import numpy as np
+import pytest
+
+import ccfd_b200 as cc
+from tests.golden import cases as CASES
+
+pytestmark = pytest.mark.gpu
+
+TOL = 1e-8
+
+
+@pytest.mark.parametrize("key", sorted(CASES.implicit_cases()))
+def test_implicit_steps_match_reference(ref_small, key):
+    spec = CASES.implicit_cases()[key]
+    with tempfile.TemporaryDirectory() as tmp:
+        case, _, _ = CASES.load_case(spec, tmp)
+        s = cc.Solver(case, reorder=True)
+        rep = s.run(spec["steps"])
+        prim = s.get_state()
+        s.close()
+    ref = ref_small[f"{key}/pvar"].reshape(-1, 4)
+    info = ref_small[f"{key}/info"]
+    clcd = ref_small[f"{key}/clcd"]
+    assert rep["iterations"] == int(info[1])
+    assert rep["newton_iterations"] == int(info[5])
+    assert rep["gmres_iterations"] == int(info[6])
+    err = np.abs(prim - ref).max(axis=0) / np.abs(ref).max(axis=0)
+    assert err.max() <= TOL, err
+    assert abs(rep["cl"] - clcd[0]) <= TOL and abs(rep["cd"] - clcd[1]) <= TOL
+    hist = ref_small[f"{key}/history"].reshape(-1, 8)
+    np.testing.assert_allclose(rep["residual"][:4], hist[-1, 2:6], rtol=1e-6)
