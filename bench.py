@@ -97,16 +97,23 @@ class ClockSampler:
 
 
 def algorithmic_bytes_per_stage(m: dict, venk: bool) -> int:
-    """Compulsory HBM traffic of one residual evaluation + RK stage update of
-    the two-pass (gradient -> face) scheme, each array touched once: per cell
-    primitive state read by both passes (2 x 32 B), 1/area (8), limited
-    gradients written and read (2 x 64), stage-start conservative state read
-    (32), updated primitive state written (32), Venkatakrishnan eps^2 (8); per
-    half-side neighbour index (4), least-squares weights (16), face-midpoint
-    offset (16); per face two cell indices (8), normal (16), length (8)."""
+    """Compulsory HBM traffic of one residual evaluation + RK stage of the
+    fused scheme (gradients and face fluxes never leave the chip), each array
+    touched once: per cell the primitive state read (32 B) and written (32),
+    the stage-start conservative state read (32), 1/area (8) and, with the
+    Venkatakrishnan limiter, eps^2 (8); per half-side the neighbour index
+    (4), the face / sign code of the flux sum (4), the least-squares weights
+    (16) and the face-midpoint offset (16); per face the normal (16), the
+    length (8) and the two cell indices (8)."""
     n, h, f = m["n_cells"], m["n_half_sides"], m["n_faces"]
-    per_cell = 32 + 32 + 8 + 128 + 32 + 32 + (8 if venk else 0)
-    return n * per_cell + h * (4 + 16 + 16) + f * (8 + 16 + 8)
+    per_cell = 32 + 32 + 32 + 8 + (8 if venk else 0)
+    return n * per_cell + h * (4 + 4 + 16 + 16) + f * (16 + 8 + 8)
+
+
+# DRAM bytes per launch of the stage kernel on this workload, from the ncu
+# capture summarised in profiles/k_stage_dmr500k_hllc_vk_fp64.md
+# (dram__bytes_read.sum + dram__bytes_write.sum)
+STAGE_TRAFFIC_BYTES = 151.7e6 + 13.0e6
 
 
 def make_case(tmpdir: str):
@@ -285,14 +292,15 @@ def main() -> int:
                 "l2": "inputs larger than L2 (working set > 126 MB), no flush",
             },
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm_peak,
-                         "unit": "GB/s", "frac": achieved / hbm_peak, "traffic": None,
-                         "kernel": "residual evaluation + RK stage (gradient/limiter, face flux, "
-                                   "update kernels)",
+                         "unit": "GB/s", "frac": achieved / hbm_peak,
+                         "traffic": STAGE_TRAFFIC_BYTES if (NX, NY) == (1000, 250) else None,
+                         "kernel": "k_stage: fused residual evaluation + RK stage (one CTA per "
+                                   "256-cell tile)",
                          "bytes_per_launch": bytes_stage, "avg_ms": avg_res_ms,
                          "peak_source": peak_src},
             "e2e": {"value": e2e_value, "unit": UNIT,
                     "h2d_bytes_per_step": 2 * n * 4 * 8, "d2h_bytes_per_step": n * 4 * 8},
-            "gpu_launches": int(steps_done * (2 + 3 * nrk + 1)),
+            "gpu_launches": int(steps_done * nrk + 2),
             "clocks": clk,
             "cpu_baseline": cpu,
         }
