@@ -14,6 +14,9 @@ LIB_PATH = os.path.join(_HERE, "lib", "libccfd_b200.so")
 c_int, c_long, c_double = C.c_int, C.c_long, C.c_double
 P = C.POINTER
 
+CCFD_OK, CCFD_ERR_ARG = 0, 1
+NOALLOC_MAX_CELLS = 1 << 20  # CCFD_NOALLOC_MAX_CELLS
+
 
 class Params(C.Structure):
     _fields_ = [
@@ -107,6 +110,8 @@ def _load():
         "ccfd_clcd": (c_int, [C.c_void_p, P(c_double), P(c_double)]),
         "ccfd_set_profiling": (c_int, [C.c_void_p, c_int]),
         "ccfd_get_profile": (c_int, [C.c_void_p, P(c_double), P(c_long), c_int]),
+        "ccfd_global_residual_noalloc": (c_int, [C.c_void_p, C.c_void_p, c_long, c_double,
+                                                 C.c_void_p, C.c_void_p]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)

@@ -280,6 +280,26 @@ int ccfd_get_profile(ccfd_ctx *ctx, double *residual_ms, long *residual_count,
 		     int reset);
 /* Drop-in for globalResidual on the last residual (src/analyze.c:521-539). */
 int ccfd_global_residual(ccfd_ctx *ctx, double res[4]);
+
+/* Largest cell count of ccfd_global_residual_noalloc (its static scratch
+ * holds one 4-double partial sum per 256 cells: 128 KB). */
+#define CCFD_NOALLOC_MAX_CELLS (1L << 20)
+/* Allocation-free global residual, for callers that cannot allocate device
+ * memory (a host application whose own pool allocator owns the device heap,
+ * or a serving loop whose device-memory budget is already committed to
+ * resident states).  No counterpart in the reference.  Inputs and output are
+ * device memory owned by the caller: u_t [n_cells][4] (residual field), area
+ * [n_cells] (cell areas), res [4] receives sqrt(sum(area * u_t^2) *
+ * total_area_q) per variable.  stream is a cudaStream_t (NULL: legacy default
+ * stream); the result is ready when the stream is.  Allocates nothing: the
+ * partial sums live in a file-scope device array that every device loading
+ * the library keeps until exit.  The first call on a device looks up that
+ * array's device address (cudaGetSymbolAddress, with the device current), so
+ * make the first call on each device before any stream capture.  All calls
+ * share the array: calls that overlap on the GPU race.  Returns CCFD_ERR_ARG
+ * for n_cells <= 0 or n_cells > CCFD_NOALLOC_MAX_CELLS. */
+int ccfd_global_residual_noalloc(const double *u_t, const double *area, long n_cells,
+				 double total_area_q, double *res, void *stream);
 /* Lift / drag of the wall with BC code params.wall_id: the sums of calcCoef
  * (src/analyze.c:292-387) over the reconstructed wall-face pressures of the
  * last residual, with q_inf from exact.ref_state[0] and exact.alpha. */
