@@ -116,13 +116,42 @@ def algorithmic_bytes_per_stage(m: dict, venk: bool) -> int:
 STAGE_TRAFFIC_BYTES = 151.7e6 + 13.0e6
 
 
-def make_case(tmpdir: str):
+def make_case(tmpdir: str, precision: int = 0):
     import ccfd_b200 as cc
     from ccfd_b200 import meshgen
     path = os.path.join(tmpdir, "dmr.msh")
-    meshgen.dmr_mesh(NX, NY).write_gmsh(path)
-    ini = meshgen.dmr_ini("dmr")
+    if not os.path.exists(path):
+        meshgen.dmr_mesh(NX, NY).write_gmsh(path)
+    ini = meshgen.dmr_ini("dmr", precision=precision)
     return cc.CaseData.from_text(ini, tmpdir), ini, path
+
+
+def run_mixed(tmpdir: str, steps: int, warmup: int, prim_fp64, nrk: int, bytes_stage: int):
+    """The same workload with FP32 reconstruction / face fluxes and FP64
+    accumulation and state: throughput, stage-kernel time and the state's
+    deviation from the FP64 run after the same steps."""
+    import ccfd_b200 as cc
+    case, _, _ = make_case(tmpdir, precision=1)
+    n = case.n_cells
+    s = cc.Solver(case, reorder=True)
+    s.set_profiling(True)
+    s.run(warmup)
+    s.profile(reset=True)
+    rep = s.run(steps)
+    res_ms, res_cnt = s.profile(reset=True)
+    s.set_profiling(False)
+    prim = s.get_state()
+    s.close()
+    done = rep["iterations"] - warmup
+    avg = res_ms / max(res_cnt, 1)
+    scale = np.abs(prim_fp64).max(axis=0)
+    d = np.abs(prim - prim_fp64) / scale
+    return {"value": n * nrk * done / (rep["device_ms"] / 1e3), "unit": UNIT,
+            "ms_per_step": rep["device_ms"] / max(done, 1), "dtype": "f32 flux / f64 accumulation",
+            "stage_avg_ms": avg, "stage_achieved_gbs": bytes_stage / (avg / 1e3) / 1e9,
+            "state_vs_fp64": {"l1": float(d.mean()), "linf": float(d.max()),
+                              "after_steps": int(rep["iterations"]),
+                              "norm": "per variable, relative to max|U_fp64|"}}
 
 
 def cpu_reference_sample(ini: str, mesh_path: str, steps: int, threads: int):
@@ -181,6 +210,7 @@ def main() -> int:
     ap.add_argument("--e2e-steps", type=int, default=20)
     ap.add_argument("--cpu-steps", type=int, default=3)
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
+    ap.add_argument("--no-mixed", action="store_true", help="skip the mixed-precision run")
     ap.add_argument("--nx", type=int, default=NX)
     ap.add_argument("--ny", type=int, default=NY)
     args = ap.parse_args()
@@ -226,6 +256,7 @@ def main() -> int:
             dist.barrier()
         clk = clocks.stop()
         res_ms, res_cnt = s.profile(reset=True)
+        prim_fp64 = s.get_state()
         t_ms = torch.tensor([rep["device_ms"]], device="cuda", dtype=torch.float64)
         if dist is not None:
             dist.all_reduce(t_ms, op=dist.ReduceOp.MAX)
@@ -253,6 +284,9 @@ def main() -> int:
         s.close()
 
         bytes_stage = algorithmic_bytes_per_stage(m, venk=True)
+        mixed = None
+        if not args.no_mixed:
+            mixed = run_mixed(tmp, args.steps, args.warmup, prim_fp64, nrk, bytes_stage)
         avg_res_ms = res_ms / max(res_cnt, 1)
         achieved = bytes_stage / (avg_res_ms / 1e3) / 1e9
 
@@ -303,6 +337,7 @@ def main() -> int:
             "gpu_launches": int(steps_done * nrk + 2),
             "clocks": clk,
             "cpu_baseline": cpu,
+            "mixed_precision": mixed,
         }
         print(json.dumps(line), flush=True)
     if dist is not None:

@@ -302,7 +302,7 @@ extern "C" int ccfd_upload_case(ccfd_ctx* ctx, const ccfd_mesh* m, const ccfd_bc
     td.max_g = ts.max_g;
     td.max_hs = ts.max_hs;
     td.max_f = ts.max_f;
-    td.smem_bytes = 32 * ts.max_e + 64 * ts.max_g + 16 * (ts.max_hs + (ts.max_hs & 1)) + 32 * ts.max_f;
+    td.smem_bytes = stage_smem_bytes(td, 0);  // FP64 staging: the larger of the two layouts
     int smem_max = 0;
     CK(cudaDeviceGetAttribute(&smem_max, cudaDevAttrMaxSharedMemoryPerBlockOptin, ctx->device));
     if (td.smem_bytes > smem_max) {
@@ -444,6 +444,10 @@ static void fill_stage(ccfd_ctx* ctx, StageLaunch& L) {
     L.limiter = ctx->params.limiter;
     L.flux_id = ctx->params.flux;
     L.ns = ctx->params.eqn == CCFD_NAVIER_STOKES;
+    // mixed precision: FP32 face fluxes in the explicit scheme; the implicit
+    // scheme keeps FP64 residuals (its finite-difference Jacobian-vector
+    // products divide residual differences by a tiny perturbation)
+    L.fp32 = ctx->params.precision == CCFD_MIXED && !ctx->params.implicit;
     L.ghost_pface = ctx->ghost_pface;
     L.flags = ctx->flags;
     L.ticket = ctx->ticket;

@@ -46,6 +46,7 @@ struct StageLaunch {
     double tfix;           // time when ctrl == nullptr
     double a_time;         // stage time = t + a_time * dt
     int order, limiter, flux_id, ns;
+    int fp32;              // 1: FP32 reconstruction and face fluxes (mixed precision)
     int mode;              // 0: residual u_t only; 1: RK stage
     const double4* prim_in;
     double4* prim_out;     // RK: updated primitive state
@@ -65,6 +66,7 @@ struct StageLaunch {
 };
 
 void launch_stage(const StageLaunch& L, cudaStream_t st);
+int stage_smem_bytes(const TileDev& T, int fp32);
 void launch_dt(const DevMesh& m, const Phys& P, const Ctrl* ctrl, const StepParams& sp,
                const double4* prim, double2* partial, int* bad_partial, cudaStream_t st);
 void launch_step_begin(Ctrl* ctrl, const StepParams& sp, const double2* partial,

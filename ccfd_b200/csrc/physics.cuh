@@ -786,20 +786,21 @@ __device__ __forceinline__ void convective_flux(const Phys& P, const FluxIn<T>& 
 
 // diffusionFlux, src/fluxCalculation.c:855-873 (state: mean primitive state,
 // gx / gy: face gradients of the primitive variables); f[0] = g[0] = 0
-__device__ __forceinline__ void diffusion_flux(const Phys& P, const double st[4],
-                                               const double gx[4], const double gy[4],
-                                               double f[4], double g[4]) {
-    const double mu = P.mu;
-    f[0] = 0.0;
-    f[1] = (4.0 / 3.0 * gx[1] - 2.0 / 3.0 * gy[2]) * mu;
+template <typename T>
+__device__ __forceinline__ void diffusion_flux(const Phys& P, const T st[4], const T gx[4],
+                                               const T gy[4], T f[4], T g[4]) {
+    const T mu = T(P.mu), c43 = T(4.0 / 3.0), c23 = T(2.0 / 3.0);
+    const T gam = T(P.gam), gam1 = T(P.gam1), Pr = T(P.Pr);
+    f[0] = T(0.0);
+    f[1] = (c43 * gx[1] - c23 * gy[2]) * mu;
     f[2] = (gy[1] + gx[2]) * mu;
-    f[3] = (4.0 / 3.0 * st[1] * gx[1] - 2.0 / 3.0 * st[1] * gy[2] + (gx[2] + gy[1]) * st[2] +
-            P.gam / (P.gam1 * P.Pr * st[0] * st[0]) * (st[0] * gx[3] - st[3] * gx[0])) * mu;
-    g[0] = 0.0;
+    f[3] = (c43 * st[1] * gx[1] - c23 * st[1] * gy[2] + (gx[2] + gy[1]) * st[2] +
+            gam / (gam1 * Pr * st[0] * st[0]) * (st[0] * gx[3] - st[3] * gx[0])) * mu;
+    g[0] = T(0.0);
     g[1] = (gy[1] + gx[2]) * mu;
-    g[2] = (4.0 / 3.0 * gy[2] - 2.0 / 3.0 * gx[1]) * mu;
-    g[3] = (4.0 / 3.0 * st[2] * gy[2] - 2.0 / 3.0 * st[2] * gx[1] + (gy[1] + gx[2]) * st[1] +
-            P.gam / (P.gam1 * P.Pr * st[0] * st[0]) * (st[0] * gy[3] - st[3] * gy[0])) * mu;
+    g[2] = (c43 * gy[2] - c23 * gx[1]) * mu;
+    g[3] = (c43 * st[2] * gy[2] - c23 * st[2] * gx[1] + (gy[1] + gx[2]) * st[1] +
+            gam / (gam1 * Pr * st[0] * st[0]) * (st[0] * gy[3] - st[3] * gy[0])) * mu;
 }
 
 }  // namespace ccfd

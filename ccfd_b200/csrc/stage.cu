@@ -41,60 +41,88 @@ __device__ __forceinline__ bool inactive(const Ctrl* ctrl) { return ctrl && !ctr
 __device__ __forceinline__ void ld4(const double4& v, double q[4]) {
     q[0] = v.x; q[1] = v.y; q[2] = v.z; q[3] = v.w;
 }
-
+__device__ __forceinline__ void ld4(const float4& v, float q[4]) {
+    q[0] = v.x; q[1] = v.y; q[2] = v.z; q[3] = v.w;
+}
 __device__ __forceinline__ double4 mk4(const double q[4]) {
     return make_double4(q[0], q[1], q[2], q[3]);
+}
+__device__ __forceinline__ float4 mk4(const float q[4]) {
+    return make_float4(q[0], q[1], q[2], q[3]);
+}
+
+// shared-memory vector types of the stage kernel: FP64 throughout, or FP32
+// reconstruction and face fluxes (mixed precision; state, residual sums and
+// the update stay FP64)
+template <typename T> struct Vec;
+template <> struct Vec<double> { using v4 = double4; using v2 = double2; };
+template <> struct Vec<float> { using v4 = float4; using v2 = float2; };
+
+template <typename T>
+__device__ __forceinline__ typename Vec<T>::v4 cvt4(const double4& v) {
+    if constexpr (sizeof(T) == 8) return v;
+    else return make_float4(float(v.x), float(v.y), float(v.z), float(v.w));
+}
+template <typename T>
+__device__ __forceinline__ typename Vec<T>::v2 cvt2(double a, double b) {
+    if constexpr (sizeof(T) == 8) return make_double2(a, b);
+    else return make_float2(float(a), float(b));
+}
+__device__ __forceinline__ double4 to_d4(const double4& v) { return v; }
+__device__ __forceinline__ double4 to_d4(const float4& v) {
+    return make_double4(v.x, v.y, v.z, v.w);
 }
 
 // Limited least-squares gradient of one cell (src/reconstruction.c:25-192,
 // 252-312).  nbr(k, qn) fetches the k-th neighbour state in side order,
 // gw(k) the side's (GP.x, GP.y, w.x, w.y).
-template <class Nbr, class GW>
-__device__ __forceinline__ void cell_gradient(int limiter, const double q[4], int nh, double eps2,
-                                              Nbr nbr, GW gw, double ux[4], double uy[4]) {
-    double umin[4] = {q[0], q[1], q[2], q[3]}, umax[4] = {q[0], q[1], q[2], q[3]};
-    double gpx[4] = {0, 0, 0, 0}, gpy[4] = {0, 0, 0, 0};
+template <typename T, class Nbr, class GW>
+__device__ __forceinline__ void cell_gradient(int limiter, const T q[4], int nh, T eps2, Nbr nbr,
+                                              GW gw, T ux[4], T uy[4]) {
+    T umin[4] = {q[0], q[1], q[2], q[3]}, umax[4] = {q[0], q[1], q[2], q[3]};
+    T gpx[4] = {0, 0, 0, 0}, gpy[4] = {0, 0, 0, 0};
 #pragma unroll
-    for (int v = 0; v < 4; ++v) ux[v] = uy[v] = 0.0;
+    for (int v = 0; v < 4; ++v) ux[v] = uy[v] = T(0.0);
 #pragma unroll
     for (int k = 0; k < 4; ++k) {
         if (k < nh) {
             double4 g = gw(k);
-            gpx[k] = g.x;
-            gpy[k] = g.y;
-            double qn[4];
+            gpx[k] = T(g.x);
+            gpy[k] = T(g.y);
+            const T wx = T(g.z), wy = T(g.w);
+            T qn[4];
             nbr(k, qn);
 #pragma unroll
             for (int v = 0; v < 4; ++v) {
-                double d = qn[v] - q[v];
-                ux[v] += g.z * d;
-                uy[v] += g.w * d;
+                T d = qn[v] - q[v];
+                ux[v] += wx * d;
+                uy[v] += wy * d;
                 umin[v] = fmin(umin[v], qn[v]);
                 umax[v] = fmax(umax[v], qn[v]);
             }
         }
     }
-    double phi[4] = {1.0, 1.0, 1.0, 1.0};
+    T phi[4] = {T(1.0), T(1.0), T(1.0), T(1.0)};
 #pragma unroll
     for (int v = 0; v < 4; ++v) {
-        double mn = umin[v] - q[v], mx = umax[v] - q[v];
-        double mn2 = mn * mn, mx2 = mx * mx;
+        T mn = umin[v] - q[v], mx = umax[v] - q[v];
+        T mn2 = mn * mn, mx2 = mx * mx;
 #pragma unroll
         for (int k = 0; k < 4; ++k) {
             if (k < nh) {
-                double uD = ux[v] * gpx[k] + uy[v] * gpy[k];
-                double pl = 1.0;
+                T uD = ux[v] * gpx[k] + uy[v] * gpy[k];
+                T pl = T(1.0);
                 if (limiter == 1) {
-                    if (uD > 0.0) pl = fmin(1.0, mx / uD);
-                    else if (uD < 0.0) pl = fmin(1.0, mn / uD);
+                    if (uD > T(0.0)) pl = fmin(T(1.0), mx / uD);
+                    else if (uD < T(0.0)) pl = fmin(T(1.0), mn / uD);
                 } else {
-                    double uD2 = uD * uD;
-                    if (uD > 0.0)
-                        pl = 1.0 / uD * (((mx2 + eps2) * uD + 2.0 * uD2 * mx) /
-                                         (mx2 + 2.0 * uD2 + uD * mx + eps2));
-                    else if (uD < 0.0)
-                        pl = 1.0 / uD * (((mn2 + eps2) * uD + 2.0 * uD2 * mn) /
-                                         (mn2 + 2.0 * uD2 + uD * mn + eps2));
+                    T uD2 = uD * uD;
+                    if (uD > T(0.0))
+                        pl = T(1.0) / uD * (((mx2 + eps2) * uD + T(2.0) * uD2 * mx) /
+                                            (mx2 + T(2.0) * uD2 + uD * mx + eps2));
+                    else if (uD < T(0.0))
+                        pl = T(1.0) / uD * (((mn2 + eps2) * uD + T(2.0) * uD2 * mn) /
+                                            (mn2 + T(2.0) * uD2 + uD * mn + eps2));
                 }
                 phi[v] = fmin(phi[v], pl);
             }
@@ -111,36 +139,35 @@ __device__ __forceinline__ void cell_gradient(int limiter, const double q[4], in
 // and back, with the viscous contribution, scaled by the face length
 // (src/fluxCalculation.c:885-996).  q0 / q1 are the cell-centre states and
 // g0x..g1y the cell gradients (Navier-Stokes only).
-template <int FLUX, int NS>
-__device__ __forceinline__ void face_flux(const Phys& P, double nx, double ny, double len,
-                                          const double L[4], const double R[4], const double q0[4],
-                                          const double q1[4], const double g0x[4],
-                                          const double g0y[4], const double g1x[4],
-                                          const double g1y[4], double4 bb, double F[4],
-                                          unsigned* flags) {
-    FluxIn<double> s;
+template <int FLUX, int NS, typename T>
+__device__ __forceinline__ void face_flux(const Phys& P, T nx, T ny, T len, const T L[4], const T R[4],
+                                          const T q0[4], const T q1[4], const T g0x[4],
+                                          const T g0y[4], const T g1x[4], const T g1y[4], double4 bbd,
+                                          T F[4], unsigned* flags) {
+    FluxIn<T> s;
     s.rL = L[0]; s.uL = nx * L[1] + ny * L[2]; s.vL = -ny * L[1] + nx * L[2]; s.pL = L[3];
     s.rR = R[0]; s.uR = nx * R[1] + ny * R[2]; s.vR = -ny * R[1] + nx * R[2]; s.pR = R[3];
-    double fc[4];
-    convective_flux<FLUX, double>(P, s, fc, flags);
+    T fc[4];
+    convective_flux<FLUX, T>(P, s, fc, flags);
     F[0] = fc[0];
     F[1] = nx * fc[1] - ny * fc[2];
     F[2] = ny * fc[1] + nx * fc[2];
     F[3] = fc[3];
     if (NS) {
-        double st[4], gx[4], gy[4];
-        double bx = bb.x / bb.z, by = bb.y / bb.z;
+        T st[4], gx[4], gy[4];
+        const T bbz = T(bbd.z);
+        T bx = T(bbd.x) / bbz, by = T(bbd.y) / bbz;
 #pragma unroll
         for (int v = 0; v < 4; ++v) {
-            st[v] = 0.5 * (R[v] + L[v]);
-            double gxm = 0.5 * (g0x[v] + g1x[v]);
-            double gym = 0.5 * (g0y[v] + g1y[v]);
-            double corr = gxm * bx + gym * by - (q1[v] - q0[v]) / bb.z;
+            st[v] = T(0.5) * (R[v] + L[v]);
+            T gxm = T(0.5) * (g0x[v] + g1x[v]);
+            T gym = T(0.5) * (g0y[v] + g1y[v]);
+            T corr = gxm * bx + gym * by - (q1[v] - q0[v]) / bbz;
             gx[v] = gxm - corr * bx;
             gy[v] = gym - corr * by;
         }
-        double fdx[4], fdy[4];
-        diffusion_flux(P, st, gx, gy, fdx, fdy);
+        T fdx[4], fdy[4];
+        diffusion_flux<T>(P, st, gx, gy, fdx, fdy);
 #pragma unroll
         for (int v = 0; v < 4; ++v) F[v] -= (fdx[v] * nx + fdy[v] * ny);
     }
@@ -369,12 +396,15 @@ __device__ __forceinline__ void step_end_block(Ctrl* ctrl, const StepParams& sp,
     finish_dt(ctrl, sp, s_dt.x, s_dt.y, s_bad);
 }
 
-// fused residual evaluation (+ RK stage) of one tile per CTA
-template <int FLUX, int ORDER, int NS>
+// fused residual evaluation (+ RK stage) of one tile per CTA; FT is the
+// arithmetic type of the reconstruction and the face fluxes
+template <int FLUX, int ORDER, int NS, typename FT>
 #ifndef CCFD_STAGE_MIN_BLOCKS
 #define CCFD_STAGE_MIN_BLOCKS 3
 #endif
 __global__ void __launch_bounds__(kThreads, CCFD_STAGE_MIN_BLOCKS) k_stage(StageLaunch L) {
+    using V4 = typename Vec<FT>::v4;
+    using V2 = typename Vec<FT>::v2;
     extern __shared__ double4 smem[];
     if (inactive(L.ctrl)) return;
     const DevMesh& m = L.mesh;
@@ -385,24 +415,23 @@ __global__ void __launch_bounds__(kThreads, CCFD_STAGE_MIN_BLOCKS) k_stage(Stage
     const int nT = cnt.x, nG = cnt.y, nEc = cnt.z, nE = cnt.w;
     const int e0 = T.e_off[t];
     const double time = stage_time(L.ctrl, L.tfix, L.a_time);
-    double4* ps = smem;                                   // [max_e] states
-    double4* gs = ps + T.max_e;                           // [2 max_g] gradients
-    double2* hgp = reinterpret_cast<double2*>(gs + 2 * T.max_g);  // [max_hs] GP
-    double4* fs = reinterpret_cast<double4*>(hgp + T.max_hs + (T.max_hs & 1));  // [max_f]
+    V4* ps = reinterpret_cast<V4*>(smem);             // [max_e] states
+    V4* gs = ps + T.max_e;                            // [2 max_g] gradients
+    V2* hgp = reinterpret_cast<V2*>(gs + 2 * T.max_g);  // [max_hs] GP
+    V4* fs = reinterpret_cast<V4*>(hgp + T.max_hs + (T.max_hs & 1));  // [max_f]
 
     // A: stage the states of the tile and its rings; ghost cells get the
     // boundary state at their mirrored barycentre (second order only: the
     // reference sets ghost cell states in its second-order reconstruction
     // and leaves them zero otherwise)
-    for (int e = tid; e < nEc; e += kThreads) ps[e] = L.prim_in[T.e_ref[e0 + e]];
+    for (int e = tid; e < nEc; e += kThreads) ps[e] = cvt4<FT>(L.prim_in[T.e_ref[e0 + e]]);
     for (int e = nEc + tid; e < nE; e += kThreads) {
         int g = -1 - T.e_ref[e0 + e];
-        double gq[4] = {0.0, 0.0, 0.0, 0.0};
-        if (ORDER == 2) {
-            ld4(ghost_bary(L.ghosts.bc, L.ghosts.gn, L.phys_g, g, time,
-                           L.prim_in[L.ghosts.cell[g]], L.flags), gq);
-        }
-        ps[e] = mk4(gq);
+        double4 gq = make_double4(0.0, 0.0, 0.0, 0.0);
+        if (ORDER == 2)
+            gq = ghost_bary(L.ghosts.bc, L.ghosts.gn, L.phys_g, g, time, L.prim_in[L.ghosts.cell[g]],
+                            L.flags);
+        ps[e] = cvt4<FT>(gq);
     }
     __syncthreads();
 
@@ -413,16 +442,16 @@ __global__ void __launch_bounds__(kThreads, CCFD_STAGE_MIN_BLOCKS) k_stage(Stage
             int d = T.e_ref[e0 + i];
             int h0 = m.hs_off[d], nh = m.hs_off[d + 1] - h0;
             int lo = T.hs_loc[gb + i];
-            double q[4], ux[4], uy[4];
+            FT q[4], ux[4], uy[4];
             ld4(ps[i], q);
-            double eps2 = L.limiter == 2 ? m.venk_eps2[d] : 0.0;
-            auto nbr = [&](int k, double qn[4]) { ld4(ps[T.hs_nbl[hb + lo + k]], qn); };
+            FT eps2 = L.limiter == 2 ? FT(m.venk_eps2[d]) : FT(0.0);
+            auto nbr = [&](int k, FT qn[4]) { ld4(ps[T.hs_nbl[hb + lo + k]], qn); };
             auto gw = [&](int k) {
                 double4 g = m.hs_gw[h0 + k];
-                hgp[lo + k] = make_double2(g.x, g.y);
+                hgp[lo + k] = cvt2<FT>(g.x, g.y);
                 return g;
             };
-            cell_gradient(L.limiter, q, nh, eps2, nbr, gw, ux, uy);
+            cell_gradient<FT>(L.limiter, q, nh, eps2, nbr, gw, ux, uy);
             gs[2 * i] = mk4(ux);
             gs[2 * i + 1] = mk4(uy);
         }
@@ -435,13 +464,13 @@ __global__ void __launch_bounds__(kThreads, CCFD_STAGE_MIN_BLOCKS) k_stage(Stage
         int fid = T.f_id[f0 + j];
         int lr = T.f_lr[f0 + j];
         int il = lr & 0xffff, ir = lr >> 16;
-        double q0[4], q1[4], Lf[4], Rf[4];
-        double g0x[4] = {0, 0, 0, 0}, g0y[4] = {0, 0, 0, 0}, g1x[4] = {0, 0, 0, 0}, g1y[4] = {0, 0, 0, 0};
+        FT q0[4], q1[4], Lf[4], Rf[4];
+        FT g0x[4] = {0, 0, 0, 0}, g0y[4] = {0, 0, 0, 0}, g1x[4] = {0, 0, 0, 0}, g1y[4] = {0, 0, 0, 0};
         ld4(ps[il], q0);
         ld4(ps[ir], q1);
         int hh = T.f_hs[f0 + j];
         if (ORDER == 2) {
-            double2 gpl = hgp[hh & 0xffff];
+            V2 gpl = hgp[hh & 0xffff];
             ld4(gs[2 * il], g0x);
             ld4(gs[2 * il + 1], g0y);
 #pragma unroll
@@ -450,11 +479,11 @@ __global__ void __launch_bounds__(kThreads, CCFD_STAGE_MIN_BLOCKS) k_stage(Stage
 #pragma unroll
             for (int v = 0; v < 4; ++v) Lf[v] = q0[v];
         }
-        double nx, ny, len;
+        FT nx, ny, len;
         double4 bb = make_double4(0, 0, 1, 0);
         if (fid >= 0) {
             if (ORDER == 2) {
-                double2 gpr = hgp[hh >> 16];
+                V2 gpr = hgp[hh >> 16];
                 ld4(gs[2 * ir], g1x);
                 ld4(gs[2 * ir + 1], g1y);
 #pragma unroll
@@ -464,19 +493,20 @@ __global__ void __launch_bounds__(kThreads, CCFD_STAGE_MIN_BLOCKS) k_stage(Stage
                 for (int v = 0; v < 4; ++v) Rf[v] = q1[v];
             }
             double4 nl = m.face_nl[fid];
-            nx = nl.x; ny = nl.y; len = nl.z;
+            nx = FT(nl.x); ny = FT(nl.y); len = FT(nl.z);
             if (NS) bb = m.face_bb[fid];
         } else {
             int g = -1 - fid;
-            ld4(ghost_face(L.ghosts.bc, L.ghosts.gn, L.ghosts.ml, L.phys_g, g, time, mk4(Lf),
-                           L.flags), Rf);
-            if (L.ghost_pface) L.ghost_pface[g] = Lf[3];
+            double4 Rd = ghost_face(L.ghosts.bc, L.ghosts.gn, L.ghosts.ml, L.phys_g, g, time,
+                                    to_d4(mk4(Lf)), L.flags);
+            ld4(cvt4<FT>(Rd), Rf);
+            if (L.ghost_pface) L.ghost_pface[g] = double(Lf[3]);
             double4 gn = L.ghosts.gn[g];
-            nx = gn.z; ny = gn.w; len = L.ghosts.ml[g].z;
+            nx = FT(gn.z); ny = FT(gn.w); len = FT(L.ghosts.ml[g].z);
             if (NS) bb = L.ghosts.bb[g];
         }
-        double F[4];
-        face_flux<FLUX, NS>(P, nx, ny, len, Lf, Rf, q0, q1, g0x, g0y, g1x, g1y, bb, F, L.flags);
+        FT F[4];
+        face_flux<FLUX, NS, FT>(P, nx, ny, len, Lf, Rf, q0, q1, g0x, g0y, g1x, g1y, bb, F, L.flags);
         fs[j] = mk4(F);
     }
     __syncthreads();
@@ -492,14 +522,14 @@ __global__ void __launch_bounds__(kThreads, CCFD_STAGE_MIN_BLOCKS) k_stage(Stage
         double s[4] = {0.0, 0.0, 0.0, 0.0};
         for (int h = h0; h < h1; ++h) {
             int code = T.u_code[h];
-            double F[4];
+            FT F[4];
             ld4(fs[code >> 1], F);
             if (code & 1) {
 #pragma unroll
-                for (int v = 0; v < 4; ++v) s[v] += -F[v];
+                for (int v = 0; v < 4; ++v) s[v] += -double(F[v]);
             } else {
 #pragma unroll
-                for (int v = 0; v < 4; ++v) s[v] += F[v];
+                for (int v = 0; v < 4; ++v) s[v] += double(F[v]);
             }
         }
         double4 geo = m.cell_geo[d];
@@ -508,8 +538,8 @@ __global__ void __launch_bounds__(kThreads, CCFD_STAGE_MIN_BLOCKS) k_stage(Stage
         for (int v = 0; v < 4; ++v) ut[v] = (0.0 - s[v]) * geo.y;
         if (L.u_t) L.u_t[d] = mk4(ut);
         if (!rk && L.grad_out) {
-            L.grad_out[2 * d] = ORDER == 2 ? gs[2 * i] : make_double4(0, 0, 0, 0);
-            L.grad_out[2 * d + 1] = ORDER == 2 ? gs[2 * i + 1] : make_double4(0, 0, 0, 0);
+            L.grad_out[2 * d] = ORDER == 2 ? to_d4(gs[2 * i]) : make_double4(0, 0, 0, 0);
+            L.grad_out[2 * d + 1] = ORDER == 2 ? to_d4(gs[2 * i + 1]) : make_double4(0, 0, 0, 0);
         }
         if (rk) {
             double c0[4], cn[4], pn[4];
@@ -635,31 +665,47 @@ void imp_step_end_launch(Ctrl* ctrl, const StepParams& sp, const double* res_par
 }
 
 // ------------------------------------------------------------ dispatchers
-template <int FLUX, int ORDER, int NS>
-static void launch_k_stage(const StageLaunch& L, cudaStream_t st) {
-    auto kern = k_stage<FLUX, ORDER, NS>;
-    static int configured = 0;
-    if (configured < L.tiles.smem_bytes) {
-        cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, L.tiles.smem_bytes);
-        configured = L.tiles.smem_bytes;
-    }
-    kern<<<L.tiles.n_tiles, kThreads, L.tiles.smem_bytes, st>>>(L);
+template <typename FT>
+static int stage_smem_bytes(const TileDev& T) {
+    using V4 = typename Vec<FT>::v4;
+    using V2 = typename Vec<FT>::v2;
+    return (int)(sizeof(V4) * (T.max_e + 2 * T.max_g) + sizeof(V2) * (T.max_hs + (T.max_hs & 1)) +
+                 sizeof(V4) * T.max_f);
 }
 
-template <int FLUX>
+template <int FLUX, int ORDER, int NS, typename FT>
+static void launch_k_stage(const StageLaunch& L, cudaStream_t st) {
+    auto kern = k_stage<FLUX, ORDER, NS, FT>;
+    const int smem = stage_smem_bytes<FT>(L.tiles);
+    static int configured = 0;
+    if (configured < smem) {
+        cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+        configured = smem;
+    }
+    kern<<<L.tiles.n_tiles, kThreads, smem, st>>>(L);
+}
+
+template <int FLUX, typename FT>
 static void launch_flux(const StageLaunch& L, cudaStream_t st) {
     if (L.order == 2) {
-        if (L.ns) launch_k_stage<FLUX, 2, 1>(L, st);
-        else launch_k_stage<FLUX, 2, 0>(L, st);
+        if (L.ns) launch_k_stage<FLUX, 2, 1, FT>(L, st);
+        else launch_k_stage<FLUX, 2, 0, FT>(L, st);
     } else {
-        if (L.ns) launch_k_stage<FLUX, 1, 1>(L, st);
-        else launch_k_stage<FLUX, 1, 0>(L, st);
+        if (L.ns) launch_k_stage<FLUX, 1, 1, FT>(L, st);
+        else launch_k_stage<FLUX, 1, 0, FT>(L, st);
     }
+}
+
+int stage_smem_bytes(const TileDev& T, int fp32) {
+    return fp32 ? stage_smem_bytes<float>(T) : stage_smem_bytes<double>(T);
 }
 
 void launch_stage(const StageLaunch& L, cudaStream_t st) {
-#define CCFD_FLUX_CASE(ID) \
-    case ID: launch_flux<ID>(L, st); break;
+#define CCFD_FLUX_CASE(ID)                                  \
+    case ID:                                                \
+        if (L.fp32) launch_flux<ID, float>(L, st);          \
+        else launch_flux<ID, double>(L, st);                \
+        break;
     switch (L.flux_id) {
         CCFD_FLUX_CASE(1) CCFD_FLUX_CASE(2) CCFD_FLUX_CASE(3) CCFD_FLUX_CASE(4)
         CCFD_FLUX_CASE(5) CCFD_FLUX_CASE(6) CCFD_FLUX_CASE(7) CCFD_FLUX_CASE(8)
