@@ -23,7 +23,7 @@ import numpy as np
 
 from . import _native as N
 
-__all__ = ["CaseData", "Solver", "set_device", "CcfdError", "mesh_arrays", "PRIMITIVE", "CONSERVATIVE"]
+__all__ = ["CaseData", "Solver", "Batch", "Server", "estimate_device_bytes", "set_device", "CcfdError", "mesh_arrays", "PRIMITIVE", "CONSERVATIVE"]
 
 PRIMITIVE, CONSERVATIVE = N.PRIMITIVE, N.CONSERVATIVE
 
@@ -225,10 +225,124 @@ class Solver:
                "ccfd_get_profile")
         return ms.value, cnt.value
 
+    def device_bytes(self) -> int:
+        b = C.c_size_t()
+        _check(N.lib.ccfd_device_bytes(self._ctx, C.byref(b)), "ccfd_device_bytes")
+        return b.value
+
     def clcd(self):
         cl, cd = C.c_double(), C.c_double()
         _check(N.lib.ccfd_clcd(self._ctx, C.byref(cl), C.byref(cd)), "ccfd_clcd")
         return cl.value, cd.value
+
+
+class Batch:
+    """Many solvers stepped together on one device (see ccfd_batch_* in the
+    C header).  A solver in a batch is stepped only by the batch; its state
+    and report stay readable."""
+
+    def __init__(self, device: int = 0):
+        self._b = C.c_void_p()
+        _check(N.lib.ccfd_batch_create(int(device), C.byref(self._b)), "ccfd_batch_create")
+        self.members: list[Solver] = []
+
+    def add(self, solver: "Solver", nsteps: int = 0) -> None:
+        _check(N.lib.ccfd_batch_add(self._b, solver._ctx, int(nsteps)), "ccfd_batch_add")
+        self.members.append(solver)
+
+    def remove(self, solver: "Solver") -> None:
+        _check(N.lib.ccfd_batch_remove(self._b, solver._ctx), "ccfd_batch_remove")
+        self.members.remove(solver)
+
+    def step(self, steps: int = 1) -> int:
+        """Advance every running member by up to ``steps`` time steps;
+        returns how many members can still step."""
+        n = C.c_int()
+        _check(N.lib.ccfd_batch_step(self._b, int(steps), C.byref(n)), "ccfd_batch_step")
+        return n.value
+
+    def report(self, solver: "Solver") -> dict:
+        rep = N.Report()
+        _check(N.lib.ccfd_batch_report(self._b, solver._ctx, C.byref(rep)), "ccfd_batch_report")
+        return report_dict(rep)
+
+    def close(self) -> None:
+        if self._b:
+            N.lib.ccfd_batch_destroy(self._b)
+            self._b = C.c_void_p()
+            self.members = []
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Server:
+    """Request loop with continuous batching (see ccfd_server_* in the C
+    header): cases queue in arrival order, are admitted by a device-memory
+    budget, run together and are retired when they stop."""
+
+    def __init__(self, device: int = 0, hbm_budget_bytes: int = 150 * 10**9, max_running: int = 4096):
+        self._s = C.c_void_p()
+        _check(N.lib.ccfd_server_create(int(device), int(hbm_budget_bytes), int(max_running),
+                                        C.byref(self._s)), "ccfd_server_create")
+        self._cases: dict[int, CaseData] = {}
+
+    def submit(self, case: "CaseData", nsteps: int = 0) -> int:
+        rid = C.c_long()
+        _check(N.lib.ccfd_server_submit(self._s, case._ptr, int(nsteps), C.byref(rid)),
+               "ccfd_server_submit")
+        self._cases[rid.value] = case  # the server reads the case until it finishes
+        return rid.value
+
+    def poll(self, steps: int = 16) -> tuple[int, int, int]:
+        """(queued, running, finished-not-fetched) after one scheduling round."""
+        q, r, d = C.c_int(), C.c_int(), C.c_int()
+        _check(N.lib.ccfd_server_poll(self._s, int(steps), C.byref(q), C.byref(r), C.byref(d)),
+               "ccfd_server_poll")
+        return q.value, r.value, d.value
+
+    def result(self, rid: int, with_state: bool = True):
+        """(report, final primitive state or None, (t_submit, t_admit, t_done)),
+        or None while the request is queued or running."""
+        case = self._cases[rid]
+        rep = N.Report()
+        prim = np.empty((case.n_cells, 4)) if with_state else None
+        times = (C.c_double * 3)()
+        st = N.lib.ccfd_server_result(self._s, int(rid), C.byref(rep),
+                                      _dptr(prim) if with_state else None, times)
+        if st == 16:  # CCFD_ERR_BUSY
+            return None
+        del self._cases[rid]
+        out = report_dict(rep)
+        out["status"] = st
+        return out, prim, tuple(times)
+
+    def memory(self) -> tuple[int, int]:
+        used, budget = C.c_size_t(), C.c_size_t()
+        _check(N.lib.ccfd_server_memory(self._s, C.byref(used), C.byref(budget)), "ccfd_server_memory")
+        return used.value, budget.value
+
+    def close(self) -> None:
+        if self._s:
+            N.lib.ccfd_server_destroy(self._s)
+            self._s = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def estimate_device_bytes(case: "CaseData") -> int:
+    b = C.c_size_t()
+    c = case.c
+    _check(N.lib.ccfd_estimate_device_bytes(C.byref(c.params), C.byref(c.mesh), C.byref(b)),
+           "ccfd_estimate_device_bytes")
+    return b.value
 
 
 def report_dict(rep: N.Report) -> dict:

@@ -112,6 +112,21 @@ def _load():
         "ccfd_get_profile": (c_int, [C.c_void_p, P(c_double), P(c_long), c_int]),
         "ccfd_global_residual_noalloc": (c_int, [C.c_void_p, C.c_void_p, c_long, c_double,
                                                  C.c_void_p, C.c_void_p]),
+        "ccfd_batch_create": (c_int, [c_int, P(C.c_void_p)]),
+        "ccfd_batch_destroy": (None, [C.c_void_p]),
+        "ccfd_batch_add": (c_int, [C.c_void_p, C.c_void_p, c_long]),
+        "ccfd_batch_remove": (c_int, [C.c_void_p, C.c_void_p]),
+        "ccfd_batch_step": (c_int, [C.c_void_p, c_int, P(c_int)]),
+        "ccfd_batch_report": (c_int, [C.c_void_p, C.c_void_p, P(Report)]),
+        "ccfd_batch_size": (c_int, [C.c_void_p, P(c_int)]),
+        "ccfd_estimate_device_bytes": (c_int, [P(Params), P(Mesh), P(C.c_size_t)]),
+        "ccfd_device_bytes": (c_int, [C.c_void_p, P(C.c_size_t)]),
+        "ccfd_server_create": (c_int, [c_int, C.c_size_t, c_int, P(C.c_void_p)]),
+        "ccfd_server_destroy": (None, [C.c_void_p]),
+        "ccfd_server_submit": (c_int, [C.c_void_p, C.c_void_p, c_long, P(c_long)]),
+        "ccfd_server_poll": (c_int, [C.c_void_p, c_int, P(c_int), P(c_int), P(c_int)]),
+        "ccfd_server_result": (c_int, [C.c_void_p, c_long, P(Report), P(c_double), P(c_double)]),
+        "ccfd_server_memory": (c_int, [C.c_void_p, P(C.c_size_t), P(C.c_size_t)]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)

@@ -41,6 +41,7 @@ def _nvcc() -> str:
 def _headers() -> list[str]:
     return (glob.glob(os.path.join(CSRC, "**", "*.h"), recursive=True)
             + glob.glob(os.path.join(CSRC, "**", "*.cuh"), recursive=True)
+            + glob.glob(os.path.join(CSRC, "**", "*.inc"), recursive=True)
             + glob.glob(os.path.join(INC, "*.h")))
 
 

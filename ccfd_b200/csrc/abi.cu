@@ -25,12 +25,13 @@ using namespace ccfd;
         }                                   \
     } while (0)
 
-static int status_from_flags(unsigned f) {
+int ccfd_status_from_flags(unsigned f) {
     if (f & FLAG_DT) return CCFD_ERR_DT;
     if (f & FLAG_VACUUM) return CCFD_ERR_VACUUM;
     if (f & FLAG_STATE) return CCFD_ERR_STATE;
     if (f & FLAG_SINGULAR) return CCFD_ERR_SINGULAR;
     if (f & FLAG_GMRES) return CCFD_ERR_GMRES;
+    if (f & FLAG_NEWTON) return CCFD_ERR_NEWTON;
     return CCFD_OK;
 }
 
@@ -141,6 +142,7 @@ extern "C" int ccfd_create(const ccfd_params* params, ccfd_ctx** out) {
 
 extern "C" void ccfd_destroy(ccfd_ctx* ctx) {
     if (!ctx) return;
+    if (ctx->batch) ccfd_batch_remove((ccfd_batch*)ctx->batch, ctx);
     cudaStreamSynchronize(ctx->stream);
     free_device(ctx);
     if (ctx->ev_run0) cudaEventDestroy(ctx->ev_run0);
@@ -432,7 +434,7 @@ extern "C" int ccfd_upload_case(ccfd_ctx* ctx, const ccfd_mesh* m, const ccfd_bc
     return CCFD_OK;
 }
 
-static void fill_stage(ccfd_ctx* ctx, StageLaunch& L) {
+void ccfd_fill_stage(ccfd_ctx* ctx, StageLaunch& L) {
     memset(&L, 0, sizeof(L));
     L.mesh = ctx->mesh;
     L.tiles = ctx->tiles;
@@ -460,13 +462,18 @@ static int check_flags(ccfd_ctx* ctx) {
     CK(cudaMemcpyAsync(&f, ctx->flags, sizeof(unsigned), cudaMemcpyDeviceToHost, ctx->stream));
     CK(cudaStreamSynchronize(ctx->stream));
     if (f) CK(cudaMemsetAsync(ctx->flags, 0, sizeof(unsigned), ctx->stream));
-    return status_from_flags(f);
+    return ccfd_status_from_flags(f);
 }
 
-static double4* cur_prim(ccfd_ctx* ctx) { return ctx->prim_buf[ctx->cur]; }
+// primitive buffer of the current state (a batch member's parity lives in
+// its control block, whose host copy the batch refreshes after each call)
+static double4* cur_prim(ccfd_ctx* ctx) {
+    return ctx->prim_buf[ctx->batch ? ctx->h_ctrl->par : ctx->cur];
+}
 
 extern "C" int ccfd_set_state(ccfd_ctx* ctx, const double* state, int kind) {
     if (!ctx || !state || !ctx->uploaded) return CCFD_ERR_ARG;
+    if (ctx->batch) return CCFD_ERR_BUSY;
     CK(cudaSetDevice(ctx->device));
     const long N = ctx->N;
     std::vector<double4> prim(N), cons(N);
@@ -507,6 +514,7 @@ extern "C" int ccfd_get_state(ccfd_ctx* ctx, double* state, int kind) {
 
 extern "C" int ccfd_set_time(ccfd_ctx* ctx, double t) {
     if (!ctx || !ctx->uploaded) return CCFD_ERR_ARG;
+    if (ctx->batch) return CCFD_ERR_BUSY;
     CK(cudaSetDevice(ctx->device));
     CK(cudaMemcpyAsync(ctx->h_ctrl, ctx->ctrl, sizeof(Ctrl), cudaMemcpyDeviceToHost, ctx->stream));
     CK(cudaStreamSynchronize(ctx->stream));
@@ -532,7 +540,7 @@ extern "C" int ccfd_get_time(ccfd_ctx* ctx, double* t) {
 // Residual of the current state into ctx->u_t (device); no host copies.
 int ccfd_residual_device(ccfd_ctx* ctx, double time) {
     StageLaunch L;
-    fill_stage(ctx, L);
+    ccfd_fill_stage(ctx, L);
     L.ctrl = nullptr;
     L.tfix = time;
     L.mode = 0;
@@ -547,7 +555,7 @@ int ccfd_residual_device(ccfd_ctx* ctx, double time) {
 
 int ccfd_residual_of(ccfd_ctx* ctx, const double4* prim, double time, double4* ut) {
     StageLaunch L;
-    fill_stage(ctx, L);
+    ccfd_fill_stage(ctx, L);
     L.ctrl = nullptr;
     L.tfix = time;
     L.mode = 0;
@@ -561,6 +569,7 @@ int ccfd_residual_of(ccfd_ctx* ctx, const double4* prim, double time, double4* u
 
 extern "C" int ccfd_residual(ccfd_ctx* ctx, double time, double* u_t_out, double* grad_out) {
     if (!ctx || !ctx->uploaded) return CCFD_ERR_ARG;
+    if (ctx->batch) return CCFD_ERR_BUSY;
     CK(cudaSetDevice(ctx->device));
     int st = ccfd_residual_device(ctx, time);
     if (st) return st;
@@ -603,6 +612,7 @@ extern "C" int ccfd_global_residual(ccfd_ctx* ctx, double res[4]) {
 
 extern "C" int ccfd_time_step(ccfd_ctx* ctx, double* dt_out) {
     if (!ctx || !dt_out || !ctx->uploaded) return CCFD_ERR_ARG;
+    if (ctx->batch) return CCFD_ERR_BUSY;
     CK(cudaSetDevice(ctx->device));
     launch_dt(ctx->mesh, ctx->phys, nullptr, ctx->sp, cur_prim(ctx), ctx->dt_partial, ctx->dt_bad, ctx->stream);
     CK(cudaGetLastError());
@@ -635,7 +645,7 @@ static int record_step(ccfd_ctx* ctx, int par, const std::vector<cudaEvent_t>* e
     const StepParams& sp = ctx->sp;
     for (int s = 1; s <= sp.nrk; ++s) {
         StageLaunch L;
-        fill_stage(ctx, L);
+        ccfd_fill_stage(ctx, L);
         L.ctrl = ctx->ctrl;
         L.a_time = sp.rk[s - 1];
         L.mode = 1;
@@ -683,7 +693,7 @@ static int build_graph(ccfd_ctx* ctx, int par, int steps, cudaGraphExec_t* exec,
     return CCFD_OK;
 }
 
-static void fill_report(ccfd_ctx* ctx, ccfd_report* r) {
+void ccfd_fill_report(ccfd_ctx* ctx, ccfd_report* r) {
     const Ctrl& c = *ctx->h_ctrl;
     memset(r, 0, sizeof(*r));
     r->t = c.t;
@@ -697,7 +707,7 @@ static void fill_report(ccfd_ctx* ctx, ccfd_report* r) {
     r->finished = c.finished;
     r->newton_iterations = ctx->newton_total;
     r->gmres_iterations = ctx->gmres_total;
-    r->status = status_from_flags(c.flags);
+    r->status = ccfd_status_from_flags(c.flags);
 }
 
 // accumulate the stage times of the steps that ran (their event pairs come
@@ -737,6 +747,7 @@ extern "C" int ccfd_get_profile(ccfd_ctx* ctx, double* residual_ms, long* residu
 
 extern "C" int ccfd_run_explicit(ccfd_ctx* ctx, long nsteps, ccfd_report* report) {
     if (!ctx || !ctx->uploaded) return CCFD_ERR_ARG;
+    if (ctx->batch) return CCFD_ERR_BUSY;
     if (ctx->params.implicit) return ccfd_run_implicit(ctx, nsteps, report);
     CK(cudaSetDevice(ctx->device));
     int st;
@@ -784,10 +795,10 @@ extern "C" int ccfd_run_explicit(ccfd_ctx* ctx, long nsteps, ccfd_report* report
     CK(cudaMemcpyAsync(&f, ctx->flags, sizeof(unsigned), cudaMemcpyDeviceToHost, ctx->stream));
     CK(cudaStreamSynchronize(ctx->stream));
     if (report) {
-        fill_report(ctx, report);
+        ccfd_fill_report(ctx, report);
         report->device_ms = run_ms;
     }
-    return status_from_flags(c.flags | f);
+    return ccfd_status_from_flags(c.flags | f);
 }
 
 extern "C" int ccfd_clcd(ccfd_ctx* ctx, double* cl, double* cd) {

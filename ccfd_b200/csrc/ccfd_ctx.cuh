@@ -60,8 +60,16 @@ struct ccfd_ctx {
     long prof_count = 0;
     cudaEvent_t ev_run0 = nullptr, ev_run1 = nullptr;
     void* implicit_state = nullptr;  // owned by the implicit solver
+    void* batch = nullptr;           // the batch this context is stepped by, if any
 };
 
+// launch record of a residual evaluation / RK stage of this context with
+// the fields common to all stages filled in (abi.cu)
+void ccfd_fill_stage(ccfd_ctx* ctx, ccfd::StageLaunch& L);
+// status code of device error flags; report from the host copy of the
+// control block (abi.cu)
+int ccfd_status_from_flags(unsigned f);
+void ccfd_fill_report(ccfd_ctx* ctx, ccfd_report* r);
 // device-side residual of the current state into ctx->u_t (abi.cu)
 int ccfd_residual_device(ccfd_ctx* ctx, double time);
 // residual of an arbitrary primitive state into ut (abi.cu)

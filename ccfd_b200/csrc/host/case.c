@@ -40,6 +40,7 @@ const char *ccfd_strerror(int s)
 	case CCFD_ERR_UNSUPPORTED: return "option not supported";
 	case CCFD_ERR_NOT_CONVERGED: return "Maximum Iteration Number Reached";
 	case CCFD_ERR_GMRES: return "GMRES breakdown";
+	case CCFD_ERR_BUSY: return "context is being stepped by a batch";
 	default: return "unknown status";
 	}
 }

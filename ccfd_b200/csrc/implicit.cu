@@ -829,8 +829,7 @@ static int implicit_step(ccfd_ctx* ctx, ImpState* S) {
     return CCFD_OK;
 }
 
-extern "C" int ccfd_run_implicit(ccfd_ctx* ctx, long nsteps, ccfd_report* report) {
-    if (!ctx || !ctx->uploaded) return CCFD_ERR_ARG;
+static int run_implicit(ccfd_ctx* ctx, long nsteps, ccfd_report* report) {
     CK(cudaSetDevice(ctx->device));
     ImpState* S = (ImpState*)ctx->implicit_state;
     if (!S || !S->ready) return CCFD_ERR_ARG;
@@ -885,5 +884,49 @@ extern "C" int ccfd_run_implicit(ccfd_ctx* ctx, long nsteps, ccfd_report* report
     if (status) return status;
     if (c.flags & FLAG_DT) return CCFD_ERR_DT;
     if (c.flags & FLAG_STATE) return CCFD_ERR_STATE;
+    return CCFD_OK;
+}
+
+extern "C" int ccfd_run_implicit(ccfd_ctx* ctx, long nsteps, ccfd_report* report) {
+    if (!ctx || !ctx->uploaded) return CCFD_ERR_ARG;
+    if (ctx->batch) return CCFD_ERR_BUSY;
+    return run_implicit(ctx, nsteps, report);
+}
+
+// ---------------------------------------------------------------- batching
+// Implicit batch members are stepped one after another by the
+// single-instance driver, each within its own step budget; the batch stream
+// is idle meanwhile (the member's own stream carries the work).
+int ccfd_implicit_batch_join(ccfd_batch*, ccfd_ctx* ctx) {
+    ImpState* S = (ImpState*)ctx->implicit_state;
+    return (S && S->ready) ? CCFD_OK : CCFD_ERR_ARG;
+}
+
+int ccfd_implicit_batch_leave(ccfd_batch*, ccfd_ctx*) { return CCFD_OK; }
+
+int ccfd_implicit_batch_steps(ccfd_batch*, const std::vector<ccfd_ctx*>& members, int steps) {
+    for (ccfd_ctx* ctx : members) {
+        Ctrl& c = *ctx->h_ctrl;
+        CK(cudaMemcpy(&c, ctx->ctrl, sizeof(Ctrl), cudaMemcpyDeviceToHost));
+        if (c.done || c.iter >= c.stop_at) continue;
+        long long budget = c.stop_at;
+        long n = (long)std::min<long long>(steps, budget - c.iter);
+        int st = run_implicit(ctx, n, nullptr);
+        // restore the member's own budget (the driver set stop_at for this call)
+        CK(cudaMemcpy(&ctx->ctrl->stop_at, &budget, sizeof(long long), cudaMemcpyHostToDevice));
+        if (st && st != CCFD_ERR_NEWTON && st != CCFD_ERR_SINGULAR && st != CCFD_ERR_GMRES &&
+            st != CCFD_ERR_STATE && st != CCFD_ERR_DT)
+            return st;
+        if (st) {
+            // a failed member stops; its status stays readable in its report
+            unsigned f = st == CCFD_ERR_NEWTON ? FLAG_NEWTON : st == CCFD_ERR_SINGULAR ? FLAG_SINGULAR
+                       : st == CCFD_ERR_GMRES ? FLAG_GMRES : st == CCFD_ERR_DT ? FLAG_DT : FLAG_STATE;
+            CK(cudaMemcpy(&c, ctx->ctrl, sizeof(Ctrl), cudaMemcpyDeviceToHost));
+            c.flags |= f;
+            c.done = 1;
+            c.active = 0;
+            CK(cudaMemcpy(ctx->ctrl, &c, sizeof(Ctrl), cudaMemcpyHostToDevice));
+        }
+    }
     return CCFD_OK;
 }

@@ -47,7 +47,8 @@ struct StageLaunch {
     double a_time;         // stage time = t + a_time * dt
     int order, limiter, flux_id, ns;
     int fp32;              // 1: FP32 reconstruction and face fluxes (mixed precision)
-    int mode;              // 0: residual u_t only; 1: RK stage
+    int mode;              // 0: residual u_t only; 1: RK stage; -1: no-op (batched stage slot)
+    const int* skip;       // batched residual evaluations: skipped while *skip != 0
     const double4* prim_in;
     double4* prim_out;     // RK: updated primitive state
     double4* cons0;        // RK: stage-start conservative state (updated in place at the last stage)
@@ -65,7 +66,22 @@ struct StageLaunch {
     const double* wall_nl; // their (n.x, n.y, len)
 };
 
+// Stage slots per instance and buffer parity in a batched RK launch record
+// array (RK schemes have at most 5 stages).
+constexpr int kBatchStages = 6;
+
+// One launch of the stage kernel over the concatenated tiles of several
+// instances that share the kernel variant (flux, order, equations, precision).
+struct BatchLaunch {
+    const StageLaunch* recs;  // rk_mode: [inst][2][kBatchStages], else [inst]
+    const int2* tmap;         // [n_tiles] (instance, tile)
+    int n_tiles, smem_bytes;
+    int rk_mode, stage;
+    int flux_id, order, ns, fp32;
+};
+
 void launch_stage(const StageLaunch& L, cudaStream_t st);
+void launch_stage_batch(const BatchLaunch& B, cudaStream_t st);
 int stage_smem_bytes(const TileDev& T, int fp32);
 void launch_dt(const DevMesh& m, const Phys& P, const Ctrl* ctrl, const StepParams& sp,
                const double4* prim, double2* partial, int* bad_partial, cudaStream_t st);

@@ -48,6 +48,7 @@ enum DevFlag : unsigned {
     FLAG_STATE = 4u,     // non-finite residual
     FLAG_SINGULAR = 8u,  // singular LU-SGS block
     FLAG_GMRES = 16u,
+    FLAG_NEWTON = 32u,   // Newton not converged (set by the host driver)
 };
 
 template <typename T>

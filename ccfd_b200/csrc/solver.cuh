@@ -40,6 +40,7 @@ struct Ctrl {
     int have_first;
     double cl, cd;
     double visc_dominates;
+    int par;         // primitive buffer holding the current state (batched RK runs)
 };
 
 // Run parameters of the explicit integrator (kernel argument).

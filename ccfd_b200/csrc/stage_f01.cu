@@ -1,0 +1,3 @@
+// Stage kernels of convective flux 1 (fluxFunction = 1).
+#define CCFD_FLUX_ID 1
+#include "stage_flux.inc"

@@ -1,0 +1,3 @@
+// Stage kernels of convective flux 2 (fluxFunction = 2).
+#define CCFD_FLUX_ID 2
+#include "stage_flux.inc"

@@ -1,0 +1,3 @@
+// Stage kernels of convective flux 4 (fluxFunction = 4).
+#define CCFD_FLUX_ID 4
+#include "stage_flux.inc"

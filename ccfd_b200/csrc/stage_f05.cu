@@ -1,0 +1,3 @@
+// Stage kernels of convective flux 5 (fluxFunction = 5).
+#define CCFD_FLUX_ID 5
+#include "stage_flux.inc"

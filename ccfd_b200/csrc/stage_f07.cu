@@ -1,0 +1,3 @@
+// Stage kernels of convective flux 7 (fluxFunction = 7).
+#define CCFD_FLUX_ID 7
+#include "stage_flux.inc"

@@ -1,0 +1,3 @@
+// Stage kernels of convective flux 8 (fluxFunction = 8).
+#define CCFD_FLUX_ID 8
+#include "stage_flux.inc"

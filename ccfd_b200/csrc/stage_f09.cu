@@ -1,0 +1,3 @@
+// Stage kernels of convective flux 9 (fluxFunction = 9).
+#define CCFD_FLUX_ID 9
+#include "stage_flux.inc"

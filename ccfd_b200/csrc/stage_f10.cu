@@ -1,0 +1,3 @@
+// Stage kernels of convective flux 10 (fluxFunction = 10).
+#define CCFD_FLUX_ID 10
+#include "stage_flux.inc"

@@ -40,7 +40,8 @@ enum ccfd_status {
 	CCFD_ERR_BUDGET = 12,      /* request exceeds the device-memory budget */
 	CCFD_ERR_UNSUPPORTED = 13, /* option not built (e.g. periodic BC)      */
 	CCFD_ERR_NOT_CONVERGED = 14, /* maxIter reached, timeDiscretization.c:737-750 */
-	CCFD_ERR_GMRES = 15          /* GMRES breakdown (zero Hessenberg pivot)  */
+	CCFD_ERR_GMRES = 15,         /* GMRES breakdown (zero Hessenberg pivot)  */
+	CCFD_ERR_BUSY = 16           /* context is being stepped by a batch      */
 };
 
 /* enumerations: numbering identical to the reference's src/main.h */
@@ -280,6 +281,57 @@ int ccfd_get_profile(ccfd_ctx *ctx, double *residual_ms, long *residual_count,
 		     int reset);
 /* Drop-in for globalResidual on the last residual (src/analyze.c:521-539). */
 int ccfd_global_residual(ccfd_ctx *ctx, double res[4]);
+
+/* ------------------------------------------------------------- batching
+ * Many contexts stepped together on one GPU (no counterpart in the
+ * reference, which runs one case per process).  A member is an uploaded
+ * context; while it is in a batch, the batch owns it: ccfd_run_*,
+ * ccfd_set_state, ccfd_residual and ccfd_set_time return CCFD_ERR_BUSY,
+ * ccfd_get_state and ccfd_batch_report read its current state and control
+ * block.  Explicit members advance in multi-instance stage launches over
+ * their concatenated tiles (one launch per kernel variant and RK stage,
+ * replayed from a CUDA graph); implicit members advance in lockstep Newton /
+ * GMRES / LU-SGS iterations whose kernels cover every member at once.  Each
+ * member keeps its own time step, CFL, stop criteria and flags. */
+typedef struct ccfd_batch ccfd_batch;
+int ccfd_batch_create(int device, ccfd_batch **out);
+void ccfd_batch_destroy(ccfd_batch *b);   /* releases the members too */
+/* join with a budget of nsteps time steps (<= 0: until the member stops) */
+int ccfd_batch_add(ccfd_batch *b, ccfd_ctx *ctx, long nsteps);
+int ccfd_batch_remove(ccfd_batch *b, ccfd_ctx *ctx);
+/* advance every running member by up to `steps` time steps; *n_running
+ * receives the number of members that can still step */
+int ccfd_batch_step(ccfd_batch *b, int steps, int *n_running);
+/* a member's report (device_ms: the batch's accumulated device time) */
+int ccfd_batch_report(ccfd_batch *b, ccfd_ctx *ctx, ccfd_report *r);
+int ccfd_batch_size(ccfd_batch *b, int *n);
+
+/* ------------------------------------------------------------- serving
+ * A request loop with continuous batching (no counterpart in the reference).
+ * Requests queue in arrival order; ccfd_server_poll admits them first come,
+ * first served while their estimated device memory fits the budget and fewer
+ * than max_running run, uploads each into its own context, steps all running
+ * requests together in one batch, and retires the ones that stopped (final
+ * state copied to the host, device memory released). */
+typedef struct ccfd_server ccfd_server;
+/* device memory a case will hold once uploaded (an upper estimate) */
+int ccfd_estimate_device_bytes(const ccfd_params *p, const ccfd_mesh *m, size_t *bytes);
+/* device memory a context holds */
+int ccfd_device_bytes(ccfd_ctx *ctx, size_t *bytes);
+int ccfd_server_create(int device, size_t hbm_budget_bytes, int max_running, ccfd_server **out);
+void ccfd_server_destroy(ccfd_server *s);
+/* queue case c (kept alive by the caller until its result is fetched) with
+ * a budget of nsteps steps (<= 0: until it stops); CCFD_ERR_BUDGET if it
+ * can never fit */
+int ccfd_server_submit(ccfd_server *s, const ccfd_case *c, long nsteps, long *id);
+/* admit, advance the running requests by up to `steps` steps, retire */
+int ccfd_server_poll(ccfd_server *s, int steps, int *n_queued, int *n_running, int *n_done);
+/* a finished request: report, final primitive state [n_cells][4] (may be
+ * NULL), times {submit, admit, done} in seconds of a monotonic host clock
+ * (may be NULL); returns the request's status and forgets it, or
+ * CCFD_ERR_BUSY while it is queued or running */
+int ccfd_server_result(ccfd_server *s, long id, ccfd_report *rep, double *prim, double times[3]);
+int ccfd_server_memory(ccfd_server *s, size_t *used, size_t *budget);
 
 /* Largest cell count of ccfd_global_residual_noalloc (its static scratch
  * holds one 4-double partial sum per 256 cells: 128 KB). */
