@@ -243,6 +243,8 @@ extern "C" int ccfd_batch_create(int device, ccfd_batch** out) {
     return CCFD_OK;
 }
 
+void ccfd_implicit_batch_release(ccfd_batch* b);
+
 extern "C" void ccfd_batch_destroy(ccfd_batch* b) {
     if (!b) return;
     cudaSetDevice(b->device);
@@ -252,6 +254,7 @@ extern "C" void ccfd_batch_destroy(ccfd_batch* b) {
         c->cur = c->h_ctrl->par;
         c->batch = nullptr;
     }
+    ccfd_implicit_batch_release(b);
     drop_group_memory(b);
     if (b->d_ctrl_ptr) cudaFree((void*)b->d_ctrl_ptr);
     if (b->d_ctrl) cudaFree(b->d_ctrl);
@@ -264,6 +267,7 @@ extern "C" void ccfd_batch_destroy(ccfd_batch* b) {
 
 int ccfd_implicit_batch_join(ccfd_batch* b, ccfd_ctx* ctx);
 int ccfd_implicit_batch_leave(ccfd_batch* b, ccfd_ctx* ctx);
+void ccfd_implicit_batch_release(ccfd_batch* b);
 
 extern "C" int ccfd_batch_add(ccfd_batch* b, ccfd_ctx* ctx, long nsteps) {
     if (!b || !ctx || !ctx->uploaded || ctx->batch || ctx->device != b->device) return CCFD_ERR_ARG;

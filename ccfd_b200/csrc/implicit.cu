@@ -25,12 +25,22 @@
 // lower (forward) / higher (backward) reference number, so every level is a
 // set of independent cells and the sweep result is exactly the sequential
 // one.
+//
+// Every kernel works on a set of members (independent cases) at once:
+// blockIdx.y selects the member's descriptor, blockIdx.x the block of its
+// cells.  All members advance in lockstep through the same sequence of
+// Newton and Krylov iterations; a member whose GMRES cycle or Newton loop has
+// ended (or failed) is switched off by flags in device memory and its blocks
+// return at once, so the result of every member is exactly that of the
+// member running alone.  A single case is a set of one.
 #include <cuda_runtime.h>
 #include <float.h>
 #include <math.h>
 #include <string.h>
 
 #include <algorithm>
+#include <map>
+#include <tuple>
 #include <vector>
 
 #include "ccfd_ctx.cuh"
@@ -49,6 +59,37 @@ enum Sc {
     SC_H = 16
 };
 
+// per-member control words (ImpDev::ctl)
+enum Ctl {
+    CTL_NEWTON = 0,    // Newton loop of the current time step running
+    CTL_INNER,         // Newton iterations of the current time step
+    CTL_GMRES_TOTAL,   // GMRES iterations so far (report)
+    CTL_NEWTON_TOTAL,  // Newton iterations so far (report)
+    CTL_SKIP_JAC,      // residual evaluations of the Jacobian colour loop skipped
+    CTL_STATUS,        // failure status (ccfd_status) of the current step
+    CTL_SKIP_NEWTON,   // == !CTL_NEWTON (skip word of the Newton residuals)
+    CTL_SKIP_GMRES,    // GMRES iteration skipped (cycle ended or Newton off)
+    CTL_WORDS = 8
+};
+
+// Device descriptor of one member (pointers into its context and state).
+struct ImpDev {
+    long N;
+    int K, nb, precond, n_newton;
+    double gam1, eps_gmres, eps2newton;
+    double4 *XK, *Q, *RXK, *F, *dX, *W, *V, *Z, *ptmp, *ut, *dxs, *cons, *prim, *pert;
+    double *D, *Dinv, *O, *sc, *partial;
+    int* flag;  // [0] GMRES cycle done, [1] final m, [2] singular, [3] non-finite
+    int* ctl;   // Ctl words
+    Ctrl* ctrl;
+    const int *hs_off, *hs_nb, *twin;
+    int ncol;
+    const int *color_off, *color_cells;
+    int n_lev_f, n_lev_b;
+    const int *lev_f_off, *lev_f_cells, *lev_b_off, *lev_b_cells;
+    const int *lo_off, *lo_nb, *lo_h, *up_off, *up_nb, *up_h;
+};
+
 struct ImpState {
     int K = 0;            // nKdim
     long N = 0;
@@ -57,11 +98,13 @@ struct ImpState {
     double4 *dxs = nullptr;
     double *D = nullptr, *Dinv = nullptr, *O = nullptr;  // [N][16], [N][16], [H][16]
     double* sc = nullptr;        // device scalars
-    int* flag = nullptr;         // [0] gmres done, [1] m_final, [2] singular
+    int* flag = nullptr;         // [0] gmres done, [1] m_final, [2] singular, [3] non-finite
+    int* ctl = nullptr;          // Ctl words
     double* partial = nullptr;   // per-block partial sums
     int nb = 0;
     // colouring (device cell lists per colour) and neighbour twins
     std::vector<int> color_off;  // host copy of the colour offsets
+    int* color_off_d = nullptr;
     int* color_cells = nullptr;
     int* twin = nullptr;         // [H] half-side of the neighbour that points back
     // LU-SGS level schedules
@@ -70,6 +113,7 @@ struct ImpState {
     int *lo_off = nullptr, *lo_nb = nullptr, *lo_h = nullptr;
     int *up_off = nullptr, *up_nb = nullptr, *up_h = nullptr;
     bool ready = false;
+    void* solo = nullptr;        // the member set of this context running alone
 };
 
 __device__ __forceinline__ void ld(const double4& v, double q[4]) {
@@ -102,22 +146,90 @@ __device__ __forceinline__ void block_partial(double v, double* partial) {
     }
 }
 
-__global__ void k_dot(const double4* __restrict__ a, const double4* __restrict__ b, long n,
-                      double* __restrict__ partial, const int* __restrict__ skip) {
-    if (skip && skip[0]) return;
-    long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
-    double v = i < n ? cell_dot(a[i], b[i]) : 0.0;
-    block_partial(v, partial);
+__device__ __forceinline__ bool newton_on(const ImpDev& d) { return d.ctl[CTL_NEWTON] != 0; }
+__device__ __forceinline__ bool gmres_on(const ImpDev& d) { return d.ctl[CTL_SKIP_GMRES] == 0; }
+
+// a member's step fails: its Newton loop and GMRES cycle stop, the control
+// block records the error and the member does not step again
+__device__ void fail_member(const ImpDev& d, int status, unsigned devflag) {
+    d.ctl[CTL_STATUS] = status;
+    d.ctl[CTL_NEWTON_TOTAL] += d.ctl[CTL_INNER];
+    d.ctl[CTL_NEWTON] = 0;
+    d.ctl[CTL_SKIP_NEWTON] = 1;
+    d.ctl[CTL_SKIP_GMRES] = 1;
+    d.flag[0] = 1;
+    d.ctrl->flags |= devflag;
+    d.ctrl->done = 1;
+    d.ctrl->active = 0;
 }
 
-// fixed-order final reduction; mode 0: sum, 1: sqrt(sum),
-// 2: sqrt(DBL_EPSILON) / sqrt(sum) (the finite-difference step)
-__global__ void k_final(const double* __restrict__ partial, int nb, double* out, int mode,
-                        const int* __restrict__ skip) {
-    if (skip && skip[0]) return;
+#define MEMBER const ImpDev& d = I[blockIdx.y]
+#define CELL_INDEX                                           \
+    if ((int)blockIdx.x >= d.nb) return;                     \
+    const long i = (long)blockIdx.x * blockDim.x + threadIdx.x
+
+// start of a time step: members whose control block lets them step run
+// their Newton loop
+__global__ void kb_step_prepare(const ImpDev* __restrict__ I) {
+    MEMBER;
+    if (threadIdx.x) return;
+    int on = d.ctrl->active != 0;
+    d.ctl[CTL_NEWTON] = on;
+    d.ctl[CTL_SKIP_NEWTON] = !on;
+    d.ctl[CTL_SKIP_GMRES] = 1;
+    d.ctl[CTL_INNER] = 0;
+    d.ctl[CTL_STATUS] = 0;
+}
+
+// Q = cVar; pVar = consPrim(cVar) (src/timeDiscretization.c:420-433)
+__global__ void kb_step_begin(const ImpDev* __restrict__ I) {
+    MEMBER;
+    if (!newton_on(d)) return;
+    CELL_INDEX;
+    if (i >= d.N) return;
+    double c[4], p[4];
+    double4 cv = d.cons[i];
+    d.Q[i] = cv;
+    ld(cv, c);
+    cons_prim(d.gam1, c, p);
+    d.prim[i] = mk(p);
+}
+
+// F = (cVar - Q) - alpha dt u_t and its dot partial; at the step start also
+// XK = cVar (src/timeDiscretization.c:439-449, 533-536)
+__global__ void kb_newton_F(const ImpDev* __restrict__ I, int copy_xk) {
+    MEMBER;
+    if (!newton_on(d)) return;
+    CELL_INDEX;
+    double v = 0.0;
+    if (i < d.N) {
+        const double adt = 1.0 * d.ctrl->dt;
+        double c[4], q[4], u[4], f[4];
+        double4 cv = d.cons[i];
+        ld(cv, c);
+        ld(d.Q[i], q);
+        ld(d.RXK[i], u);
+#pragma unroll
+        for (int k = 0; k < 4; ++k) f[k] = c[k] - q[k] - adt * u[k];
+        double4 fv = mk(f);
+        d.F[i] = fv;
+        if (copy_xk) d.XK[i] = cv;
+        v = cell_dot(fv, fv);
+    }
+    block_partial(v, d.partial);
+}
+
+enum FinalTarget { FT_NORM_X0 = 0, FT_NORM_XK, FT_EPSFD, FT_H };
+
+// fixed-order final reduction of a member's partials; mode 0: sum,
+// 1: sqrt(sum), 2: sqrt(DBL_EPSILON) / sqrt(sum) (the finite-difference step)
+__global__ void kb_final(const ImpDev* __restrict__ I, int target, int row, int col, int mode,
+                         int gmres_gate) {
+    MEMBER;
+    if (gmres_gate ? !gmres_on(d) : !newton_on(d)) return;
     __shared__ double sh[kB];
     double v = 0.0;
-    for (int i = threadIdx.x; i < nb; i += blockDim.x) v += partial[i];
+    for (int k = threadIdx.x; k < d.nb; k += blockDim.x) v += d.partial[k];
     sh[threadIdx.x] = v;
     __syncthreads();
     for (int s = blockDim.x / 2; s > 0; s >>= 1) {
@@ -128,127 +240,155 @@ __global__ void k_final(const double* __restrict__ partial, int nb, double* out,
         double r = sh[0];
         if (mode == 1) r = sqrt(r);
         else if (mode == 2) r = sqrt(DBL_EPSILON) / sqrt(r);
+        double* out = target == FT_NORM_X0 ? d.sc + SC_NORM_X0
+                    : target == FT_NORM_XK ? d.sc + SC_NORM_XK
+                    : target == FT_EPSFD   ? d.sc + SC_EPSFD
+                                           : d.sc + SC_H + row * (d.K + 1) + col;
         *out = r;
     }
 }
 
-__global__ void k_copy(double4* __restrict__ dst, const double4* __restrict__ src, long n) {
-    long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i < n) dst[i] = src[i];
-}
-
-__global__ void k_cons2prim(const double4* __restrict__ cons, double4* __restrict__ prim, long n,
-                            double gam1) {
-    long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
-    double c[4], p[4];
-    ld(cons[i], c);
-    cons_prim(gam1, c, p);
-    prim[i] = mk(p);
-}
-
-// F = (cVar - Q) - alpha dt u_t and its dot partial
-// (src/timeDiscretization.c:439-449, 533-536)
-__global__ void k_newton_F(const double4* __restrict__ cons, const double4* __restrict__ Q,
-                           const double4* __restrict__ ut, double adt, double4* __restrict__ F,
-                           long n, double* __restrict__ partial) {
-    long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
-    double v = 0.0;
-    if (i < n) {
-        double c[4], q[4], u[4], f[4];
-        ld(cons[i], c);
-        ld(Q[i], q);
-        ld(ut[i], u);
-#pragma unroll
-        for (int k = 0; k < 4; ++k) f[k] = c[k] - q[k] - adt * u[k];
-        double4 fv = mk(f);
-        F[i] = fv;
-        v = cell_dot(fv, fv);
+// eps2newtonLoc and the first test of the Newton loop
+// (src/timeDiscretization.c:469-478)
+__global__ void kb_newton_start(const ImpDev* __restrict__ I) {
+    MEMBER;
+    if (threadIdx.x || !newton_on(d)) return;
+    double n0 = d.sc[SC_NORM_X0];
+    double eps2loc = fmax(1e-8 * 1e-8 * d.N * d.eps2newton / n0, d.eps2newton);
+    d.sc[SC_EPS2LOC] = eps2loc;
+    d.sc[SC_NORM_XK] = n0;
+    if (!((n0 > eps2loc * n0) && (0 < d.n_newton))) {
+        d.ctl[CTL_NEWTON] = 0;
+        d.ctl[CTL_SKIP_NEWTON] = 1;
+        if (d.n_newton == 0) {
+            d.ctl[CTL_STATUS] = CCFD_ERR_NEWTON;
+            d.ctrl->flags |= FLAG_NEWTON;
+            d.ctrl->done = 1;
+            d.ctrl->active = 0;
+        }
     }
-    block_partial(v, partial);
 }
 
-// R0 = -B, delX = 0, V0 = R0 / normR0 (src/linearSolver.c:392-408)
-__global__ void k_gmres_init(const double4* __restrict__ B, const double* __restrict__ sc,
-                             double4* __restrict__ V0, double4* __restrict__ dX, long n) {
-    long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
+// GMRES set-up: normB = sqrt(|F|^2), abortCrit, gam[0]; R0 = -B, delX = 0,
+// V0 = R0 / normR0 (src/linearSolver.c:385-408)
+__global__ void kb_gmres_init(const ImpDev* __restrict__ I) {
+    MEMBER;
+    if (!newton_on(d)) return;
+    CELL_INDEX;
+    const double nr = sqrt(d.sc[SC_NORM_XK]);
+    if (i == 0) {
+        double* H = d.sc + SC_H;
+        double* gam = H + (d.K + 1) * (d.K + 1);
+        d.sc[SC_NORMB] = nr;
+        d.sc[SC_ABORT] = d.eps_gmres * nr;
+        gam[0] = nr;
+    }
+    if (i >= d.N) return;
     double b[4], v[4];
-    ld(B[i], b);
-    double nr = sc[SC_NORMB];
+    ld(d.F[i], b);
 #pragma unroll
     for (int k = 0; k < 4; ++k) v[k] = -b[k] / nr;
-    V0[i] = mk(v);
-    dX[i] = make_double4(0.0, 0.0, 0.0, 0.0);
+    d.V[i] = mk(v);
+    d.dX[i] = make_double4(0.0, 0.0, 0.0, 0.0);
+}
+
+// flags of a new GMRES cycle (after kb_gmres_init has run on every block)
+__global__ void kb_gmres_flags(const ImpDev* __restrict__ I) {
+    MEMBER;
+    if (threadIdx.x) return;
+    int on = newton_on(d);
+    d.flag[0] = on ? 0 : 1;
+    d.flag[1] = d.flag[2] = d.flag[3] = 0;
+    d.ctl[CTL_SKIP_GMRES] = !on;
+}
+
+// Z_m = V_m when the preconditioner is off
+__global__ void kb_copy_vz(const ImpDev* __restrict__ I, int m) {
+    MEMBER;
+    if (d.precond || !gmres_on(d)) return;
+    CELL_INDEX;
+    if (i < d.N) d.Z[(long)m * d.N + i] = d.V[(long)m * d.N + i];
+}
+
+__global__ void kb_dot_zz(const ImpDev* __restrict__ I, int m) {
+    MEMBER;
+    if (!gmres_on(d)) return;
+    CELL_INDEX;
+    double v = 0.0;
+    if (i < d.N) {
+        double4 z = d.Z[(long)m * d.N + i];
+        v = cell_dot(z, z);
+    }
+    block_partial(v, d.partial);
 }
 
 // U = XK + eps v, pVar = consPrim(U) (src/linearSolver.c:350-360)
-__global__ void k_mv_prep(const double4* __restrict__ XK, const double4* __restrict__ v,
-                          const double* __restrict__ sc, double4* __restrict__ prim, long n,
-                          double gam1, const int* __restrict__ skip) {
-    if (skip[0]) return;
-    long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
+__global__ void kb_mv_prep(const ImpDev* __restrict__ I, int m) {
+    MEMBER;
+    if (!gmres_on(d)) return;
+    CELL_INDEX;
+    if (i >= d.N) return;
     double x[4], z[4], c[4], p[4];
-    ld(XK[i], x);
-    ld(v[i], z);
-    double e = sc[SC_EPSFD];
+    ld(d.XK[i], x);
+    ld(d.Z[(long)m * d.N + i], z);
+    double e = d.sc[SC_EPSFD];
 #pragma unroll
     for (int k = 0; k < 4; ++k) c[k] = x[k] + e * z[k];
-    cons_prim(gam1, c, p);
-    prim[i] = mk(p);
+    cons_prim(d.gam1, c, p);
+    d.ptmp[i] = mk(p);
 }
 
 // W = v - alpha dt (u_t - R_XK) / eps (src/linearSolver.c:364-372), and the
 // partial of the first Gram-Schmidt product V0 . W
-__global__ void k_mv_finish(const double4* __restrict__ v, const double4* __restrict__ ut,
-                            const double4* __restrict__ rxk, const double* __restrict__ sc,
-                            double adt, double4* __restrict__ W, const double4* __restrict__ V0,
-                            long n, double* __restrict__ partial, const int* __restrict__ skip) {
-    if (skip[0]) return;
-    long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
-    double d = 0.0;
-    if (i < n) {
+__global__ void kb_mv_finish(const ImpDev* __restrict__ I, int m) {
+    MEMBER;
+    if (!gmres_on(d)) return;
+    CELL_INDEX;
+    double dd = 0.0;
+    if (i < d.N) {
+        const double adt = 1.0 * d.ctrl->dt;
         double z[4], u[4], r[4], w[4];
-        ld(v[i], z);
-        ld(ut[i], u);
-        ld(rxk[i], r);
-        double e = sc[SC_EPSFD];
+        ld(d.Z[(long)m * d.N + i], z);
+        ld(d.ut[i], u);
+        ld(d.RXK[i], r);
+        double e = d.sc[SC_EPSFD];
 #pragma unroll
         for (int k = 0; k < 4; ++k) w[k] = z[k] - adt * (u[k] - r[k]) / e;
         double4 wv = mk(w);
-        W[i] = wv;
-        d = cell_dot(V0[i], wv);
+        d.W[i] = wv;
+        dd = cell_dot(d.V[i], wv);
     }
-    block_partial(d, partial);
+    block_partial(dd, d.partial);
 }
 
-// W -= h V_prev (modified Gram-Schmidt step, src/linearSolver.c:440-450),
-// then the partial of V_next . W (or W . W when V_next is null)
-__global__ void k_mgs(double4* __restrict__ W, const double4* __restrict__ Vp,
-                      const double* __restrict__ h, const double4* __restrict__ Vn, long n,
-                      double* __restrict__ partial, const int* __restrict__ skip) {
-    if (skip[0]) return;
-    long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
-    double d = 0.0;
-    if (i < n) {
+// W -= H[nn][m] V_nn (modified Gram-Schmidt step, src/linearSolver.c:
+// 440-450), then the partial of V_{nn+1} . W (or W . W after the last one)
+__global__ void kb_mgs(const ImpDev* __restrict__ I, int nn, int m) {
+    MEMBER;
+    if (!gmres_on(d)) return;
+    CELL_INDEX;
+    double dd = 0.0;
+    if (i < d.N) {
         double w[4], p[4];
-        ld(W[i], w);
-        ld(Vp[i], p);
-        double hh = *h;
+        ld(d.W[i], w);
+        ld(d.V[(long)nn * d.N + i], p);
+        double hh = d.sc[SC_H + nn * (d.K + 1) + m];
 #pragma unroll
         for (int k = 0; k < 4; ++k) w[k] -= hh * p[k];
         double4 wv = mk(w);
-        W[i] = wv;
-        d = Vn ? cell_dot(Vn[i], wv) : cell_dot(wv, wv);
+        d.W[i] = wv;
+        dd = nn < m ? cell_dot(d.V[(long)(nn + 1) * d.N + i], wv) : cell_dot(wv, wv);
     }
-    block_partial(d, partial);
+    block_partial(dd, d.partial);
 }
 
 // Givens rotations, residual estimate and stop test of iteration m, and the
 // back substitution when the cycle ends (src/linearSolver.c:454-481)
-__global__ void k_givens(double* sc, int* flag, int m, int K) {
-    if (flag[0]) return;
+__global__ void kb_givens(const ImpDev* __restrict__ I, int m) {
+    MEMBER;
+    if (threadIdx.x || !gmres_on(d)) return;
+    const int K = d.K;
+    double* sc = d.sc;
     double* H = sc + SC_H;  // H[r * (K + 1) + c]
     double* gam = H + (K + 1) * (K + 1);
     double* C = gam + (K + 1);
@@ -272,98 +412,140 @@ __global__ void k_givens(double* sc, int* flag, int m, int K) {
             for (int o = nn + 1; o <= m; ++o) alp[nn] -= H[nn * ld + o] * alp[o];
             alp[nn] /= H[nn * ld + nn];
         }
-        flag[0] = 1;
-        flag[1] = m;
-        if (!isfinite(alp[0])) flag[3] = 1;
+        d.flag[0] = 1;
+        d.flag[1] = m;
+        if (!isfinite(alp[0])) d.flag[3] = 1;
+        d.ctl[CTL_SKIP_GMRES] = 1;
     }
 }
 
 // V[m+1] = W / H[m+1][m] (src/linearSolver.c:496-502)
-__global__ void k_vnext(const double4* __restrict__ W, const double* __restrict__ h,
-                        double4* __restrict__ Vn, long n, const int* __restrict__ flag) {
-    if (flag[0]) return;
-    long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
+__global__ void kb_vnext(const ImpDev* __restrict__ I, int m) {
+    MEMBER;
+    if (!gmres_on(d)) return;
+    CELL_INDEX;
+    if (i >= d.N) return;
     double w[4];
-    ld(W[i], w);
-    double hh = *h;
+    ld(d.W[i], w);
+    double hh = d.sc[SC_H + (m + 1) * (d.K + 1) + m];
 #pragma unroll
     for (int k = 0; k < 4; ++k) w[k] = w[k] / hh;
-    Vn[i] = mk(w);
+    d.V[(long)(m + 1) * d.N + i] = mk(w);
 }
 
-// delX += alp[nn] Z[nn], nn = 0..m in order (src/linearSolver.c:482-490)
-__global__ void k_delx(double4* __restrict__ dX, const double4* __restrict__ Z,
-                       const double* __restrict__ alp, const int* __restrict__ flag, long n) {
-    long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
-    int m = flag[1];
+// end of a GMRES cycle: iteration count, breakdown test
+__global__ void kb_gmres_end(const ImpDev* __restrict__ I) {
+    MEMBER;
+    if (threadIdx.x || !newton_on(d)) return;
+    d.ctl[CTL_GMRES_TOTAL] += min(d.flag[1], d.K - 1) + 1;
+    if (d.flag[3]) fail_member(d, CCFD_ERR_GMRES, FLAG_GMRES);
+}
+
+// delX += alp[nn] Z[nn], nn = 0..m in order (src/linearSolver.c:482-490);
+// XK += delX, cVar = XK, pVar = consPrim(cVar) (src/timeDiscretization.c:
+// 505-520)
+__global__ void kb_newton_update(const ImpDev* __restrict__ I) {
+    MEMBER;
+    if (!newton_on(d)) return;
+    CELL_INDEX;
+    if (i >= d.N) return;
+    const double* alp = d.sc + SC_H + (d.K + 1) * (d.K + 1) + (d.K + 1) + 2 * d.K;
+    int m = d.flag[1];
     double x[4];
-    ld(dX[i], x);
+    ld(d.dX[i], x);
     for (int nn = 0; nn <= m; ++nn) {
         double z[4];
-        ld(Z[(long)nn * n + i], z);
+        ld(d.Z[(long)nn * d.N + i], z);
         double a = alp[nn];
 #pragma unroll
         for (int k = 0; k < 4; ++k) x[k] += a * z[k];
     }
-    dX[i] = mk(x);
+    d.dX[i] = mk(x);
+    double xk[4], p[4];
+    ld(d.XK[i], xk);
+#pragma unroll
+    for (int k = 0; k < 4; ++k) xk[k] += x[k];
+    double4 xv = mk(xk);
+    d.XK[i] = xv;
+    d.cons[i] = xv;
+    cons_prim(d.gam1, xk, p);
+    d.prim[i] = mk(p);
 }
 
-// XK += delX, cVar = XK, pVar = consPrim(cVar) (src/timeDiscretization.c:505-520)
-__global__ void k_newton_update(double4* __restrict__ XK, const double4* __restrict__ dX,
-                                double4* __restrict__ cons, double4* __restrict__ prim, long n,
-                                double gam1) {
-    long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
-    double x[4], d[4], p[4];
-    ld(XK[i], x);
-    ld(dX[i], d);
-#pragma unroll
-    for (int k = 0; k < 4; ++k) x[k] += d[k];
-    double4 xv = mk(x);
-    XK[i] = xv;
-    cons[i] = xv;
-    cons_prim(gam1, x, p);
-    prim[i] = mk(p);
+// Newton loop test after an update (src/timeDiscretization.c:478-549)
+__global__ void kb_newton_check(const ImpDev* __restrict__ I) {
+    MEMBER;
+    if (threadIdx.x || !newton_on(d)) return;
+    int inner = ++d.ctl[CTL_INNER];
+    double nk = d.sc[SC_NORM_XK], n0 = d.sc[SC_NORM_X0], eps2loc = d.sc[SC_EPS2LOC];
+    if (!isfinite(nk)) {
+        fail_member(d, CCFD_ERR_STATE, FLAG_STATE);
+        return;
+    }
+    if ((nk > eps2loc * n0) && (inner < d.n_newton)) return;
+    if (inner == d.n_newton) {
+        fail_member(d, CCFD_ERR_NEWTON, FLAG_NEWTON);
+        return;
+    }
+    d.ctl[CTL_NEWTON_TOTAL] += inner;
+    d.ctl[CTL_NEWTON] = 0;
+    d.ctl[CTL_SKIP_NEWTON] = 1;
 }
 
 // ---------------------------------------------------------------- Jacobian
-// perturb (sign +1) or restore (sign 0) variable v of the cells of a colour
-__global__ void k_jac_perturb(double4* __restrict__ prim, const double4* __restrict__ base,
-                              const int* __restrict__ cells, int n, int v, double eps, int add) {
+// gate of colour c: members that build a preconditioner and have colour c
+__global__ void kb_jac_gate(const ImpDev* __restrict__ I, int c) {
+    MEMBER;
+    if (threadIdx.x) return;
+    d.ctl[CTL_SKIP_JAC] = !(newton_on(d) && d.precond && c < d.ncol);
+}
+
+// perturbed copy of the state (buildMatrix works on a copy of pVar)
+__global__ void kb_jac_copy(const ImpDev* __restrict__ I) {
+    MEMBER;
+    if (!newton_on(d) || !d.precond) return;
+    CELL_INDEX;
+    if (i < d.N) d.pert[i] = d.prim[i];
+}
+
+// perturb (add) or restore variable v of the cells of colour c
+__global__ void kb_jac_perturb(const ImpDev* __restrict__ I, int c, int v, int add) {
+    MEMBER;
+    if (d.ctl[CTL_SKIP_JAC]) return;
+    const int off = d.color_off[c], n = d.color_off[c + 1] - off;
     int k = blockIdx.x * blockDim.x + threadIdx.x;
     if (k >= n) return;
-    int d = cells[k];
+    const double reps = sqrt(DBL_EPSILON);
+    int cell = d.color_cells[off + k];
     double q[4];
-    ld(base[d], q);
-    if (add) q[v] += eps;
-    prim[d] = mk(q);
+    ld(d.prim[cell], q);
+    if (add) q[v] += reps;
+    d.pert[cell] = mk(q);
 }
 
 // record column v of the diagonal block of each perturbed cell and of the
 // off-diagonal blocks of its face neighbours (src/linearSolver.c:203-222)
-__global__ void k_jac_collect(const int* __restrict__ cells, int n, int v,
-                              const double4* __restrict__ ut, const double4* __restrict__ rxk,
-                              const int* __restrict__ hs_off, const int* __restrict__ hs_nb,
-                              const int* __restrict__ twin, double* __restrict__ D,
-                              double* __restrict__ O, double sreps) {
+__global__ void kb_jac_collect(const ImpDev* __restrict__ I, int c, int v) {
+    MEMBER;
+    if (d.ctl[CTL_SKIP_JAC]) return;
+    const int off = d.color_off[c], n = d.color_off[c + 1] - off;
     int k = blockIdx.x * blockDim.x + threadIdx.x;
     if (k >= n) return;
-    int d = cells[k];
+    const double sreps = 1.0 / sqrt(DBL_EPSILON);
+    int cell = d.color_cells[off + k];
     double u[4], r[4];
-    ld(ut[d], u);
-    ld(rxk[d], r);
+    ld(d.ut[cell], u);
+    ld(d.RXK[cell], r);
 #pragma unroll
-    for (int j = 0; j < 4; ++j) D[16 * (long)d + 4 * j + v] = 0.0 + (u[j] - r[j]) * sreps;
-    for (int h = hs_off[d]; h < hs_off[d + 1]; ++h) {
-        int e = hs_nb[h];
+    for (int j = 0; j < 4; ++j) d.D[16 * (long)cell + 4 * j + v] = 0.0 + (u[j] - r[j]) * sreps;
+    for (int h = d.hs_off[cell]; h < d.hs_off[cell + 1]; ++h) {
+        int e = d.hs_nb[h];
         if (e < 0) continue;
-        ld(ut[e], u);
-        ld(rxk[e], r);
-        long t = twin[h];
+        ld(d.ut[e], u);
+        ld(d.RXK[e], r);
+        long t = d.twin[h];
 #pragma unroll
-        for (int j = 0; j < 4; ++j) O[16 * t + 4 * j + v] = 0.0 + (u[j] - r[j]) * sreps;
+        for (int j = 0; j < 4; ++j) d.O[16 * t + 4 * j + v] = 0.0 + (u[j] - r[j]) * sreps;
     }
 }
 
@@ -406,50 +588,59 @@ __device__ bool inv4(const double a[16], double r[16]) {
 
 // I - dt J on the stored blocks and the inverses of the diagonal blocks
 // (src/linearSolver.c:226-251)
-__global__ void k_jac_finish(double* __restrict__ D, double* __restrict__ Dinv,
-                             double* __restrict__ O, const int* __restrict__ hs_off, long n,
-                             double dt, int* __restrict__ flag) {
-    long d = (long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (d >= n) return;
+__global__ void kb_jac_finish(const ImpDev* __restrict__ I) {
+    MEMBER;
+    if (!newton_on(d) || !d.precond) return;
+    CELL_INDEX;
+    if (i >= d.N) return;
+    const double dt = d.ctrl->dt;
     double a[16], r[16];
 #pragma unroll
-    for (int k = 0; k < 16; ++k) a[k] = D[16 * d + k] * -dt;
+    for (int k = 0; k < 16; ++k) a[k] = d.D[16 * i + k] * -dt;
 #pragma unroll
     for (int k = 0; k < 4; ++k) a[5 * k] += 1.0;
 #pragma unroll
-    for (int k = 0; k < 16; ++k) D[16 * d + k] = a[k];
+    for (int k = 0; k < 16; ++k) d.D[16 * i + k] = a[k];
     if (!inv4(a, r)) {
-        atomicOr(&flag[2], 1);
+        atomicOr(&d.flag[2], 1);
 #pragma unroll
         for (int k = 0; k < 16; ++k) r[k] = 0.0;
     }
 #pragma unroll
-    for (int k = 0; k < 16; ++k) Dinv[16 * d + k] = r[k];
-    for (long h = hs_off[d]; h < hs_off[d + 1]; ++h)
+    for (int k = 0; k < 16; ++k) d.Dinv[16 * i + k] = r[k];
+    for (long h = d.hs_off[i]; h < d.hs_off[i + 1]; ++h)
 #pragma unroll
-        for (int k = 0; k < 16; ++k) O[16 * h + k] = O[16 * h + k] * -dt;
+        for (int k = 0; k < 16; ++k) d.O[16 * h + k] = d.O[16 * h + k] * -dt;
+}
+
+// a singular diagonal block ends the member's step
+// (src/linearSolver.c:245-249)
+__global__ void kb_jac_check(const ImpDev* __restrict__ I) {
+    MEMBER;
+    if (threadIdx.x || !newton_on(d) || !d.precond) return;
+    if (d.flag[2]) fail_member(d, CCFD_ERR_SINGULAR, FLAG_SINGULAR);
 }
 
 // ---------------------------------------------------------------- LU-SGS
-// One CTA walks the levels of the forward sweep (lower neighbours), then
-// the backward sweep (upper neighbours) (src/linearSolver.c:261-333).
-__global__ void __launch_bounds__(1024) k_lusgs(
-    const double4* __restrict__ B, double4* __restrict__ dxs, double4* __restrict__ dx,
-    const double* __restrict__ Dinv, const double* __restrict__ O, int nlf,
-    const int* __restrict__ lf_off, const int* __restrict__ lf_cells, int nlb,
-    const int* __restrict__ lb_off, const int* __restrict__ lb_cells,
-    const int* __restrict__ lo_off, const int* __restrict__ lo_nb, const int* __restrict__ lo_h,
-    const int* __restrict__ up_off, const int* __restrict__ up_nb, const int* __restrict__ up_h,
-    const int* __restrict__ skip) {
-    if (skip[0]) return;
-    for (int L = 0; L < nlf; ++L) {
-        for (int k = lf_off[L] + threadIdx.x; k < lf_off[L + 1]; k += blockDim.x) {
-            int i = lf_cells[k];
+// One CTA per member walks the levels of the forward sweep (lower
+// neighbours), then the backward sweep (upper neighbours)
+// (src/linearSolver.c:261-333): Z_m = LU-SGS(V_m).
+__global__ void __launch_bounds__(1024) kb_lusgs(const ImpDev* __restrict__ I, int m) {
+    const ImpDev& d = I[blockIdx.x];
+    if (!d.precond || !gmres_on(d)) return;
+    const double4* B = d.V + (long)m * d.N;
+    double4* dxs = d.dxs;
+    double4* dx = d.Z + (long)m * d.N;
+    const double* Dinv = d.Dinv;
+    const double* O = d.O;
+    for (int L = 0; L < d.n_lev_f; ++L) {
+        for (int k = d.lev_f_off[L] + threadIdx.x; k < d.lev_f_off[L + 1]; k += blockDim.x) {
+            int i = d.lev_f_cells[k];
             double t1[4] = {0.0, 0.0, 0.0, 0.0};
-            for (int q = lo_off[i]; q < lo_off[i + 1]; ++q) {
-                const double* blk = O + 16 * (long)lo_h[q];
+            for (int q = d.lo_off[i]; q < d.lo_off[i + 1]; ++q) {
+                const double* blk = O + 16 * (long)d.lo_h[q];
                 double x[4];
-                ld(dxs[lo_nb[q]], x);
+                ld(dxs[d.lo_nb[q]], x);
 #pragma unroll
                 for (int a = 0; a < 4; ++a)
 #pragma unroll
@@ -468,14 +659,14 @@ __global__ void __launch_bounds__(1024) k_lusgs(
         }
         __syncthreads();
     }
-    for (int L = 0; L < nlb; ++L) {
-        for (int k = lb_off[L] + threadIdx.x; k < lb_off[L + 1]; k += blockDim.x) {
-            int i = lb_cells[k];
+    for (int L = 0; L < d.n_lev_b; ++L) {
+        for (int k = d.lev_b_off[L] + threadIdx.x; k < d.lev_b_off[L + 1]; k += blockDim.x) {
+            int i = d.lev_b_cells[k];
             double t1[4] = {0.0, 0.0, 0.0, 0.0};
-            for (int q = up_off[i]; q < up_off[i + 1]; ++q) {
-                const double* blk = O + 16 * (long)up_h[q];
+            for (int q = d.up_off[i]; q < d.up_off[i + 1]; ++q) {
+                const double* blk = O + 16 * (long)d.up_h[q];
                 double x[4];
-                ld(dx[up_nb[q]], x);
+                ld(dx[d.up_nb[q]], x);
 #pragma unroll
                 for (int a = 0; a < 4; ++a)
 #pragma unroll
@@ -495,6 +686,21 @@ __global__ void __launch_bounds__(1024) k_lusgs(
         }
         __syncthreads();
     }
+}
+
+// number of members whose Newton loop (what = 0) / GMRES cycle (what = 1)
+// is still running
+__global__ void kb_count(const ImpDev* __restrict__ I, int n, int what, int* out) {
+    __shared__ int cnt;
+    if (threadIdx.x == 0) cnt = 0;
+    __syncthreads();
+    for (int k = threadIdx.x; k < n; k += blockDim.x) {
+        const ImpDev& d = I[k];
+        int on = what ? gmres_on(d) : newton_on(d);
+        if (on) atomicAdd(&cnt, 1);
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) *out = cnt;
 }
 
 }  // namespace
@@ -537,8 +743,13 @@ static int iupload(ccfd_ctx* ctx, T** p, const std::vector<T>& h) {
 
 // Host set-up: colouring, twins, level schedules (device cell numbering,
 // reference cell order for the sweeps).  Needs the device CSR on the host.
+struct ImpSet;
+static void set_free(ImpSet* M);
+
 void ccfd_implicit_free(ccfd_ctx* ctx) {
-    delete (ImpState*)ctx->implicit_state;
+    ImpState* S = (ImpState*)ctx->implicit_state;
+    if (S && S->solo) set_free((ImpSet*)S->solo);
+    delete S;
     ctx->implicit_state = nullptr;
 }
 
@@ -557,7 +768,8 @@ int ccfd_implicit_setup(ccfd_ctx* ctx, const std::vector<int>& hs_off, const std
         (st = ialloc(ctx, &S->V, (size_t)(K + 1) * N)) || (st = ialloc(ctx, &S->Z, (size_t)K * N)) ||
         (st = ialloc(ctx, &S->ptmp, N)) || (st = ialloc(ctx, &S->ut, N)) ||
         (st = ialloc(ctx, &S->sc, SC_H + (K + 1) * (K + 1) + 4 * (K + 1) + 8)) ||
-        (st = ialloc(ctx, &S->flag, 8)) || (st = ialloc(ctx, &S->partial, S->nb + 1)))
+        (st = ialloc(ctx, &S->flag, 8)) || (st = ialloc(ctx, &S->ctl, CTL_WORDS)) ||
+        (st = ialloc(ctx, &S->partial, S->nb + 1)))
         return st;
     if (ctx->params.precond) {
         if ((st = ialloc(ctx, &S->D, 16 * (size_t)N)) || (st = ialloc(ctx, &S->Dinv, 16 * (size_t)N)) ||
@@ -662,6 +874,7 @@ int ccfd_implicit_setup(ccfd_ctx* ctx, const std::vector<int>& hs_off, const std
         S->n_lev_f = nlf;
         S->n_lev_b = nlb;
         if ((st = iupload(ctx, &S->twin, twin)) || (st = iupload(ctx, &S->color_cells, ccells)) ||
+            (st = iupload(ctx, &S->color_off_d, coff)) ||
             (st = iupload(ctx, &S->lo_off, lo_off)) || (st = iupload(ctx, &S->lo_nb, lo_nb)) ||
             (st = iupload(ctx, &S->lo_h, lo_h)) || (st = iupload(ctx, &S->up_off, up_off)) ||
             (st = iupload(ctx, &S->up_nb, up_nb)) || (st = iupload(ctx, &S->up_h, up_h)) ||
@@ -671,161 +884,293 @@ int ccfd_implicit_setup(ccfd_ctx* ctx, const std::vector<int>& hs_off, const std
     }
     CK(cudaMemsetAsync(S->sc, 0, sizeof(double) * (SC_H + (K + 1) * (K + 1) + 4 * (K + 1) + 8), ctx->stream));
     CK(cudaMemsetAsync(S->flag, 0, sizeof(int) * 8, ctx->stream));
+    CK(cudaMemsetAsync(S->ctl, 0, sizeof(int) * CTL_WORDS, ctx->stream));
     CK(cudaStreamSynchronize(ctx->stream));
     S->ready = true;
     return CCFD_OK;
 }
 
-// residual of the primitive state `prim` at time `time` into `ut` (fused
-// stage kernel in residual mode)
-int ccfd_residual_of(ccfd_ctx* ctx, const double4* prim, double time, double4* ut);
+// ---------------------------------------------------------------- driver
+// A set of implicit members stepped in lockstep on one stream: their device
+// descriptors, and per kernel variant the residual-evaluation launch records
+// (matrix-vector products at t + dt, Newton residuals at t + dt, Jacobian
+// columns at t) over the concatenated tiles of the members.
+struct ImpGroup {
+    int flux, order, ns, fp32;
+    int n_tiles = 0, smem = 0;
+    StageLaunch *rec_mv = nullptr, *rec_nt = nullptr, *rec_jac = nullptr;
+    int2* tmap = nullptr;
+};
 
-static double host_scalar(ccfd_ctx* ctx, const double* p) {
-    double v = 0.0;
-    cudaMemcpyAsync(&v, p, sizeof(double), cudaMemcpyDeviceToHost, ctx->stream);
-    cudaStreamSynchronize(ctx->stream);
-    return v;
+struct ImpSet {
+    std::vector<ccfd_ctx*> members;
+    ImpDev* dev = nullptr;
+    std::vector<ImpGroup> groups;
+    int n = 0, max_nb = 0, max_col = 0, max_colsize = 0, max_K = 0, max_newton = 0;
+    bool any_precond = false;
+    int* d_count = nullptr;
+    int* h_count = nullptr;
+    cudaStream_t stream = nullptr;
+    int last_cuda_error = 0;
+};
+
+static void set_free(ImpSet* M) {
+    if (!M) return;
+    for (auto& g : M->groups) {
+        cudaFree(g.rec_mv);
+        cudaFree(g.rec_nt);
+        cudaFree(g.rec_jac);
+        cudaFree(g.tmap);
+    }
+    if (M->dev) cudaFree(M->dev);
+    if (M->d_count) cudaFree(M->d_count);
+    if (M->h_count) cudaFreeHost(M->h_count);
+    delete M;
 }
 
-// buildMatrix (src/linearSolver.c:186-252) at the current primitive state
-static int build_matrix(ccfd_ctx* ctx, ImpState* S, double t, double dt) {
-    const long N = S->N;
-    double4* base = ctx->prim_buf[ctx->cur];
-    double4* pert = ctx->prim_buf[ctx->cur ^ 1];
-    CK(cudaMemcpyAsync(pert, base, sizeof(double4) * N, cudaMemcpyDeviceToDevice, ctx->stream));
-    const double reps = sqrt(DBL_EPSILON), sreps = 1.0 / reps;
-    const int ncol = (int)S->color_off.size() - 1;
-    for (int c = 0; c < ncol; ++c) {
-        int off = S->color_off[c], n = S->color_off[c + 1] - off;
-        int nb = (n + kB - 1) / kB;
-        for (int v = 0; v < 4; ++v) {
-            k_jac_perturb<<<nb, kB, 0, ctx->stream>>>(pert, base, S->color_cells + off, n, v, reps, 1);
-            int st = ccfd_residual_of(ctx, pert, t, S->ut);
-            if (st) return st;
-            k_jac_collect<<<nb, kB, 0, ctx->stream>>>(S->color_cells + off, n, v, S->ut, S->RXK,
-                                                      ctx->mesh.hs_off, ctx->mesh.hs_nb, S->twin, S->D, S->O,
-                                                      sreps);
-            k_jac_perturb<<<nb, kB, 0, ctx->stream>>>(pert, base, S->color_cells + off, n, v, reps, 0);
-        }
-    }
-    k_jac_finish<<<S->nb, kB, 0, ctx->stream>>>(S->D, S->Dinv, S->O, ctx->mesh.hs_off, N, dt, S->flag);
-    CK(cudaGetLastError());
-    return CCFD_OK;
+#define CKM(x)                              \
+    do {                                    \
+        cudaError_t e_ = (x);               \
+        if (e_ != cudaSuccess) {            \
+            M->last_cuda_error = (int)e_;   \
+            return CCFD_ERR_CUDA;           \
+        }                                   \
+    } while (0)
+
+static ImpDev make_dev(ccfd_ctx* ctx) {
+    ImpState* S = (ImpState*)ctx->implicit_state;
+    ImpDev d;
+    memset(&d, 0, sizeof(d));
+    d.N = S->N;
+    d.K = S->K;
+    d.nb = S->nb;
+    d.precond = ctx->params.precond;
+    d.n_newton = ctx->params.n_newton_iter;
+    d.gam1 = ctx->phys.gam1;
+    d.eps_gmres = ctx->params.eps_gmres;
+    d.eps2newton = ctx->params.eps_newton * ctx->params.eps_newton;
+    d.XK = S->XK; d.Q = S->Q; d.RXK = S->RXK; d.F = S->F; d.dX = S->dX; d.W = S->W;
+    d.V = S->V; d.Z = S->Z; d.ptmp = S->ptmp; d.ut = S->ut; d.dxs = S->dxs;
+    d.cons = ctx->cons0;
+    d.prim = ctx->prim_buf[ctx->cur];
+    d.pert = ctx->prim_buf[ctx->cur ^ 1];
+    d.D = S->D; d.Dinv = S->Dinv; d.O = S->O; d.sc = S->sc; d.partial = S->partial;
+    d.flag = S->flag;
+    d.ctl = S->ctl;
+    d.ctrl = ctx->ctrl;
+    d.hs_off = ctx->mesh.hs_off;
+    d.hs_nb = ctx->mesh.hs_nb;
+    d.twin = S->twin;
+    d.ncol = ctx->params.precond ? (int)S->color_off.size() - 1 : 0;
+    d.color_off = S->color_off_d;
+    d.color_cells = S->color_cells;
+    d.n_lev_f = S->n_lev_f; d.n_lev_b = S->n_lev_b;
+    d.lev_f_off = S->lev_f_off; d.lev_f_cells = S->lev_f_cells;
+    d.lev_b_off = S->lev_b_off; d.lev_b_cells = S->lev_b_cells;
+    d.lo_off = S->lo_off; d.lo_nb = S->lo_nb; d.lo_h = S->lo_h;
+    d.up_off = S->up_off; d.up_nb = S->up_nb; d.up_h = S->up_h;
+    return d;
 }
 
-// GMRES_M (src/linearSolver.c:385-510): B = F_XK, result in S->dX
-static int gmres(ccfd_ctx* ctx, ImpState* S, double time, double t, double dt, double alpha, int* iters) {
-    const long N = S->N;
-    const int K = S->K, nb = S->nb;
-    const double gam1 = ctx->phys.gam1;
-    double* H = S->sc + SC_H;
-    double* gam = H + (K + 1) * (K + 1);
-    double* alp = gam + (K + 1) + 2 * K;
-    int* flag = S->flag;
-    cudaStream_t st = ctx->stream;
-    // abortCrit = epsGMRES * normB; normR0 = normB; gam[0] = normR0
-    double normB = host_scalar(ctx, S->sc + SC_NORMB);
-    double hv[2] = {ctx->params.eps_gmres * normB, normB};
-    CK(cudaMemcpyAsync(S->sc + SC_ABORT, &hv[0], sizeof(double), cudaMemcpyHostToDevice, st));
-    CK(cudaMemcpyAsync(gam, &hv[1], sizeof(double), cudaMemcpyHostToDevice, st));
-    CK(cudaMemsetAsync(flag, 0, sizeof(int) * 4, st));
-    k_gmres_init<<<nb, kB, 0, st>>>(S->F, S->sc, S->V, S->dX, N);
-    if (ctx->params.precond) {
-        int s = build_matrix(ctx, S, t, dt);
-        if (s) return s;
-    }
-    const double adt = alpha * dt;
-    int m = 0;
-    for (m = 0; m < K; ++m) {
-        double4* Vm = S->V + (long)m * N;
-        double4* Zm = S->Z + (long)m * N;
+static int set_build(const std::vector<ccfd_ctx*>& members, cudaStream_t stream, ImpSet** out) {
+    ImpSet* M = new ImpSet();
+    *out = M;
+    M->members = members;
+    M->n = (int)members.size();
+    M->stream = stream;
+    std::vector<ImpDev> hd;
+    std::map<std::tuple<int, int, int, int>, std::vector<int>> by_variant;
+    for (int k = 0; k < M->n; ++k) {
+        ccfd_ctx* ctx = members[k];
+        ImpState* S = (ImpState*)ctx->implicit_state;
+        hd.push_back(make_dev(ctx));
+        M->max_nb = std::max(M->max_nb, S->nb);
+        M->max_K = std::max(M->max_K, S->K);
+        M->max_newton = std::max(M->max_newton, ctx->params.n_newton_iter);
         if (ctx->params.precond) {
-            k_lusgs<<<1, 1024, 0, st>>>(Vm, S->dxs, Zm, S->Dinv, S->O, S->n_lev_f, S->lev_f_off, S->lev_f_cells,
-                                        S->n_lev_b, S->lev_b_off, S->lev_b_cells, S->lo_off, S->lo_nb, S->lo_h,
-                                        S->up_off, S->up_nb, S->up_h, flag);
-        } else {
-            k_copy<<<nb, kB, 0, st>>>(Zm, Vm, N);
+            M->any_precond = true;
+            int ncol = (int)S->color_off.size() - 1;
+            M->max_col = std::max(M->max_col, ncol);
+            for (int c = 0; c < ncol; ++c)
+                M->max_colsize = std::max(M->max_colsize, S->color_off[c + 1] - S->color_off[c]);
         }
-        // matrixVector: epsFD = sqrt(eps) / |Z|
-        k_dot<<<nb, kB, 0, st>>>(Zm, Zm, N, S->partial, flag);
-        k_final<<<1, kB, 0, st>>>(S->partial, nb, S->sc + SC_EPSFD, 2, flag);
-        k_mv_prep<<<nb, kB, 0, st>>>(S->XK, Zm, S->sc, S->ptmp, N, gam1, flag);
-        int s = ccfd_residual_of(ctx, S->ptmp, time, S->ut);
-        if (s) return s;
-        k_mv_finish<<<nb, kB, 0, st>>>(Zm, S->ut, S->RXK, S->sc, adt, S->W, S->V, N, S->partial, flag);
-        // modified Gram-Schmidt
-        for (int nn = 0; nn <= m; ++nn) {
-            double* hnm = H + nn * (K + 1) + m;
-            k_final<<<1, kB, 0, st>>>(S->partial, nb, hnm, 0, flag);
-            const double4* Vnext = nn < m ? S->V + (long)(nn + 1) * N : nullptr;
-            k_mgs<<<nb, kB, 0, st>>>(S->W, S->V + (long)nn * N, hnm, Vnext, N, S->partial, flag);
-        }
-        double* hm1 = H + (m + 1) * (K + 1) + m;
-        k_final<<<1, kB, 0, st>>>(S->partial, nb, hm1, 1, flag);
-        k_givens<<<1, 1, 0, st>>>(S->sc, flag, m, K);
-        k_vnext<<<nb, kB, 0, st>>>(S->W, hm1, S->V + (long)(m + 1) * N, N, flag);
-        CK(cudaGetLastError());
-        int hf[4];
-        CK(cudaMemcpyAsync(hf, flag, sizeof(int) * 4, cudaMemcpyDeviceToHost, st));
-        CK(cudaStreamSynchronize(st));
-        if (hf[2]) return CCFD_ERR_SINGULAR;
-        if (hf[0]) {
-            if (hf[3]) return CCFD_ERR_GMRES;
-            break;
-        }
+        StageLaunch probe;
+        ccfd_fill_stage(ctx, probe);
+        by_variant[std::make_tuple(probe.flux_id, probe.order, probe.ns, probe.fp32)].push_back(k);
     }
-    k_delx<<<nb, kB, 0, st>>>(S->dX, S->Z, alp, flag, N);
-    CK(cudaGetLastError());
-    *iters = std::min(m, K - 1) + 1;
+    CKM(cudaMalloc(&M->dev, sizeof(ImpDev) * M->n));
+    CKM(cudaMemcpyAsync(M->dev, hd.data(), sizeof(ImpDev) * M->n, cudaMemcpyHostToDevice, stream));
+    CKM(cudaMalloc(&M->d_count, sizeof(int)));
+    CKM(cudaMallocHost(&M->h_count, sizeof(int)));
+    for (auto& kv : by_variant) {
+        ImpGroup g;
+        std::tie(g.flux, g.order, g.ns, g.fp32) = kv.first;
+        const std::vector<int>& idx = kv.second;
+        std::vector<StageLaunch> mv(idx.size()), nt(idx.size()), jac(idx.size());
+        std::vector<int2> tmap;
+        TileDev big;
+        memset(&big, 0, sizeof(big));
+        for (size_t j = 0; j < idx.size(); ++j) {
+            ccfd_ctx* ctx = members[idx[j]];
+            ImpState* S = (ImpState*)ctx->implicit_state;
+            StageLaunch L;
+            ccfd_fill_stage(ctx, L);
+            L.ctrl = ctx->ctrl;
+            L.mode = 0;
+            L.res_partial = ctx->res_partial;
+            // matrix-vector product: R(XK + eps Z_m) at t + dt
+            L.a_time = 1.0;
+            L.prim_in = S->ptmp;
+            L.u_t = S->ut;
+            L.skip = S->ctl + CTL_SKIP_GMRES;
+            mv[j] = L;
+            // Newton residual R(XK) at t + dt
+            L.prim_in = ctx->prim_buf[ctx->cur];
+            L.u_t = S->RXK;
+            L.skip = S->ctl + CTL_SKIP_NEWTON;
+            nt[j] = L;
+            // Jacobian columns at t
+            L.a_time = 0.0;
+            L.prim_in = ctx->prim_buf[ctx->cur ^ 1];
+            L.u_t = S->ut;
+            L.skip = S->ctl + CTL_SKIP_JAC;
+            jac[j] = L;
+            for (int t = 0; t < ctx->tiles.n_tiles; ++t) tmap.push_back(make_int2((int)j, t));
+            big.max_e = std::max(big.max_e, ctx->tiles.max_e);
+            big.max_g = std::max(big.max_g, ctx->tiles.max_g);
+            big.max_hs = std::max(big.max_hs, ctx->tiles.max_hs);
+            big.max_f = std::max(big.max_f, ctx->tiles.max_f);
+        }
+        g.n_tiles = (int)tmap.size();
+        g.smem = stage_smem_bytes(big, g.fp32);
+        size_t rb = sizeof(StageLaunch) * idx.size();
+        CKM(cudaMalloc(&g.rec_mv, rb));
+        CKM(cudaMalloc(&g.rec_nt, rb));
+        CKM(cudaMalloc(&g.rec_jac, rb));
+        CKM(cudaMalloc(&g.tmap, sizeof(int2) * tmap.size()));
+        CKM(cudaMemcpyAsync(g.rec_mv, mv.data(), rb, cudaMemcpyHostToDevice, stream));
+        CKM(cudaMemcpyAsync(g.rec_nt, nt.data(), rb, cudaMemcpyHostToDevice, stream));
+        CKM(cudaMemcpyAsync(g.rec_jac, jac.data(), rb, cudaMemcpyHostToDevice, stream));
+        CKM(cudaMemcpyAsync(g.tmap, tmap.data(), sizeof(int2) * tmap.size(), cudaMemcpyHostToDevice, stream));
+        M->groups.push_back(g);
+    }
+    CKM(cudaStreamSynchronize(stream));
     return CCFD_OK;
 }
 
-static int finish_partial(ccfd_ctx* ctx, ImpState* S, double* out, int mode) {
-    k_final<<<1, kB, 0, ctx->stream>>>(S->partial, S->nb, out, mode, nullptr);
-    CK(cudaGetLastError());
+enum RecKind { REC_MV, REC_NT, REC_JAC };
+
+static void residuals(ImpSet* M, RecKind kind) {
+    for (auto& g : M->groups) {
+        BatchLaunch B;
+        B.recs = kind == REC_MV ? g.rec_mv : kind == REC_NT ? g.rec_nt : g.rec_jac;
+        B.tmap = g.tmap;
+        B.n_tiles = g.n_tiles;
+        B.smem_bytes = g.smem;
+        B.rk_mode = 0;
+        B.stage = 0;
+        B.flux_id = g.flux;
+        B.order = g.order;
+        B.ns = g.ns;
+        B.fp32 = g.fp32;
+        launch_stage_batch(B, M->stream);
+    }
+}
+
+static int count_on(ImpSet* M, int what, int* out) {
+    kb_count<<<1, 256, 0, M->stream>>>(M->dev, M->n, what, M->d_count);
+    CKM(cudaMemcpyAsync(M->h_count, M->d_count, sizeof(int), cudaMemcpyDeviceToHost, M->stream));
+    CKM(cudaStreamSynchronize(M->stream));
+    *out = *M->h_count;
     return CCFD_OK;
 }
 
-// one implicitTimeStep (src/timeDiscretization.c:412-552) at ctrl->t, ctrl->dt
-static int implicit_step(ccfd_ctx* ctx, ImpState* S) {
-    const long N = S->N;
-    const int nb = S->nb;
-    cudaStream_t st = ctx->stream;
-    const double gam1 = ctx->phys.gam1;
-    const ccfd_params& p = ctx->params;
-    Ctrl& c = *ctx->h_ctrl;
-    const double t = c.t, dt = c.dt, alpha = 1.0, beta = 1.0;
-    double4* prim = ctx->prim_buf[ctx->cur];
-    // Q = cVar; pVar = consPrim(cVar)
-    k_copy<<<nb, kB, 0, st>>>(S->Q, ctx->cons0, N);
-    k_cons2prim<<<nb, kB, 0, st>>>(ctx->cons0, prim, N, gam1);
-    const double time = t + beta * dt;
-    int s = ccfd_residual_of(ctx, prim, time, S->RXK);
-    if (s) return s;
-    k_newton_F<<<nb, kB, 0, st>>>(ctx->cons0, S->Q, S->RXK, alpha * dt, S->F, N, S->partial);
-    k_copy<<<nb, kB, 0, st>>>(S->XK, ctx->cons0, N);
-    if ((s = finish_partial(ctx, S, S->sc + SC_NORM_X0, 0))) return s;
-    const double eps2newton = p.eps_newton * p.eps_newton;
-    double n0 = host_scalar(ctx, S->sc + SC_NORM_X0);
-    double eps2loc = fmax(1e-8 * 1e-8 * N * eps2newton / n0, eps2newton);
-    double nk = n0;
-    int inner = 0;
-    while ((nk > eps2loc * n0) && (inner < p.n_newton_iter)) {
-        inner++;
-        double nb_ = sqrt(nk);
-        CK(cudaMemcpyAsync(S->sc + SC_NORMB, &nb_, sizeof(double), cudaMemcpyHostToDevice, st));
-        int it = 0;
-        if ((s = gmres(ctx, S, time, t, dt, alpha, &it))) return s;
-        ctx->gmres_total += it;
-        k_newton_update<<<nb, kB, 0, st>>>(S->XK, S->dX, ctx->cons0, prim, N, gam1);
-        if ((s = ccfd_residual_of(ctx, prim, time, S->RXK))) return s;
-        k_newton_F<<<nb, kB, 0, st>>>(ctx->cons0, S->Q, S->RXK, alpha * dt, S->F, N, S->partial);
-        if ((s = finish_partial(ctx, S, S->sc + SC_NORM_XK, 0))) return s;
-        nk = host_scalar(ctx, S->sc + SC_NORM_XK);
-        if (!isfinite(nk)) return CCFD_ERR_STATE;
+// One implicitTimeStep (src/timeDiscretization.c:412-552) of every member
+// whose control block lets it step, in lockstep.
+static int set_step(ImpSet* M) {
+    cudaStream_t st = M->stream;
+    const dim3 gv(M->max_nb, M->n), g1(1, M->n);
+    kb_step_prepare<<<g1, 32, 0, st>>>(M->dev);
+    kb_step_begin<<<gv, kB, 0, st>>>(M->dev);
+    residuals(M, REC_NT);
+    kb_newton_F<<<gv, kB, 0, st>>>(M->dev, 1);
+    kb_final<<<g1, kB, 0, st>>>(M->dev, FT_NORM_X0, 0, 0, 0, 0);
+    kb_newton_start<<<g1, 32, 0, st>>>(M->dev);
+    CKM(cudaGetLastError());
+    for (int it = 0; it < M->max_newton; ++it) {
+        int on = 0, s;
+        if ((s = count_on(M, 0, &on))) return s;
+        if (!on) break;
+        // GMRES_M (src/linearSolver.c:385-510)
+        kb_gmres_init<<<gv, kB, 0, st>>>(M->dev);
+        kb_gmres_flags<<<g1, 32, 0, st>>>(M->dev);
+        if (M->any_precond) {
+            // buildMatrix (src/linearSolver.c:186-252)
+            kb_jac_copy<<<gv, kB, 0, st>>>(M->dev);
+            const dim3 gc((M->max_colsize + kB - 1) / kB, M->n);
+            for (int c = 0; c < M->max_col; ++c) {
+                kb_jac_gate<<<g1, 32, 0, st>>>(M->dev, c);
+                for (int v = 0; v < 4; ++v) {
+                    kb_jac_perturb<<<gc, kB, 0, st>>>(M->dev, c, v, 1);
+                    residuals(M, REC_JAC);
+                    kb_jac_collect<<<gc, kB, 0, st>>>(M->dev, c, v);
+                    kb_jac_perturb<<<gc, kB, 0, st>>>(M->dev, c, v, 0);
+                }
+            }
+            kb_jac_finish<<<gv, kB, 0, st>>>(M->dev);
+            kb_jac_check<<<g1, 32, 0, st>>>(M->dev);
+        }
+        for (int m = 0; m < M->max_K; ++m) {
+            if (M->any_precond) kb_lusgs<<<M->n, 1024, 0, st>>>(M->dev, m);
+            kb_copy_vz<<<gv, kB, 0, st>>>(M->dev, m);
+            // matrixVector: epsFD = sqrt(eps) / |Z|
+            kb_dot_zz<<<gv, kB, 0, st>>>(M->dev, m);
+            kb_final<<<g1, kB, 0, st>>>(M->dev, FT_EPSFD, 0, 0, 2, 1);
+            kb_mv_prep<<<gv, kB, 0, st>>>(M->dev, m);
+            residuals(M, REC_MV);
+            kb_mv_finish<<<gv, kB, 0, st>>>(M->dev, m);
+            // modified Gram-Schmidt
+            for (int nn = 0; nn <= m; ++nn) {
+                kb_final<<<g1, kB, 0, st>>>(M->dev, FT_H, nn, m, 0, 1);
+                kb_mgs<<<gv, kB, 0, st>>>(M->dev, nn, m);
+            }
+            kb_final<<<g1, kB, 0, st>>>(M->dev, FT_H, m + 1, m, 1, 1);
+            kb_givens<<<g1, 32, 0, st>>>(M->dev, m);
+            kb_vnext<<<gv, kB, 0, st>>>(M->dev, m);
+            CKM(cudaGetLastError());
+            if ((s = count_on(M, 1, &on))) return s;
+            if (!on) break;
+        }
+        kb_gmres_end<<<g1, 32, 0, st>>>(M->dev);
+        kb_newton_update<<<gv, kB, 0, st>>>(M->dev);
+        residuals(M, REC_NT);
+        kb_newton_F<<<gv, kB, 0, st>>>(M->dev, 0);
+        kb_final<<<g1, kB, 0, st>>>(M->dev, FT_NORM_XK, 0, 0, 0, 0);
+        kb_newton_check<<<g1, 32, 0, st>>>(M->dev);
+        CKM(cudaGetLastError());
     }
-    ctx->newton_total += inner;
-    if (inner == p.n_newton_iter) return CCFD_ERR_NEWTON;
+    // global residual of the final residual evaluation, stop tests and the
+    // next dt (calcTimeStep of the new state) of the members that stepped
+    for (ccfd_ctx* ctx : M->members) {
+        launch_dt(ctx->mesh, ctx->phys, nullptr, ctx->sp, ctx->prim_buf[ctx->cur], ctx->dt_partial, ctx->dt_bad,
+                  st);
+        imp_step_end_launch(ctx->ctrl, ctx->sp, ctx->res_partial, ctx->tiles.n_tiles, ctx->dt_partial,
+                            ctx->dt_bad, ctx->nb_cells, ctx->wall_ghost, ctx->wall_nl, ctx->ghost_pface, st);
+    }
+    CKM(cudaGetLastError());
+    return CCFD_OK;
+}
+
+// iteration counters of the members into their contexts (reports)
+static int set_pull_counts(ImpSet* M) {
+    for (ccfd_ctx* ctx : M->members) {
+        ImpState* S = (ImpState*)ctx->implicit_state;
+        int ctl[CTL_WORDS];
+        CKM(cudaMemcpyAsync(ctl, S->ctl, sizeof(ctl), cudaMemcpyDeviceToHost, M->stream));
+        CKM(cudaStreamSynchronize(M->stream));
+        ctx->newton_total = ctl[CTL_NEWTON_TOTAL];
+        ctx->gmres_total = ctl[CTL_GMRES_TOTAL];
+    }
     return CCFD_OK;
 }
 
@@ -834,6 +1179,14 @@ static int run_implicit(ccfd_ctx* ctx, long nsteps, ccfd_report* report) {
     ImpState* S = (ImpState*)ctx->implicit_state;
     if (!S || !S->ready) return CCFD_ERR_ARG;
     cudaStream_t st = ctx->stream;
+    int s;
+    if (!S->solo) {
+        ImpSet* M = nullptr;
+        s = set_build({ctx}, st, &M);
+        S->solo = M;
+        if (s) return s;
+    }
+    ImpSet* M = (ImpSet*)S->solo;
     CK(cudaMemcpyAsync(ctx->h_ctrl, ctx->ctrl, sizeof(Ctrl), cudaMemcpyDeviceToHost, st));
     CK(cudaStreamSynchronize(st));
     Ctrl& c = *ctx->h_ctrl;
@@ -842,46 +1195,44 @@ static int run_implicit(ccfd_ctx* ctx, long nsteps, ccfd_report* report) {
     c.stop_at = stop_at;
     CK(cudaMemcpyAsync(&ctx->ctrl->stop_at, &c.stop_at, sizeof(long long), cudaMemcpyHostToDevice, st));
     CK(cudaEventRecord(ctx->ev_run0, st));
-    int status = CCFD_OK;
-    double4* prim = ctx->prim_buf[ctx->cur];
-    launch_dt(ctx->mesh, ctx->phys, ctx->ctrl, ctx->sp, prim, ctx->dt_partial, ctx->dt_bad, st);
+    launch_dt(ctx->mesh, ctx->phys, ctx->ctrl, ctx->sp, ctx->prim_buf[ctx->cur], ctx->dt_partial, ctx->dt_bad, st);
     launch_step_begin(ctx->ctrl, ctx->sp, ctx->dt_partial, ctx->dt_bad, ctx->nb_cells, st);
     CK(cudaMemcpyAsync(ctx->h_ctrl, ctx->ctrl, sizeof(Ctrl), cudaMemcpyDeviceToHost, st));
     CK(cudaStreamSynchronize(st));
+    int status = CCFD_OK;
+    int ctl_status = 0;
     while (!c.done && c.active && c.iter < stop_at) {
-        status = implicit_step(ctx, S);
-        if (status) break;
-        // global residual of the final residual evaluation, stop tests and
-        // the next dt (calcTimeStep of the new state)
-        launch_dt(ctx->mesh, ctx->phys, nullptr, ctx->sp, prim, ctx->dt_partial, ctx->dt_bad, st);
-        imp_step_end_launch(ctx->ctrl, ctx->sp, ctx->res_partial, ctx->tiles.n_tiles, ctx->dt_partial,
-                            ctx->dt_bad, ctx->nb_cells, ctx->wall_ghost, ctx->wall_nl, ctx->ghost_pface, st);
-        CK(cudaGetLastError());
+        if ((status = set_step(M))) break;
         CK(cudaMemcpyAsync(ctx->h_ctrl, ctx->ctrl, sizeof(Ctrl), cudaMemcpyDeviceToHost, st));
+        CK(cudaMemcpyAsync(&ctl_status, S->ctl + CTL_STATUS, sizeof(int), cudaMemcpyDeviceToHost, st));
         CK(cudaStreamSynchronize(st));
+        if (ctl_status) {
+            status = ctl_status;
+            break;
+        }
     }
     CK(cudaEventRecord(ctx->ev_run1, st));
     CK(cudaEventSynchronize(ctx->ev_run1));
     float run_ms = 0.0f;
     CK(cudaEventElapsedTime(&run_ms, ctx->ev_run0, ctx->ev_run1));
+    if ((s = set_pull_counts(M))) return s;
     CK(cudaMemcpyAsync(ctx->h_ctrl, ctx->ctrl, sizeof(Ctrl), cudaMemcpyDeviceToHost, st));
     CK(cudaStreamSynchronize(st));
     if (report) {
-        memset(report, 0, sizeof(*report));
-        report->t = c.t;
-        report->dt = c.dt;
-        report->iterations = c.iter;
-        for (int v = 0; v < 6; ++v) report->residual[v] = c.res[v];
-        for (int v = 0; v < 4; ++v) report->first_residual[v] = c.res_first[v];
-        report->cl = c.cl;
-        report->cd = c.cd;
-        report->converged = c.converged;
-        report->finished = c.finished;
-        report->newton_iterations = ctx->newton_total;
-        report->gmres_iterations = ctx->gmres_total;
+        ccfd_fill_report(ctx, report);
+        report->status = status ? status : report->status;
         report->device_ms = run_ms;
     }
-    if (status) return status;
+    if (status) {
+        // a failed step leaves the context usable: clear the stop flags the
+        // device raised for it, as the single-case driver always did
+        c.done = 0;
+        c.active = 0;
+        c.flags = 0;
+        CK(cudaMemcpyAsync(ctx->ctrl, &c, sizeof(Ctrl), cudaMemcpyHostToDevice, st));
+        CK(cudaStreamSynchronize(st));
+        return status;
+    }
     if (c.flags & FLAG_DT) return CCFD_ERR_DT;
     if (c.flags & FLAG_STATE) return CCFD_ERR_STATE;
     return CCFD_OK;
@@ -894,39 +1245,68 @@ extern "C" int ccfd_run_implicit(ccfd_ctx* ctx, long nsteps, ccfd_report* report
 }
 
 // ---------------------------------------------------------------- batching
-// Implicit batch members are stepped one after another by the
-// single-instance driver, each within its own step budget; the batch stream
-// is idle meanwhile (the member's own stream carries the work).
-int ccfd_implicit_batch_join(ccfd_batch*, ccfd_ctx* ctx) {
+// The implicit members of a batch form one lockstep set on the batch stream
+// (rebuilt when the membership changes).
+struct BatchImp {
+    ImpSet* set = nullptr;
+    std::vector<ccfd_ctx*> key;
+};
+static std::map<const ccfd_batch*, BatchImp> g_batch_imp;
+
+cudaStream_t ccfd_batch_stream(ccfd_batch* b);
+
+int ccfd_implicit_batch_join(ccfd_batch* b, ccfd_ctx* ctx) {
     ImpState* S = (ImpState*)ctx->implicit_state;
-    return (S && S->ready) ? CCFD_OK : CCFD_ERR_ARG;
+    if (!S || !S->ready) return CCFD_ERR_ARG;
+    cudaStream_t st = ccfd_batch_stream(b);
+    launch_dt(ctx->mesh, ctx->phys, ctx->ctrl, ctx->sp, ctx->prim_buf[ctx->cur], ctx->dt_partial, ctx->dt_bad, st);
+    launch_step_begin(ctx->ctrl, ctx->sp, ctx->dt_partial, ctx->dt_bad, ctx->nb_cells, st);
+    CK(cudaGetLastError());
+    CK(cudaStreamSynchronize(st));
+    return CCFD_OK;
 }
 
-int ccfd_implicit_batch_leave(ccfd_batch*, ccfd_ctx*) { return CCFD_OK; }
-
-int ccfd_implicit_batch_steps(ccfd_batch*, const std::vector<ccfd_ctx*>& members, int steps) {
-    for (ccfd_ctx* ctx : members) {
-        Ctrl& c = *ctx->h_ctrl;
-        CK(cudaMemcpy(&c, ctx->ctrl, sizeof(Ctrl), cudaMemcpyDeviceToHost));
-        if (c.done || c.iter >= c.stop_at) continue;
-        long long budget = c.stop_at;
-        long n = (long)std::min<long long>(steps, budget - c.iter);
-        int st = run_implicit(ctx, n, nullptr);
-        // restore the member's own budget (the driver set stop_at for this call)
-        CK(cudaMemcpy(&ctx->ctrl->stop_at, &budget, sizeof(long long), cudaMemcpyHostToDevice));
-        if (st && st != CCFD_ERR_NEWTON && st != CCFD_ERR_SINGULAR && st != CCFD_ERR_GMRES &&
-            st != CCFD_ERR_STATE && st != CCFD_ERR_DT)
-            return st;
-        if (st) {
-            // a failed member stops; its status stays readable in its report
-            unsigned f = st == CCFD_ERR_NEWTON ? FLAG_NEWTON : st == CCFD_ERR_SINGULAR ? FLAG_SINGULAR
-                       : st == CCFD_ERR_GMRES ? FLAG_GMRES : st == CCFD_ERR_DT ? FLAG_DT : FLAG_STATE;
-            CK(cudaMemcpy(&c, ctx->ctrl, sizeof(Ctrl), cudaMemcpyDeviceToHost));
-            c.flags |= f;
-            c.done = 1;
-            c.active = 0;
-            CK(cudaMemcpy(ctx->ctrl, &c, sizeof(Ctrl), cudaMemcpyHostToDevice));
+int ccfd_implicit_batch_leave(ccfd_batch* b, ccfd_ctx* ctx) {
+    auto it = g_batch_imp.find(b);
+    if (it != g_batch_imp.end()) {
+        if (it->second.set) {
+            set_pull_counts(it->second.set);
+            set_free(it->second.set);
         }
+        g_batch_imp.erase(it);
     }
+    (void)ctx;
     return CCFD_OK;
+}
+
+void ccfd_implicit_batch_release(ccfd_batch* b) {
+    auto it = g_batch_imp.find(b);
+    if (it == g_batch_imp.end()) return;
+    if (it->second.set) set_free(it->second.set);
+    g_batch_imp.erase(it);
+}
+
+int ccfd_implicit_batch_steps(ccfd_batch* b, const std::vector<ccfd_ctx*>& members, int steps) {
+    BatchImp& bi = g_batch_imp[b];
+    if (bi.key != members) {
+        if (bi.set) set_free(bi.set);
+        bi.set = nullptr;
+        bi.key = members;
+        int s = set_build(members, ccfd_batch_stream(b), &bi.set);
+        if (s) return s;
+    }
+    ImpSet* M = bi.set;
+    for (int k = 0; k < steps; ++k) {
+        // members that can still step
+        int any = 0;
+        for (ccfd_ctx* ctx : members) {
+            CKM(cudaMemcpyAsync(ctx->h_ctrl, ctx->ctrl, sizeof(Ctrl), cudaMemcpyDeviceToHost, M->stream));
+        }
+        CKM(cudaStreamSynchronize(M->stream));
+        for (ccfd_ctx* ctx : members) any |= ctx->h_ctrl->active && !ctx->h_ctrl->done;
+        if (!any) break;
+        int s = set_step(M);
+        if (s) return s;
+    }
+    return set_pull_counts(M);
 }
