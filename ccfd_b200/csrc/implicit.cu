@@ -52,6 +52,7 @@ using namespace ccfd;
 namespace {
 
 constexpr int kB = 256;  // threads per block of the vector kernels
+constexpr int kSweepThreads = 512;  // threads of the LU-SGS CTA (one per member), 4 per cell
 
 // device scalars of one implicit step (offsets into ImpState::sc)
 enum Sc {
@@ -86,8 +87,11 @@ struct ImpDev {
     int ncol;
     const int *color_off, *color_cells;
     int n_lev_f, n_lev_b;
-    const int *lev_f_off, *lev_f_cells, *lev_b_off, *lev_b_cells;
-    const int *lo_off, *lo_nb, *lo_h, *up_off, *up_nb, *up_h;
+    // sweeps in level order: level offsets; per position the cell, its
+    // lower (forward) / upper (backward) neighbours and the half-sides of
+    // their off-diagonal blocks in side order, -1 padded to four
+    const int *lev_f_off, *fw_cell, *lev_b_off, *bw_cell;
+    const int4 *fw_nb, *fw_h, *bw_nb, *bw_h;
 };
 
 struct ImpState {
@@ -109,9 +113,8 @@ struct ImpState {
     int* twin = nullptr;         // [H] half-side of the neighbour that points back
     // LU-SGS level schedules
     int n_lev_f = 0, n_lev_b = 0;
-    int *lev_f_off = nullptr, *lev_f_cells = nullptr, *lev_b_off = nullptr, *lev_b_cells = nullptr;
-    int *lo_off = nullptr, *lo_nb = nullptr, *lo_h = nullptr;
-    int *up_off = nullptr, *up_nb = nullptr, *up_h = nullptr;
+    int *lev_f_off = nullptr, *fw_cell = nullptr, *lev_b_off = nullptr, *bw_cell = nullptr;
+    int4 *fw_nb = nullptr, *fw_h = nullptr, *bw_nb = nullptr, *bw_h = nullptr;
     bool ready = false;
     void* solo = nullptr;        // the member set of this context running alone
 };
@@ -622,70 +625,120 @@ __global__ void kb_jac_check(const ImpDev* __restrict__ I) {
 }
 
 // ---------------------------------------------------------------- LU-SGS
-// One CTA per member walks the levels of the forward sweep (lower
-// neighbours), then the backward sweep (upper neighbours)
+// Four consecutive threads treat one cell of a level, thread a its row a:
+// forward  dxs_i = Dinv_i (b_i - sum_lower O_ij dxs_j)
+// backward dx_i  = dxs_i - Dinv_i (sum_upper O_ij dx_j)
+// Row a of the neighbour sum accumulates the neighbours in side order and
+// the columns in order, exactly as the reference's loops do; the four rows
+// are exchanged by shuffles for the product with Dinv_i.  All loads of a
+// cell depend only on its indices (prefetched one level ahead) and on
+// results of earlier levels, so they are issued together.
+template <bool FWD>
+__device__ __forceinline__ void sweep_row(int i, int4 nb, int4 hh, int a, unsigned mask, int lane0,
+                                          const double* __restrict__ B, const double* src, double* dst,
+                                          const double* dxs, const double* __restrict__ Dinv,
+                                          const double* __restrict__ O) {
+    const int nbv[4] = {nb.x, nb.y, nb.z, nb.w};
+    const int hv[4] = {hh.x, hh.y, hh.z, hh.w};
+    // component a of each neighbour state and row a of each block
+    double xa[4];
+    double4 orow[4];
+#pragma unroll
+    for (int q = 0; q < 4; ++q)
+        if (nbv[q] >= 0) {
+            xa[q] = src[4 * (long)nbv[q] + a];
+            orow[q] = reinterpret_cast<const double4*>(O + 16 * (long)hv[q])[a];
+        }
+    const double4 drow = reinterpret_cast<const double4*>(Dinv + 16 * (long)i)[a];
+    const double own_a = FWD ? B[4 * (long)i + a] : dxs[4 * (long)i + a];
+    double t1a = 0.0;
+#pragma unroll
+    for (int q = 0; q < 4; ++q)
+        if (nbv[q] >= 0) {
+            double o[4];
+            ld(orow[q], o);
+#pragma unroll
+            for (int b = 0; b < 4; ++b) t1a += o[b] * __shfl_sync(mask, xa[q], lane0 + b);
+        }
+    double di[4];
+    ld(drow, di);
+    double t2 = 0.0;
+    if (FWD) {
+#pragma unroll
+        for (int c = 0; c < 4; ++c)
+            t2 += di[c] * (__shfl_sync(mask, own_a, lane0 + c) - __shfl_sync(mask, t1a, lane0 + c));
+        dst[4 * (long)i + a] = t2;
+    } else {
+#pragma unroll
+        for (int c = 0; c < 4; ++c) t2 += di[c] * __shfl_sync(mask, t1a, lane0 + c);
+        dst[4 * (long)i + a] = own_a - t2;
+    }
+}
+
+template <bool FWD>
+__device__ __forceinline__ void sweep(int nl, const int* __restrict__ off, const int* __restrict__ cell,
+                                      const int4* __restrict__ nbs, const int4* __restrict__ hs,
+                                      const double* __restrict__ B, const double* src, double* dst,
+                                      const double* dxs, const double* __restrict__ Dinv,
+                                      const double* __restrict__ O) {
+    // the cell count per pass is a multiple of 8, so the four threads of a
+    // cell always sit in one aligned quarter of a warp
+    const int g = threadIdx.x >> 2, a = threadIdx.x & 3, ng = blockDim.x >> 2;
+    const int lane0 = (threadIdx.x & 31) & ~3;
+    const unsigned mask = 0xfu << lane0;
+    int p = nl > 0 ? off[0] + g : 0;
+    int end = nl > 0 ? off[1] : 0;
+    bool have = p < end;
+    int ci = 0;
+    int4 nb = make_int4(-1, -1, -1, -1), hh = nb;
+    if (have) {
+        ci = cell[p];
+        nb = nbs[p];
+        hh = hs[p];
+    }
+    for (int L = 0; L < nl; ++L) {
+        // prefetch the first position of the next level
+        const int nend = L + 1 < nl ? off[L + 2] : end;
+        const int np = end + g;
+        const bool nhave = L + 1 < nl && np < nend;
+        int nci = 0;
+        int4 nnb = make_int4(-1, -1, -1, -1), nhh = nnb;
+        if (nhave) {
+            nci = cell[np];
+            nnb = nbs[np];
+            nhh = hs[np];
+        }
+        if (have) {
+            int q = p;
+            while (true) {
+                sweep_row<FWD>(ci, nb, hh, a, mask, lane0, B, src, dst, dxs, Dinv, O);
+                q += ng;
+                if (q >= end) break;
+                ci = cell[q];
+                nb = nbs[q];
+                hh = hs[q];
+            }
+        }
+        __syncthreads();
+        p = np;
+        end = nend;
+        have = nhave;
+        ci = nci;
+        nb = nnb;
+        hh = nhh;
+    }
+}
+
+// One CTA per member: the forward sweep, then the backward sweep
 // (src/linearSolver.c:261-333): Z_m = LU-SGS(V_m).
-__global__ void __launch_bounds__(1024) kb_lusgs(const ImpDev* __restrict__ I, int m) {
+__global__ void __launch_bounds__(kSweepThreads) kb_lusgs(const ImpDev* __restrict__ I, int m) {
     const ImpDev& d = I[blockIdx.x];
     if (!d.precond || !gmres_on(d)) return;
-    const double4* B = d.V + (long)m * d.N;
-    double4* dxs = d.dxs;
-    double4* dx = d.Z + (long)m * d.N;
-    const double* Dinv = d.Dinv;
-    const double* O = d.O;
-    for (int L = 0; L < d.n_lev_f; ++L) {
-        for (int k = d.lev_f_off[L] + threadIdx.x; k < d.lev_f_off[L + 1]; k += blockDim.x) {
-            int i = d.lev_f_cells[k];
-            double t1[4] = {0.0, 0.0, 0.0, 0.0};
-            for (int q = d.lo_off[i]; q < d.lo_off[i + 1]; ++q) {
-                const double* blk = O + 16 * (long)d.lo_h[q];
-                double x[4];
-                ld(dxs[d.lo_nb[q]], x);
-#pragma unroll
-                for (int a = 0; a < 4; ++a)
-#pragma unroll
-                    for (int b = 0; b < 4; ++b) t1[a] += blk[4 * a + b] * x[b];
-            }
-            const double* di = Dinv + 16 * (long)i;
-            double b[4], t2[4];
-            ld(B[i], b);
-#pragma unroll
-            for (int a = 0; a < 4; ++a) {
-                t2[a] = 0.0;
-#pragma unroll
-                for (int c = 0; c < 4; ++c) t2[a] += di[4 * a + c] * (b[c] - t1[c]);
-            }
-            dxs[i] = mk(t2);
-        }
-        __syncthreads();
-    }
-    for (int L = 0; L < d.n_lev_b; ++L) {
-        for (int k = d.lev_b_off[L] + threadIdx.x; k < d.lev_b_off[L + 1]; k += blockDim.x) {
-            int i = d.lev_b_cells[k];
-            double t1[4] = {0.0, 0.0, 0.0, 0.0};
-            for (int q = d.up_off[i]; q < d.up_off[i + 1]; ++q) {
-                const double* blk = O + 16 * (long)d.up_h[q];
-                double x[4];
-                ld(dx[d.up_nb[q]], x);
-#pragma unroll
-                for (int a = 0; a < 4; ++a)
-#pragma unroll
-                    for (int b = 0; b < 4; ++b) t1[a] += blk[4 * a + b] * x[b];
-            }
-            const double* di = Dinv + 16 * (long)i;
-            double s[4], t2[4];
-            ld(dxs[i], s);
-#pragma unroll
-            for (int a = 0; a < 4; ++a) {
-                t2[a] = 0.0;
-#pragma unroll
-                for (int c = 0; c < 4; ++c) t2[a] += di[4 * a + c] * t1[c];
-                s[a] = s[a] - t2[a];
-            }
-            dx[i] = mk(s);
-        }
-        __syncthreads();
-    }
+    const double* B = reinterpret_cast<const double*>(d.V + (long)m * d.N);
+    double* dxs = reinterpret_cast<double*>(d.dxs);
+    double* dx = reinterpret_cast<double*>(d.Z + (long)m * d.N);
+    sweep<true>(d.n_lev_f, d.lev_f_off, d.fw_cell, d.fw_nb, d.fw_h, B, dxs, dxs, dxs, d.Dinv, d.O);
+    sweep<false>(d.n_lev_b, d.lev_b_off, d.bw_cell, d.bw_nb, d.bw_h, B, dx, dx, dxs, d.Dinv, d.O);
 }
 
 // number of members whose Newton loop (what = 0) / GMRES cycle (what = 1)
@@ -871,15 +924,31 @@ int ccfd_implicit_setup(ccfd_ctx* ctx, const std::vector<int>& hs_off, const std
         std::vector<int> lfo, lfc, lbo, lbc;
         bucket(lf, nlf, lfo, lfc);
         bucket(lb, nlb, lbo, lbc);
+        auto pack = [&](const std::vector<int>& cells, const std::vector<int>& off, const std::vector<int>& nb,
+                        const std::vector<int>& hh, std::vector<int4>& pn, std::vector<int4>& ph) {
+            pn.assign(N, make_int4(-1, -1, -1, -1));
+            ph.assign(N, make_int4(-1, -1, -1, -1));
+            for (long k = 0; k < N; ++k) {
+                int d = cells[k], c = 0;
+                int* n4 = &pn[k].x;
+                int* h4 = &ph[k].x;
+                for (int q = off[d]; q < off[d + 1]; ++q, ++c) {
+                    n4[c] = nb[q];
+                    h4[c] = hh[q];
+                }
+            }
+        };
+        std::vector<int4> fwn, fwh, bwn, bwh;
+        pack(lfc, lo_off, lo_nb, lo_h, fwn, fwh);
+        pack(lbc, up_off, up_nb, up_h, bwn, bwh);
         S->n_lev_f = nlf;
         S->n_lev_b = nlb;
         if ((st = iupload(ctx, &S->twin, twin)) || (st = iupload(ctx, &S->color_cells, ccells)) ||
             (st = iupload(ctx, &S->color_off_d, coff)) ||
-            (st = iupload(ctx, &S->lo_off, lo_off)) || (st = iupload(ctx, &S->lo_nb, lo_nb)) ||
-            (st = iupload(ctx, &S->lo_h, lo_h)) || (st = iupload(ctx, &S->up_off, up_off)) ||
-            (st = iupload(ctx, &S->up_nb, up_nb)) || (st = iupload(ctx, &S->up_h, up_h)) ||
-            (st = iupload(ctx, &S->lev_f_off, lfo)) || (st = iupload(ctx, &S->lev_f_cells, lfc)) ||
-            (st = iupload(ctx, &S->lev_b_off, lbo)) || (st = iupload(ctx, &S->lev_b_cells, lbc)))
+            (st = iupload(ctx, &S->lev_f_off, lfo)) || (st = iupload(ctx, &S->fw_cell, lfc)) ||
+            (st = iupload(ctx, &S->fw_nb, fwn)) || (st = iupload(ctx, &S->fw_h, fwh)) ||
+            (st = iupload(ctx, &S->lev_b_off, lbo)) || (st = iupload(ctx, &S->bw_cell, lbc)) ||
+            (st = iupload(ctx, &S->bw_nb, bwn)) || (st = iupload(ctx, &S->bw_h, bwh)))
             return st;
     }
     CK(cudaMemsetAsync(S->sc, 0, sizeof(double) * (SC_H + (K + 1) * (K + 1) + 4 * (K + 1) + 8), ctx->stream));
@@ -965,10 +1034,8 @@ static ImpDev make_dev(ccfd_ctx* ctx) {
     d.color_off = S->color_off_d;
     d.color_cells = S->color_cells;
     d.n_lev_f = S->n_lev_f; d.n_lev_b = S->n_lev_b;
-    d.lev_f_off = S->lev_f_off; d.lev_f_cells = S->lev_f_cells;
-    d.lev_b_off = S->lev_b_off; d.lev_b_cells = S->lev_b_cells;
-    d.lo_off = S->lo_off; d.lo_nb = S->lo_nb; d.lo_h = S->lo_h;
-    d.up_off = S->up_off; d.up_nb = S->up_nb; d.up_h = S->up_h;
+    d.lev_f_off = S->lev_f_off; d.fw_cell = S->fw_cell; d.fw_nb = S->fw_nb; d.fw_h = S->fw_h;
+    d.lev_b_off = S->lev_b_off; d.bw_cell = S->bw_cell; d.bw_nb = S->bw_nb; d.bw_h = S->bw_h;
     return d;
 }
 
@@ -1121,7 +1188,7 @@ static int set_step(ImpSet* M) {
             kb_jac_check<<<g1, 32, 0, st>>>(M->dev);
         }
         for (int m = 0; m < M->max_K; ++m) {
-            if (M->any_precond) kb_lusgs<<<M->n, 1024, 0, st>>>(M->dev, m);
+            if (M->any_precond) kb_lusgs<<<M->n, kSweepThreads, 0, st>>>(M->dev, m);
             kb_copy_vz<<<gv, kB, 0, st>>>(M->dev, m);
             // matrixVector: epsFD = sqrt(eps) / |Z|
             kb_dot_zz<<<gv, kB, 0, st>>>(M->dev, m);

@@ -108,3 +108,43 @@ def test_batch_join_and_leave_mid_run():
     sc.run(1)  # released by the batch
     sa.close()
     sc.close()
+
+
+def test_implicit_members_in_lockstep_equal_alone():
+    # uneven implicit members (sizes, Krylov dimensions, preconditioner on /
+    # off, Euler / Navier-Stokes) advance in lockstep Newton / GMRES /
+    # LU-SGS launches; each must match its own run alone exactly
+    imp = CASES.implicit_cases()
+    specs = {
+        "pc": (dict(imp["naca_euler_imp_pc"]), 4),
+        "nopc": (dict(imp["naca_euler_imp_nopc"]), 4),
+        "ns_pc": (dict(imp["naca_ns_imp_pc"]), 3),
+        "pc_small": ({"mesh": ("naca", 24, 8, 101), "ini": imp["naca_euler_imp_pc"]["ini"],
+                      "eqn": "euler"}, 5),
+    }
+    alone = {}
+    for k, (spec, steps) in specs.items():
+        with tempfile.TemporaryDirectory() as tmp:
+            s = _solver(spec, tmp)
+        rep = s.run(steps)
+        alone[k] = (s.get_state(), rep)
+        s.close()
+    b = cc.Batch(0)
+    solvers = {}
+    with tempfile.TemporaryDirectory() as tmp:
+        for k, (spec, steps) in specs.items():
+            solvers[k] = _solver(spec, tmp)
+    for k, s in solvers.items():
+        b.add(s, specs[k][1])
+    assert b.step(10) == 0
+    for k, s in solvers.items():
+        prim, rep = alone[k]
+        got = b.report(s)
+        assert np.array_equal(s.get_state(), prim), k
+        _same(got, rep)
+        assert got["newton_iterations"] == rep["newton_iterations"], k
+        assert got["gmres_iterations"] == rep["gmres_iterations"], k
+        assert got["cl"] == rep["cl"] and got["cd"] == rep["cd"], k
+    b.close()
+    for s in solvers.values():
+        s.close()
