@@ -154,6 +154,148 @@ def run_mixed(tmpdir: str, steps: int, warmup: int, prim_fp64, nrk: int, bytes_s
                               "norm": "per variable, relative to max|U_fp64|"}}
 
 
+def run_batched_airfoils(n_cases: int, steps: int, cfl: float) -> dict:
+    """Steady-Euler airfoils of the batched distribution: the plain FP64 GPU
+    solver looping over the cases one at a time vs all cases in one batch
+    (lockstep Newton / GMRES / LU-SGS launches over every member).  A solve
+    is `steps` implicit time steps of one airfoil; both forms do the same
+    iterations and give bit-identical states (checked)."""
+    import ccfd_b200 as cc
+    from ccfd_b200 import workloads
+    specs = workloads.airfoil_specs(n_cases)
+    with tempfile.TemporaryDirectory() as tmp:
+        cases = [workloads.airfoil_case(sp, tmp, f"af{k}", cfl=cfl) for k, sp in enumerate(specs)]
+    cells = [c.n_cells for c in cases]
+    loop_ms, loop_states, t0 = 0.0, [], time.perf_counter()
+    for c in cases:
+        s = cc.Solver(c)
+        rep = s.run(steps)
+        loop_ms += rep["device_ms"]
+        loop_states.append(s.get_state())
+        s.close()
+    loop_wall = time.perf_counter() - t0
+    b = cc.Batch(0)
+    members = [cc.Solver(c) for c in cases]
+    for s in members:
+        b.add(s, steps)
+    t0 = time.perf_counter()
+    b.step(steps)
+    batch_wall = time.perf_counter() - t0
+    reps = [b.report(s) for s in members]
+    batch_ms = reps[0]["device_ms"]
+    diff = max(float(np.abs(s.get_state() - ls).max()) for s, ls in zip(members, loop_states))
+    b.close()
+    for s in members:
+        s.close()
+    return {
+        "workload": f"{n_cases} NACA airfoils of the batched distribution (seed 20260004), O-grids "
+                    f"{min(cells)}..{max(cells)} cells, steady Euler, Roe, 2nd order VK K=5, JFNK-GMRES "
+                    f"(Krylov 30) + LU-SGS, CFL {cfl}, {steps} implicit steps per solve, FP64",
+        "cells_total": int(sum(cells)), "solves": n_cases,
+        "loop": {"device_s": loop_ms / 1e3, "wall_s": loop_wall,
+                 "solves_per_s": n_cases / (loop_ms / 1e3)},
+        "batched": {"device_s": batch_ms / 1e3, "wall_s": batch_wall,
+                    "solves_per_s": n_cases / (batch_ms / 1e3)},
+        "speedup": loop_ms / batch_ms,
+        "max_state_diff_batched_vs_loop": diff,
+        "newton_iterations": sum(r["newton_iterations"] for r in reps),
+        "gmres_iterations": sum(r["gmres_iterations"] for r in reps),
+        "failed": sum(1 for r in reps if r["status"] != 0),
+    }
+
+
+def run_serving(n_req: int, load: float, budget: int, seed: int = 20260005) -> dict:
+    """Served mixed stream: Riemann problems, cylinder-wake windows and
+    airfoils.  (1) Each request alone through the plain loop gives its
+    service time; (2) all requests submitted at once give the server's
+    capacity; (3) Poisson arrivals at `load` x capacity are served with
+    continuous batching in real time; the plain loop is scored on the same
+    arrival times (first come, first served, measured service times)."""
+    import ccfd_b200 as cc
+    from ccfd_b200 import workloads
+    reqs = workloads.stream_specs(n_req, seed, riemann_n=(256, 768), cylinder_cells=(50_000, 100_000))
+    with tempfile.TemporaryDirectory() as tmp:
+        cases = [workloads.stream_case(r, tmp, f"q{k}") for k, r in enumerate(reqs)]
+    # plain loop: per request upload, run, read the result back, release
+    service, service_dev, ref_states = [], [], []
+    for c, r in zip(cases, reqs):
+        t0 = time.perf_counter()
+        s = cc.Solver(c)
+        rep = s.run(r["steps"])
+        ref_states.append(s.get_state())
+        s.close()
+        service.append(time.perf_counter() - t0)
+        service_dev.append(rep["device_ms"] / 1e3)
+
+    def serve(arrivals):
+        srv = cc.Server(0, hbm_budget_bytes=budget, max_running=4096)
+        ids, done, lat = {}, {}, {}
+        order = np.argsort(arrivals, kind="stable")
+        k = 0
+        t0 = time.perf_counter()
+        max_used = 0
+        while len(done) < len(cases):
+            now = time.perf_counter() - t0
+            while k < len(order) and arrivals[order[k]] <= now:
+                j = int(order[k])
+                ids[j] = srv.submit(cases[j], reqs[j]["steps"])
+                k += 1
+            if len(ids) == len(done):
+                time.sleep(max(0.0, min(0.002, arrivals[order[k]] - now)) if k < len(order) else 0)
+                continue
+            srv.poll(16)
+            max_used = max(max_used, srv.memory()[0])
+            for j, rid in ids.items():
+                if j in done:
+                    continue
+                got = srv.result(rid)
+                if got is not None:
+                    done[j] = got
+                    lat[j] = got[2][2] - got[2][0]
+        makespan = time.perf_counter() - t0
+        host = srv.times()
+        srv.close()
+        return done, lat, makespan, max_used, host
+
+    done, _, makespan_all, _, host_all = serve(np.zeros(len(cases)))
+    capacity = len(cases) / makespan_all
+    rate = load * capacity
+    rng = np.random.Generator(np.random.PCG64(seed + 7))
+    arrivals = np.cumsum(rng.exponential(1.0 / rate, len(cases)))
+    arrivals -= arrivals[0]
+    done, lat, makespan, max_used, host_open = serve(arrivals)
+    same = all(np.array_equal(done[j][1], ref_states[j]) for j in range(len(cases)))
+    # the plain loop on the same arrivals: first come, first served
+    t_free, lat_loop = 0.0, []
+    for j in np.argsort(arrivals, kind="stable"):
+        start = max(t_free, arrivals[j])
+        t_free = start + service[j]
+        lat_loop.append(t_free - arrivals[j])
+    lat_s = np.array([lat[j] for j in range(len(cases))])
+    cells = [c.n_cells for c in cases]
+    kinds = [r["kind"] for r in reqs]
+    return {
+        "workload": f"{n_req} requests (seed {seed}): " + ", ".join(
+            f"{kinds.count(k)} {k}" for k in ("riemann", "cylinder", "airfoil"))
+            + "; Riemann 256^2..768^2 quads HLLC 200 RK3 steps, cylinder NS Re 100 M 0.2 50k..100k "
+              "triangles 1000 RK3 steps, airfoils 5 implicit steps (JFNK + LU-SGS, CFL 1)",
+        "cells_total": int(sum(cells)), "hbm_budget_bytes": budget, "max_resident_bytes": int(max_used),
+        "capacity_solves_per_s": capacity, "arrival_rate_per_s": rate, "load": load,
+        "served": {"solves_per_s": len(cases) / makespan, "p50_s": float(np.percentile(lat_s, 50)),
+                   "p99_s": float(np.percentile(lat_s, 99))},
+        "server_host_s": {"closed_loop": {"admit": host_all[0], "step": host_all[1], "retire": host_all[2],
+                                          "makespan": makespan_all},
+                          "open_loop": {"admit": host_open[0], "step": host_open[1], "retire": host_open[2],
+                                        "makespan": makespan}},
+        "plain_loop": {"solves_per_s": len(cases) / max(t_free, 1e-12),
+                       "capacity_solves_per_s": len(cases) / sum(service),
+                       "device_s": sum(service_dev), "wall_s": sum(service),
+                       "p50_s": float(np.percentile(lat_loop, 50)),
+                       "p99_s": float(np.percentile(lat_loop, 99))},
+        "results_equal_alone": bool(same),
+    }
+
+
 def cpu_reference_sample(ini: str, mesh_path: str, steps: int, threads: int):
     """Time the reference (compiled from its sources, oracle/_ref) on the
     host cores: returns (cell-updates/s, seconds per step, threads)."""
@@ -211,6 +353,11 @@ def main() -> int:
     ap.add_argument("--cpu-steps", type=int, default=3)
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
     ap.add_argument("--no-mixed", action="store_true", help="skip the mixed-precision run")
+    ap.add_argument("--no-batch", action="store_true", help="skip the batched-airfoil comparison")
+    ap.add_argument("--no-serve", action="store_true", help="skip the served stream")
+    ap.add_argument("--airfoils", type=int, default=32)
+    ap.add_argument("--airfoil-steps", type=int, default=5)
+    ap.add_argument("--requests", type=int, default=24)
     ap.add_argument("--nx", type=int, default=NX)
     ap.add_argument("--ny", type=int, default=NY)
     args = ap.parse_args()
@@ -287,6 +434,12 @@ def main() -> int:
         mixed = None
         if not args.no_mixed:
             mixed = run_mixed(tmp, args.steps, args.warmup, prim_fp64, nrk, bytes_stage)
+        batched = serving = None
+        if rank == 0 or world > 1:
+            if not args.no_batch:
+                batched = run_batched_airfoils(args.airfoils, args.airfoil_steps, cfl=1.0)
+            if not args.no_serve:
+                serving = run_serving(args.requests, load=0.8, budget=150 * 10**9)
         avg_res_ms = res_ms / max(res_cnt, 1)
         achieved = bytes_stage / (avg_res_ms / 1e3) / 1e9
 
@@ -338,6 +491,8 @@ def main() -> int:
             "clocks": clk,
             "cpu_baseline": cpu,
             "mixed_precision": mixed,
+            "batched_airfoils": batched,
+            "serving": serving,
         }
         print(json.dumps(line), flush=True)
     if dist is not None:

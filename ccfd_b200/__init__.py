@@ -325,6 +325,12 @@ class Server:
         _check(N.lib.ccfd_server_memory(self._s, C.byref(used), C.byref(budget)), "ccfd_server_memory")
         return used.value, budget.value
 
+    def times(self) -> tuple[float, float, float]:
+        """Host seconds spent admitting (upload), stepping and retiring."""
+        out = (C.c_double * 3)()
+        _check(N.lib.ccfd_server_times(self._s, out), "ccfd_server_times")
+        return tuple(out)
+
     def close(self) -> None:
         if self._s:
             N.lib.ccfd_server_destroy(self._s)

@@ -127,6 +127,7 @@ def _load():
         "ccfd_server_poll": (c_int, [C.c_void_p, c_int, P(c_int), P(c_int), P(c_int)]),
         "ccfd_server_result": (c_int, [C.c_void_p, c_long, P(Report), P(c_double), P(c_double)]),
         "ccfd_server_memory": (c_int, [C.c_void_p, P(C.c_size_t), P(C.c_size_t)]),
+        "ccfd_server_times": (c_int, [C.c_void_p, P(c_double)]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)

@@ -39,7 +39,9 @@ template <typename T>
 static int dalloc(ccfd_ctx* ctx, T** p, size_t n) {
     void* q = nullptr;
     if (n == 0) n = 1;
-    cudaError_t e = cudaMalloc(&q, n * sizeof(T));
+    // stream-ordered: allocating and freeing a context never waits for the
+    // work of other contexts (a serving loop admits while others step)
+    cudaError_t e = cudaMallocAsync(&q, n * sizeof(T), ctx->stream);
     if (e != cudaSuccess) {
         ctx->last_cuda_error = (int)e;
         return CCFD_ERR_NOMEM;
@@ -80,7 +82,7 @@ static void drop_graphs(ccfd_ctx* ctx) {
 static void free_device(ccfd_ctx* ctx) {
     drop_graphs(ctx);
     ccfd_implicit_free(ctx);
-    for (void* p : ctx->allocs) cudaFree(p);
+    for (void* p : ctx->allocs) cudaFreeAsync(p, ctx->stream);
     ctx->allocs.clear();
     ctx->device_bytes = 0;
     ctx->uploaded = false;
@@ -270,6 +272,31 @@ extern "C" int ccfd_upload_case(ccfd_ctx* ctx, const ccfd_mesh* m, const ccfd_bc
         counts[t] = make_int4(ts.counts[4 * t], ts.counts[4 * t + 1], ts.counts[4 * t + 2], ts.counts[4 * t + 3]);
         gl_off[t + 1] = gl_off[t] + ts.counts[4 * t + 1] + 1;
     }
+    // packed per-tile records of the gradient cells and faces
+    std::vector<int4> g_rec(gl_off[ts.n_tiles]);
+    for (int t = 0; t < ts.n_tiles; ++t) {
+        const int nG = ts.counts[4 * t + 1], e0 = ts.e_off[t], gb = gl_off[t];
+        for (int i = 0; i < nG; ++i) {
+            int d = ts.e_ref[e0 + i];
+            g_rec[gb + i] = make_int4(d, hs_off[d], hs_off[d + 1] - hs_off[d], ts.hs_loc[gb + i]);
+        }
+    }
+    const bool ns = p.eqn == CCFD_NAVIER_STOKES;
+    const size_t nTF = ts.f_id.size();
+    std::vector<int4> f_rec(nTF);
+    std::vector<double4> f_nl(nTF), f_bb(ns ? nTF : 1);
+    for (size_t j = 0; j < nTF; ++j) {
+        int fid = ts.f_id[j];
+        f_rec[j] = make_int4(fid, ts.f_lr[j], ts.f_hs[j], 0);
+        if (fid >= 0) {
+            f_nl[j] = face_nl[fid];
+            if (ns) f_bb[j] = face_bb[fid];
+        } else {
+            int g = -1 - fid;
+            f_nl[j] = make_double4(g_gn[g].z, g_gn[g].w, g_ml[g].z, 0.0);
+            if (ns) f_bb[j] = g_bb[g];
+        }
+    }
 
     int st;
     DevMesh& dm = ctx->mesh;
@@ -291,7 +318,9 @@ extern "C" int ccfd_upload_case(ccfd_ctx* ctx, const ccfd_mesh* m, const ccfd_bc
         (st = dupload_c(ctx, &td.gl_off, gl_off)) || (st = dupload_c(ctx, &td.hs_loc, hs_loc)) ||
         (st = dupload_c(ctx, &td.f_off, ts.f_off)) || (st = dupload_c(ctx, &td.f_id, ts.f_id)) ||
         (st = dupload_c(ctx, &td.f_lr, ts.f_lr)) || (st = dupload_c(ctx, &td.f_hs, ts.f_hs)) ||
-        (st = dupload_c(ctx, &td.u_code, ts.u_code))) {
+        (st = dupload_c(ctx, &td.u_code, ts.u_code)) || (st = dupload_c(ctx, &td.g_rec, g_rec)) ||
+        (st = dupload_c(ctx, &td.f_rec, f_rec)) || (st = dupload_c(ctx, &td.f_nl, f_nl)) ||
+        (st = dupload_c(ctx, &td.f_bb, f_bb))) {
         free_device(ctx);
         return st;
     }

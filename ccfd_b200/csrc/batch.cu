@@ -57,6 +57,13 @@ struct ccfd_batch {
     int ctrl_cap = 0;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     double device_ms = 0.0;
+    // kernel variants and the implicit members run on streams of their own
+    // so that their launches overlap on the device (fork / join by events)
+    std::vector<cudaStream_t> gstream;
+    std::vector<cudaEvent_t> gdone;
+    cudaEvent_t fork = nullptr;
+    cudaStream_t istream = nullptr;
+    cudaEvent_t idone = nullptr;
 };
 
 #define CKB(x)                              \
@@ -72,8 +79,8 @@ static constexpr int kMany = 16;
 
 static void drop_group_memory(ccfd_batch* b) {
     for (auto& g : b->groups) {
-        if (g.d_recs) cudaFree(g.d_recs);
-        if (g.d_tmap) cudaFree(g.d_tmap);
+        if (g.d_recs) cudaFreeAsync(g.d_recs, b->stream);
+        if (g.d_tmap) cudaFreeAsync(g.d_tmap, b->stream);
     }
     b->groups.clear();
     for (auto& g : b->graph)
@@ -110,7 +117,7 @@ static void member_records(ccfd_ctx* ctx, StageLaunch* out) {
 }
 
 // group the explicit members by kernel variant, upload their launch records
-// and tile maps, and capture the step graphs
+// and tile maps
 static int rebuild(ccfd_batch* b) {
     drop_group_memory(b);
     std::map<std::tuple<int, int, int, int>, int> key_of;
@@ -151,12 +158,20 @@ static int rebuild(ccfd_batch* b) {
         }
         g.n_tiles = (int)tmap.size();
         g.smem_bytes = stage_smem_bytes(big, g.fp32);
-        CKB(cudaMalloc(&g.d_recs, sizeof(StageLaunch) * recs.size()));
-        CKB(cudaMalloc(&g.d_tmap, sizeof(int2) * tmap.size()));
+        CKB(cudaMallocAsync(&g.d_recs, sizeof(StageLaunch) * recs.size(), b->stream));
+        CKB(cudaMallocAsync(&g.d_tmap, sizeof(int2) * tmap.size(), b->stream));
         CKB(cudaMemcpyAsync(g.d_recs, recs.data(), sizeof(StageLaunch) * recs.size(), cudaMemcpyHostToDevice,
                             b->stream));
         CKB(cudaMemcpyAsync(g.d_tmap, tmap.data(), sizeof(int2) * tmap.size(), cudaMemcpyHostToDevice,
                             b->stream));
+    }
+    while (b->gstream.size() < b->groups.size()) {
+        cudaStream_t gs;
+        cudaEvent_t ge;
+        CKB(cudaStreamCreateWithFlags(&gs, cudaStreamNonBlocking));
+        CKB(cudaEventCreateWithFlags(&ge, cudaEventDisableTiming));
+        b->gstream.push_back(gs);
+        b->gdone.push_back(ge);
     }
     // control-block gather list
     const int n = (int)b->inst.size();
@@ -173,42 +188,59 @@ static int rebuild(ccfd_batch* b) {
     for (int i = 0; i < n; ++i) ptrs[i] = b->inst[i]->ctrl;
     if (n) CKB(cudaMemcpyAsync((void*)b->d_ctrl_ptr, ptrs.data(), sizeof(Ctrl*) * n, cudaMemcpyHostToDevice, b->stream));
     CKB(cudaStreamSynchronize(b->stream));
-    // step graphs
-    if (!b->groups.empty()) {
-        for (int w = 0; w < 2; ++w) {
-            const int steps = w ? kMany : 1;
-            cudaGraph_t gr;
-            CKB(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
-            for (int i = 0; i < steps; ++i)
-                for (int s = 0; s < b->max_nrk; ++s)
-                    for (auto& g : b->groups) {
-                        BatchLaunch B;
-                        B.recs = g.d_recs;
-                        B.tmap = g.d_tmap;
-                        B.n_tiles = g.n_tiles;
-                        B.smem_bytes = g.smem_bytes;
-                        B.rk_mode = 1;
-                        B.stage = s;
-                        B.flux_id = g.flux;
-                        B.order = g.order;
-                        B.ns = g.ns;
-                        B.fp32 = g.fp32;
-                        launch_stage_batch(B, b->stream);
-                    }
-            cudaError_t e = cudaStreamEndCapture(b->stream, &gr);
-            if (e != cudaSuccess) {
-                b->last_cuda_error = (int)e;
-                return CCFD_ERR_CUDA;
+    b->dirty = false;
+    return CCFD_OK;
+}
+
+// `steps` batched steps, each variant on its own stream after the fork
+// event of the batch stream, joined back into the batch stream
+static void launch_steps(ccfd_batch* b, int steps) {
+    cudaEventRecord(b->fork, b->stream);
+    for (size_t k = 0; k < b->groups.size(); ++k) {
+        VariantGroup& g = b->groups[k];
+        cudaStream_t gs = b->gstream[k];
+        cudaStreamWaitEvent(gs, b->fork, 0);
+        for (int i = 0; i < steps; ++i)
+            for (int s = 0; s < b->max_nrk; ++s) {
+                BatchLaunch B;
+                B.recs = g.d_recs;
+                B.tmap = g.d_tmap;
+                B.n_tiles = g.n_tiles;
+                B.smem_bytes = g.smem_bytes;
+                B.rk_mode = 1;
+                B.stage = s;
+                B.flux_id = g.flux;
+                B.order = g.order;
+                B.ns = g.ns;
+                B.fp32 = g.fp32;
+                launch_stage_batch(B, gs);
             }
-            e = cudaGraphInstantiate(&b->graph[w], gr, 0);
-            cudaGraphDestroy(gr);
-            if (e != cudaSuccess) {
-                b->last_cuda_error = (int)e;
-                return CCFD_ERR_CUDA;
-            }
+        cudaEventRecord(b->gdone[k], gs);
+        cudaStreamWaitEvent(b->stream, b->gdone[k], 0);
+    }
+}
+
+// CUDA graphs of one and of kMany batched steps (captured once the
+// membership has stayed the same for a call; until then the steps are
+// launched directly, which costs less than a capture per change)
+static int capture_graphs(ccfd_batch* b) {
+    for (int w = 0; w < 2; ++w) {
+        const int steps = w ? kMany : 1;
+        cudaGraph_t gr;
+        CKB(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
+        launch_steps(b, steps);
+        cudaError_t e = cudaStreamEndCapture(b->stream, &gr);
+        if (e != cudaSuccess) {
+            b->last_cuda_error = (int)e;
+            return CCFD_ERR_CUDA;
+        }
+        e = cudaGraphInstantiate(&b->graph[w], gr, 0);
+        cudaGraphDestroy(gr);
+        if (e != cudaSuccess) {
+            b->last_cuda_error = (int)e;
+            return CCFD_ERR_CUDA;
         }
     }
-    b->dirty = false;
     return CCFD_OK;
 }
 
@@ -239,6 +271,9 @@ extern "C" int ccfd_batch_create(int device, ccfd_batch** out) {
     CKB(cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking));
     CKB(cudaEventCreate(&b->ev0));
     CKB(cudaEventCreate(&b->ev1));
+    CKB(cudaEventCreateWithFlags(&b->fork, cudaEventDisableTiming));
+    CKB(cudaEventCreateWithFlags(&b->idone, cudaEventDisableTiming));
+    CKB(cudaStreamCreateWithFlags(&b->istream, cudaStreamNonBlocking));
     *out = b;
     return CCFD_OK;
 }
@@ -261,6 +296,13 @@ extern "C" void ccfd_batch_destroy(ccfd_batch* b) {
     if (b->h_ctrl) cudaFreeHost(b->h_ctrl);
     if (b->ev0) cudaEventDestroy(b->ev0);
     if (b->ev1) cudaEventDestroy(b->ev1);
+    for (size_t k = 0; k < b->gstream.size(); ++k) {
+        cudaStreamDestroy(b->gstream[k]);
+        cudaEventDestroy(b->gdone[k]);
+    }
+    if (b->fork) cudaEventDestroy(b->fork);
+    if (b->idone) cudaEventDestroy(b->idone);
+    if (b->istream) cudaStreamDestroy(b->istream);
     cudaStreamDestroy(b->stream);
     delete b;
 }
@@ -323,19 +365,37 @@ extern "C" int ccfd_batch_step(ccfd_batch* b, int steps, int* n_running) {
     if (!b || steps <= 0) return CCFD_ERR_ARG;
     CKB(cudaSetDevice(b->device));
     int st;
-    if (b->dirty && (st = rebuild(b))) return st;
+    bool direct = false;
+    if (b->dirty) {
+        if ((st = rebuild(b))) return st;
+        direct = true;
+    } else if (!b->groups.empty() && !b->graph[0] && (st = capture_graphs(b))) {
+        return st;
+    }
     CKB(cudaEventRecord(b->ev0, b->stream));
     std::vector<ccfd_ctx*> imp;
     for (ccfd_ctx* c : b->inst)
         if (c->params.implicit) imp.push_back(c);
-    int left = steps;
+    // explicit members: queued asynchronously first ...
     bool any_explicit = !b->groups.empty();
-    while (left > 0 && any_explicit) {
-        int w = left >= kMany ? 1 : 0;
-        CKB(cudaGraphLaunch(b->graph[w], b->stream));
-        left -= w ? kMany : 1;
+    if (any_explicit && direct) {
+        launch_steps(b, steps);
+    } else if (any_explicit) {
+        for (int left = steps; left > 0;) {
+            int w = left >= kMany ? 1 : 0;
+            CKB(cudaGraphLaunch(b->graph[w], b->stream));
+            left -= w ? kMany : 1;
+        }
     }
-    if (!imp.empty() && (st = ccfd_implicit_batch_steps(b, imp, steps))) return st;
+    CKB(cudaGetLastError());
+    // ... then the implicit members are driven on their own stream while the
+    // explicit launches run
+    if (!imp.empty()) {
+        CKB(cudaStreamWaitEvent(b->istream, b->ev0, 0));
+        if ((st = ccfd_implicit_batch_steps(b, imp, steps))) return st;
+        CKB(cudaEventRecord(b->idone, b->istream));
+        CKB(cudaStreamWaitEvent(b->stream, b->idone, 0));
+    }
     CKB(cudaEventRecord(b->ev1, b->stream));
     if ((st = pull_ctrl(b))) return st;
     float ms = 0.0f;
@@ -364,3 +424,4 @@ extern "C" int ccfd_batch_size(ccfd_batch* b, int* n) {
 }
 
 cudaStream_t ccfd_batch_stream(ccfd_batch* b) { return b->stream; }
+cudaStream_t ccfd_batch_implicit_stream(ccfd_batch* b) { return b->istream; }

@@ -778,7 +778,7 @@ template <typename T>
 static int ialloc(ccfd_ctx* ctx, T** p, size_t n) {
     void* q = nullptr;
     if (n == 0) n = 1;
-    if (cudaMalloc(&q, n * sizeof(T)) != cudaSuccess) return CCFD_ERR_NOMEM;
+    if (cudaMallocAsync(&q, n * sizeof(T), ctx->stream) != cudaSuccess) return CCFD_ERR_NOMEM;
     ctx->allocs.push_back(q);
     ctx->device_bytes += n * sizeof(T);
     *p = (T*)q;
@@ -986,13 +986,13 @@ struct ImpSet {
 static void set_free(ImpSet* M) {
     if (!M) return;
     for (auto& g : M->groups) {
-        cudaFree(g.rec_mv);
-        cudaFree(g.rec_nt);
-        cudaFree(g.rec_jac);
-        cudaFree(g.tmap);
+        cudaFreeAsync(g.rec_mv, M->stream);
+        cudaFreeAsync(g.rec_nt, M->stream);
+        cudaFreeAsync(g.rec_jac, M->stream);
+        cudaFreeAsync(g.tmap, M->stream);
     }
-    if (M->dev) cudaFree(M->dev);
-    if (M->d_count) cudaFree(M->d_count);
+    if (M->dev) cudaFreeAsync(M->dev, M->stream);
+    if (M->d_count) cudaFreeAsync(M->d_count, M->stream);
     if (M->h_count) cudaFreeHost(M->h_count);
     delete M;
 }
@@ -1065,9 +1065,9 @@ static int set_build(const std::vector<ccfd_ctx*>& members, cudaStream_t stream,
         ccfd_fill_stage(ctx, probe);
         by_variant[std::make_tuple(probe.flux_id, probe.order, probe.ns, probe.fp32)].push_back(k);
     }
-    CKM(cudaMalloc(&M->dev, sizeof(ImpDev) * M->n));
+    CKM(cudaMallocAsync(&M->dev, sizeof(ImpDev) * M->n, stream));
     CKM(cudaMemcpyAsync(M->dev, hd.data(), sizeof(ImpDev) * M->n, cudaMemcpyHostToDevice, stream));
-    CKM(cudaMalloc(&M->d_count, sizeof(int)));
+    CKM(cudaMallocAsync(&M->d_count, sizeof(int), stream));
     CKM(cudaMallocHost(&M->h_count, sizeof(int)));
     for (auto& kv : by_variant) {
         ImpGroup g;
@@ -1111,10 +1111,10 @@ static int set_build(const std::vector<ccfd_ctx*>& members, cudaStream_t stream,
         g.n_tiles = (int)tmap.size();
         g.smem = stage_smem_bytes(big, g.fp32);
         size_t rb = sizeof(StageLaunch) * idx.size();
-        CKM(cudaMalloc(&g.rec_mv, rb));
-        CKM(cudaMalloc(&g.rec_nt, rb));
-        CKM(cudaMalloc(&g.rec_jac, rb));
-        CKM(cudaMalloc(&g.tmap, sizeof(int2) * tmap.size()));
+        CKM(cudaMallocAsync(&g.rec_mv, rb, stream));
+        CKM(cudaMallocAsync(&g.rec_nt, rb, stream));
+        CKM(cudaMallocAsync(&g.rec_jac, rb, stream));
+        CKM(cudaMallocAsync(&g.tmap, sizeof(int2) * tmap.size(), stream));
         CKM(cudaMemcpyAsync(g.rec_mv, mv.data(), rb, cudaMemcpyHostToDevice, stream));
         CKM(cudaMemcpyAsync(g.rec_nt, nt.data(), rb, cudaMemcpyHostToDevice, stream));
         CKM(cudaMemcpyAsync(g.rec_jac, jac.data(), rb, cudaMemcpyHostToDevice, stream));
@@ -1321,6 +1321,7 @@ struct BatchImp {
 static std::map<const ccfd_batch*, BatchImp> g_batch_imp;
 
 cudaStream_t ccfd_batch_stream(ccfd_batch* b);
+cudaStream_t ccfd_batch_implicit_stream(ccfd_batch* b);
 
 int ccfd_implicit_batch_join(ccfd_batch* b, ccfd_ctx* ctx) {
     ImpState* S = (ImpState*)ctx->implicit_state;
@@ -1359,7 +1360,7 @@ int ccfd_implicit_batch_steps(ccfd_batch* b, const std::vector<ccfd_ctx*>& membe
         if (bi.set) set_free(bi.set);
         bi.set = nullptr;
         bi.key = members;
-        int s = set_build(members, ccfd_batch_stream(b), &bi.set);
+        int s = set_build(members, ccfd_batch_implicit_stream(b), &bi.set);
         if (s) return s;
     }
     ImpSet* M = bi.set;

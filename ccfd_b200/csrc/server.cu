@@ -1,21 +1,27 @@
 // Request loop with continuous batching on one GPU.
 //
-// Requests (a case with a step budget) queue in arrival order.  Each call of
-// ccfd_server_poll admits queued requests, first come first served, while
-// their estimated device memory fits the budget and a slot is free; an
-// admitted request is uploaded into its own context and joins the running
-// batch at the next step boundary, so it overlaps on the device with the
-// requests already running.  The batch then advances every running request;
-// requests that stop (end time, convergence, step budget, error) leave the
-// batch, their final state is copied to the host and their device memory is
-// released for the next admissions.  No counterpart in the reference, which
-// runs one case per process.
+// Requests (a case with a step budget) queue in arrival order.  Worker
+// threads admit them, first come first served, while their estimated device
+// memory fits the budget and a slot is free: it uploads each admitted case
+// into its own context (host-side mesh preparation and host-to-device copies
+// on the context's stream) while the GPU keeps stepping the running
+// requests.  Each call of ccfd_server_poll moves the uploaded requests into
+// the running batch at the step boundary, so they overlap on the device with
+// the requests already running, advances the batch, and retires the
+// requests that stopped (end time, convergence, step budget, error): their
+// final state is copied to the host and their device memory is released for
+// the next admissions.  No counterpart in the reference, which runs one case
+// per process.
 #include <cuda_runtime.h>
 #include <string.h>
 
+#include <algorithm>
 #include <chrono>
+#include <condition_variable>
 #include <deque>
 #include <map>
+#include <mutex>
+#include <thread>
 #include <vector>
 
 #include "ccfd_ctx.cuh"
@@ -27,13 +33,13 @@ double now_s() {
     return duration<double>(steady_clock::now().time_since_epoch()).count();
 }
 
-enum ReqState { QUEUED = 0, RUNNING = 1, DONE = 2 };
+enum ReqState { QUEUED = 0, UPLOADING, READY, RUNNING, DONE };
 
 struct Request {
     long id = 0;
     const ccfd_case* c = nullptr;
     long nsteps = 0;
-    size_t est = 0, bytes = 0;
+    size_t est = 0, bytes = 0;  // reserved estimate, then the context's actual bytes
     ccfd_ctx* ctx = nullptr;
     int state = QUEUED;
     int status = CCFD_OK;
@@ -46,13 +52,19 @@ struct Request {
 
 struct ccfd_server {
     int device = 0;
-    size_t budget = 0, used = 0;
+    size_t budget = 0, used = 0;  // used: reserved / held device bytes
     int max_running = 0;
+    int slots = 0;                // requests uploading, ready or running
     ccfd_batch* batch = nullptr;
     std::deque<long> queue;
     std::map<long, Request> reqs;
+    std::vector<long> ready;      // uploaded, waiting for the next step boundary
     long next_id = 1;
-    int running = 0;
+    double t_admit = 0, t_step = 0, t_retire = 0;  // host seconds per phase
+    std::mutex mu;
+    std::condition_variable cv;
+    bool stop = false;
+    std::vector<std::thread> workers;  // uploads run in parallel, one request each
 };
 
 static size_t round_up(size_t x) { return (x + 255) & ~(size_t)255; }
@@ -66,8 +78,8 @@ extern "C" int ccfd_estimate_device_bytes(const ccfd_params* p, const ccfd_mesh*
     if (p->implicit) {
         const double K = (double)(p->n_kdim > 0 ? p->n_kdim : 1);
         // Krylov bases V (K+1) and Z (K), eight work vectors, D / D^-1 per
-        // cell, off-diagonal blocks per half-side, colouring and level lists
-        b += (64.0 * K + 32.0 + 8.0 * 32.0 + 256.0) * N + 144.0 * H + 16.0 * N;
+        // cell, off-diagonal blocks per half-side, colouring and sweep lists
+        b += (64.0 * K + 32.0 + 8.0 * 32.0 + 256.0 + 96.0) * N + 144.0 * H;
     }
     *bytes = round_up((size_t)(1.2 * b));
     return CCFD_OK;
@@ -77,6 +89,62 @@ extern "C" int ccfd_device_bytes(ccfd_ctx* ctx, size_t* bytes) {
     if (!ctx || !bytes) return CCFD_ERR_ARG;
     *bytes = ctx->device_bytes;
     return CCFD_OK;
+}
+
+// upload one admitted request (worker thread, server lock not held)
+static int upload(Request& r) {
+    const ccfd_case* c = r.c;
+    int st = ccfd_create(&c->params, &r.ctx);
+    if (st) {
+        r.ctx = nullptr;
+        return st;
+    }
+    st = ccfd_upload_case(r.ctx, &c->mesh, c->bc_table, c->n_bc_table, &c->exact, 1);
+    if (!st) st = ccfd_set_state(r.ctx, c->prim0, CCFD_PRIMITIVE);
+    return st;
+}
+
+static void worker_main(ccfd_server* s) {
+    cudaSetDevice(s->device);
+    std::unique_lock<std::mutex> lk(s->mu);
+    for (;;) {
+        s->cv.wait(lk, [s] {
+            if (s->stop) return true;
+            if (s->queue.empty() || s->slots >= s->max_running) return false;
+            return s->used + s->reqs[s->queue.front()].est <= s->budget;
+        });
+        if (s->stop) return;
+        long id = s->queue.front();
+        s->queue.pop_front();
+        Request& r = s->reqs[id];  // std::map references stay valid
+        r.state = UPLOADING;
+        r.t_admit = now_s();
+        s->used += r.est;
+        s->slots++;
+        lk.unlock();
+        double t0 = now_s();
+        int st = upload(r);
+        double t1 = now_s();
+        lk.lock();
+        s->t_admit += t1 - t0;
+        if (st) {
+            if (r.ctx) ccfd_destroy(r.ctx);
+            r.ctx = nullptr;
+            s->used -= r.est;
+            s->slots--;
+            r.status = st;
+            r.state = DONE;
+            r.t_done = now_s();
+        } else {
+            // hold the actual bytes from now on (never more than the estimate)
+            r.bytes = r.ctx->device_bytes;
+            s->used -= r.est;
+            s->used += r.bytes;
+            r.state = READY;
+            s->ready.push_back(id);
+        }
+        s->cv.notify_all();
+    }
 }
 
 extern "C" int ccfd_server_create(int device, size_t hbm_budget_bytes, int max_running, ccfd_server** out) {
@@ -92,16 +160,25 @@ extern "C" int ccfd_server_create(int device, size_t hbm_budget_bytes, int max_r
         delete s;
         return st;
     }
+    unsigned hw = std::thread::hardware_concurrency();
+    int nw = (int)std::max(1u, std::min(4u, hw / 2));
+    for (int k = 0; k < nw; ++k) s->workers.emplace_back(worker_main, s);
     *out = s;
     return CCFD_OK;
 }
 
 extern "C" void ccfd_server_destroy(ccfd_server* s) {
     if (!s) return;
+    {
+        std::lock_guard<std::mutex> lk(s->mu);
+        s->stop = true;
+    }
+    s->cv.notify_all();
+    for (auto& w : s->workers) w.join();
     cudaSetDevice(s->device);
+    ccfd_batch_destroy(s->batch);
     for (auto& kv : s->reqs)
         if (kv.second.ctx) ccfd_destroy(kv.second.ctx);
-    ccfd_batch_destroy(s->batch);
     delete s;
 }
 
@@ -110,86 +187,106 @@ extern "C" void ccfd_server_destroy(ccfd_server* s) {
 extern "C" int ccfd_server_submit(ccfd_server* s, const ccfd_case* c, long nsteps, long* id) {
     if (!s || !c || !id) return CCFD_ERR_ARG;
     Request r;
-    r.id = s->next_id++;
     r.c = c;
     r.nsteps = nsteps;
     r.t_submit = now_s();
     int st = ccfd_estimate_device_bytes(&c->params, &c->mesh, &r.est);
     if (st) return st;
     if (r.est > s->budget) return CCFD_ERR_BUDGET;
-    *id = r.id;
-    s->reqs[r.id] = std::move(r);
-    s->queue.push_back(*id);
+    {
+        std::lock_guard<std::mutex> lk(s->mu);
+        r.id = s->next_id++;
+        *id = r.id;
+        s->reqs[r.id] = std::move(r);
+        s->queue.push_back(*id);
+    }
+    s->cv.notify_all();
     return CCFD_OK;
 }
 
-static void finish(ccfd_server* s, Request& r, int status) {
+// retire a request that left the batch (server lock held)
+static void retire(ccfd_server* s, Request& r, int status) {
     r.status = status;
+    r.prim.resize(4 * (size_t)r.c->mesh.n_cells);
+    int gs = ccfd_get_state(r.ctx, r.prim.data(), CCFD_PRIMITIVE);
+    if (gs) r.prim.clear();
+    if (!r.status) r.status = gs;
+    ccfd_destroy(r.ctx);
+    r.ctx = nullptr;
+    s->used -= r.bytes;
+    s->slots--;
     r.state = DONE;
     r.t_done = now_s();
-    if (r.ctx) {
-        r.prim.resize(4 * (size_t)r.c->mesh.n_cells);
-        int gs = r.ctx->uploaded ? ccfd_get_state(r.ctx, r.prim.data(), CCFD_PRIMITIVE) : CCFD_ERR_ARG;
-        if (gs) r.prim.clear();
-        if (!r.status) r.status = gs;
-        ccfd_destroy(r.ctx);
-        r.ctx = nullptr;
-        s->used -= r.bytes;
-        s->running--;
-    }
 }
 
-static int admit(ccfd_server* s, Request& r) {
-    const ccfd_case* c = r.c;
-    r.t_admit = now_s();
-    r.state = RUNNING;
-    int st = ccfd_create(&c->params, &r.ctx);
-    if (st) {
-        r.ctx = nullptr;
-        return st;
-    }
-    s->running++;
-    st = ccfd_upload_case(r.ctx, &c->mesh, c->bc_table, c->n_bc_table, &c->exact, 1);
-    if (!st) st = ccfd_set_state(r.ctx, c->prim0, CCFD_PRIMITIVE);
-    if (!st) st = ccfd_batch_add(s->batch, r.ctx, r.nsteps);
-    r.bytes = r.ctx->device_bytes;
-    s->used += r.bytes;
-    return st;
-}
-
-// Admit what fits, advance the running requests by up to `steps` steps,
-// retire the ones that stopped.  Counts of queued / running / finished
-// (not yet fetched) requests are returned.
+// Move uploaded requests into the batch, advance the running requests by up
+// to `steps` steps, retire the ones that stopped.  Counts of queued (incl.
+// uploading) / running / finished-not-fetched requests are returned.
 extern "C" int ccfd_server_poll(ccfd_server* s, int steps, int* n_queued, int* n_running, int* n_done) {
     if (!s || steps <= 0) return CCFD_ERR_ARG;
     if (cudaSetDevice(s->device) != cudaSuccess) return CCFD_ERR_CUDA;
-    while (!s->queue.empty() && s->running < s->max_running) {
-        Request& r = s->reqs[s->queue.front()];
-        if (s->used + r.est > s->budget) break;  // first come, first served
-        s->queue.pop_front();
-        int st = admit(s, r);
-        if (st) finish(s, r, st);
+    std::vector<long> joining;
+    int n_batch = 0, st;
+    if ((st = ccfd_batch_size(s->batch, &n_batch))) return st;
+    {
+        std::unique_lock<std::mutex> lk(s->mu);
+        // nothing to step yet: wait briefly for an upload to complete
+        if (n_batch == 0 && s->ready.empty() && s->slots > 0)
+            s->cv.wait_for(lk, std::chrono::milliseconds(20), [s] { return !s->ready.empty(); });
+        joining.swap(s->ready);
     }
-    int n_batch = 0;
-    int st = ccfd_batch_size(s->batch, &n_batch);
-    if (st) return st;
-    if (n_batch > 0) {
-        int left = 0;
-        if ((st = ccfd_batch_step(s->batch, steps, &left))) return st;
-        for (auto& kv : s->reqs) {
-            Request& r = kv.second;
-            if (r.state != RUNNING) continue;
-            const ccfd::Ctrl& h = *r.ctx->h_ctrl;
-            if (!h.done && h.iter < h.stop_at) continue;
-            if ((st = ccfd_batch_report(s->batch, r.ctx, &r.rep))) return st;
-            if ((st = ccfd_batch_remove(s->batch, r.ctx))) return st;
-            finish(s, r, r.rep.status);
+    for (long id : joining) {
+        Request* r;
+        {
+            std::lock_guard<std::mutex> lk(s->mu);
+            r = &s->reqs[id];
+        }
+        st = ccfd_batch_add(s->batch, r->ctx, r->nsteps);
+        std::lock_guard<std::mutex> lk(s->mu);
+        if (st) {
+            retire(s, *r, st);
+            s->cv.notify_all();
+        } else {
+            r->state = RUNNING;
         }
     }
-    int q = (int)s->queue.size(), d = 0;
-    for (auto& kv : s->reqs) d += kv.second.state == DONE;
+    if ((st = ccfd_batch_size(s->batch, &n_batch))) return st;
+    if (n_batch > 0) {
+        double t1 = now_s();
+        int left = 0;
+        if ((st = ccfd_batch_step(s->batch, steps, &left))) return st;
+        double t2 = now_s();
+        std::vector<Request*> stopped;
+        {
+            std::lock_guard<std::mutex> lk(s->mu);
+            s->t_step += t2 - t1;
+            for (auto& kv : s->reqs) {
+                Request& r = kv.second;
+                if (r.state != RUNNING) continue;
+                const ccfd::Ctrl& h = *r.ctx->h_ctrl;
+                if (h.done || h.iter >= h.stop_at) stopped.push_back(&r);
+            }
+        }
+        for (Request* r : stopped) {
+            if ((st = ccfd_batch_report(s->batch, r->ctx, &r->rep))) return st;
+            if ((st = ccfd_batch_remove(s->batch, r->ctx))) return st;
+            std::lock_guard<std::mutex> lk(s->mu);
+            retire(s, *r, r->rep.status);
+        }
+        std::lock_guard<std::mutex> lk(s->mu);
+        s->t_retire += now_s() - t2;
+        s->cv.notify_all();
+    }
+    std::lock_guard<std::mutex> lk(s->mu);
+    int q = 0, run = 0, d = 0;
+    for (auto& kv : s->reqs) {
+        int stt = kv.second.state;
+        q += stt == QUEUED || stt == UPLOADING || stt == READY;
+        run += stt == RUNNING;
+        d += stt == DONE;
+    }
     if (n_queued) *n_queued = q;
-    if (n_running) *n_running = s->running;
+    if (n_running) *n_running = run;
     if (n_done) *n_done = d;
     return CCFD_OK;
 }
@@ -201,6 +298,7 @@ extern "C" int ccfd_server_poll(ccfd_server* s, int steps, int* n_queued, int* n
 extern "C" int ccfd_server_result(ccfd_server* s, long id, ccfd_report* rep, double* prim,
                                   double times[3]) {
     if (!s) return CCFD_ERR_ARG;
+    std::lock_guard<std::mutex> lk(s->mu);
     auto it = s->reqs.find(id);
     if (it == s->reqs.end()) return CCFD_ERR_ARG;
     Request& r = it->second;
@@ -220,8 +318,19 @@ extern "C" int ccfd_server_result(ccfd_server* s, long id, ccfd_report* rep, dou
     return st;
 }
 
+// host seconds spent so far uploading (worker thread), stepping and retiring
+extern "C" int ccfd_server_times(ccfd_server* s, double out[3]) {
+    if (!s || !out) return CCFD_ERR_ARG;
+    std::lock_guard<std::mutex> lk(s->mu);
+    out[0] = s->t_admit;
+    out[1] = s->t_step;
+    out[2] = s->t_retire;
+    return CCFD_OK;
+}
+
 extern "C" int ccfd_server_memory(ccfd_server* s, size_t* used, size_t* budget) {
     if (!s) return CCFD_ERR_ARG;
+    std::lock_guard<std::mutex> lk(s->mu);
     if (used) *used = s->used;
     if (budget) *budget = s->budget;
     return CCFD_OK;

@@ -438,9 +438,8 @@ __device__ __forceinline__ void stage_body(const StageLaunch& L, const int t) {
     const int hb = T.hs_off[t], gb = T.gl_off[t];
     if (ORDER == 2) {
         for (int i = tid; i < nG; i += kThreads) {
-            int d = T.e_ref[e0 + i];
-            int h0 = m.hs_off[d], nh = m.hs_off[d + 1] - h0;
-            int lo = T.hs_loc[gb + i];
+            const int4 gr = T.g_rec[gb + i];
+            const int d = gr.x, h0 = gr.y, nh = gr.z, lo = gr.w;
             FT q[4], ux[4], uy[4];
             ld4(ps[i], q);
             FT eps2 = L.limiter == 2 ? FT(m.venk_eps2[d]) : FT(0.0);
@@ -460,14 +459,15 @@ __device__ __forceinline__ void stage_body(const StageLaunch& L, const int t) {
     // C: fluxes of the tile's faces (interior faces, then boundary faces)
     const int f0 = T.f_off[t], nF = T.f_off[t + 1] - f0;
     for (int j = tid; j < nF; j += kThreads) {
-        int fid = T.f_id[f0 + j];
-        int lr = T.f_lr[f0 + j];
+        const int4 fr = T.f_rec[f0 + j];
+        const double4 nlj = T.f_nl[f0 + j];
+        const int fid = fr.x, lr = fr.y;
         int il = lr & 0xffff, ir = lr >> 16;
         FT q0[4], q1[4], Lf[4], Rf[4];
         FT g0x[4] = {0, 0, 0, 0}, g0y[4] = {0, 0, 0, 0}, g1x[4] = {0, 0, 0, 0}, g1y[4] = {0, 0, 0, 0};
         ld4(ps[il], q0);
         ld4(ps[ir], q1);
-        int hh = T.f_hs[f0 + j];
+        int hh = fr.z;
         if (ORDER == 2) {
             V2 gpl = hgp[hh & 0xffff];
             ld4(gs[2 * il], g0x);
@@ -491,18 +491,16 @@ __device__ __forceinline__ void stage_body(const StageLaunch& L, const int t) {
 #pragma unroll
                 for (int v = 0; v < 4; ++v) Rf[v] = q1[v];
             }
-            double4 nl = m.face_nl[fid];
-            nx = FT(nl.x); ny = FT(nl.y); len = FT(nl.z);
-            if (NS) bb = m.face_bb[fid];
+            nx = FT(nlj.x); ny = FT(nlj.y); len = FT(nlj.z);
+            if (NS) bb = T.f_bb[f0 + j];
         } else {
             int g = -1 - fid;
             double4 Rd = ghost_face(L.ghosts.bc, L.ghosts.gn, L.ghosts.ml, L.phys_g, g, time,
                                     to_d4(mk4(Lf)), L.flags);
             ld4(cvt4<FT>(Rd), Rf);
             if (L.ghost_pface) L.ghost_pface[g] = double(Lf[3]);
-            double4 gn = L.ghosts.gn[g];
-            nx = FT(gn.z); ny = FT(gn.w); len = FT(L.ghosts.ml[g].z);
-            if (NS) bb = L.ghosts.bb[g];
+            nx = FT(nlj.x); ny = FT(nlj.y); len = FT(nlj.z);
+            if (NS) bb = T.f_bb[f0 + j];
         }
         FT F[4];
         face_flux<FLUX, NS, FT>(P, nx, ny, len, Lf, Rf, q0, q1, g0x, g0y, g1x, g1y, bb, F, L.flags);
@@ -516,8 +514,8 @@ __device__ __forceinline__ void stage_body(const StageLaunch& L, const int t) {
     int bad = 0;
     const bool rk = L.mode == 1;
     for (int i = tid; i < nT; i += kThreads) {
-        int d = T.e_ref[e0 + i];
-        int h0 = m.hs_off[d], h1 = m.hs_off[d + 1];
+        const int4 gr = T.g_rec[gb + i];  // tile cells lead the gradient-cell list
+        const int d = gr.x, h0 = gr.y, h1 = gr.y + gr.z;
         double s[4] = {0.0, 0.0, 0.0, 0.0};
         for (int h = h0; h < h1; ++h) {
             int code = T.u_code[h];

@@ -363,3 +363,51 @@ def cylinder_mesh(n_theta: int = 128, n_r: int = 64, r0: float = 0.5, r_far: flo
     bc = [(i, (i + 1) % n_theta, wall_code) for i in range(n_theta)]
     bc += [(n_r * n_theta + i, n_r * n_theta + (i + 1) % n_theta, far_code) for i in range(n_theta)]
     return RawMesh(nodes, tria=np.array(tri), bc=np.array(bc))
+
+
+def cylinder_ini(mesh_file: str, reynolds: float = 100.0, mach: float = 0.2, steps: int = 1000,
+                 flux: int = 2, cfl: float = 0.8, wall_code: int = 201) -> str:
+    """Viscous flow past the cylinder of cylinder_mesh (diameter 1): far field
+    501 with rho = p = 1 at the given Mach number, adiabatic no-slip wall,
+    mu from the Reynolds number on the diameter; a window of `steps` RK3
+    steps."""
+    base = mesh_file[:-4] if mesh_file.endswith(".msh") else mesh_file
+    c_inf = math.sqrt(1.4 * 1.0 / 1.0)
+    mu = 1.0 * mach * c_inf * 1.0 / reynolds
+    return f"""! cylinder wake
+navierStokes = T
+mu = {mu!r}
+Pr = 0.72
+meshType = 0
+meshFormat = .msh
+meshFile = {base}
+nBC = 2
+BCtype = {wall_code}
+adiabaticWall = T
+BCtype = 501
+rho = 1.0
+mach = {mach!r}
+alpha = 0.0
+pressure = 1.0
+icType = 1
+nDomains = 1
+domainID = 1
+rho = 1.0
+mach = {mach!r}
+alpha = 0.0
+pressure = 1.0
+fluxFunction = {flux}
+spatialOrder = 2
+limiter = 2
+venk_k = 5.0
+timeOrder = 2
+nRKstages = 3
+CFL = {cfl}
+stationary = F
+tEnd = 1e10
+maxIter = {steps}
+fileName = cylinder
+IOtimeInterval = 1e10
+IOiterInterval = 100000000
+outputFormat = 3
+"""

@@ -332,6 +332,8 @@ int ccfd_server_poll(ccfd_server *s, int steps, int *n_queued, int *n_running, i
  * CCFD_ERR_BUSY while it is queued or running */
 int ccfd_server_result(ccfd_server *s, long id, ccfd_report *rep, double *prim, double times[3]);
 int ccfd_server_memory(ccfd_server *s, size_t *used, size_t *budget);
+/* host seconds spent so far admitting (upload), stepping and retiring */
+int ccfd_server_times(ccfd_server *s, double out[3]);
 
 /* Largest cell count of ccfd_global_residual_noalloc (its static scratch
  * holds one 4-double partial sum per 256 cells: 128 KB). */
