@@ -140,6 +140,15 @@ class CaseData:
     def file_name(self) -> str:
         return self.c.file_name.decode()
 
+    def write_output(self, prim: np.ndarray, time: float, iteration: int) -> str:
+        """Write the state in the reference's output format (CSV) into the
+        current directory; returns the file name."""
+        p = np.ascontiguousarray(prim, dtype=np.float64).reshape(self.n_cells, 4)
+        buf = C.create_string_buffer(600)
+        _check(N.lib.ccfd_write_output(self._ptr, _dptr(p), float(time), int(iteration), buf, 600),
+               "ccfd_write_output")
+        return buf.value.decode()
+
 
 def set_device(device: int) -> None:
     """Bind the calling thread's next contexts to a CUDA device."""
@@ -224,6 +233,19 @@ class Solver:
         _check(N.lib.ccfd_get_profile(self._ctx, C.byref(ms), C.byref(cnt), int(reset)),
                "ccfd_get_profile")
         return ms.value, cnt.value
+
+    def autotune(self, state: np.ndarray | None = None) -> dict:
+        """Pick the stage kernel's tile size and cell ordering by timing
+        (ccfd_autotune); the solver keeps the fastest and `state` (default:
+        the case's initial state)."""
+        c = self.case.c
+        prim = np.ascontiguousarray(self.case.prim0() if state is None else state,
+                                    dtype=np.float64).reshape(self.n, 4)
+        tc, ro, ms = C.c_int(), C.c_int(), C.c_double()
+        _check(N.lib.ccfd_autotune(self._ctx, C.byref(c.mesh), c.bc_table, c.n_bc_table,
+                                   C.byref(c.exact), _dptr(prim), C.byref(tc), C.byref(ro),
+                                   C.byref(ms)), "ccfd_autotune")
+        return {"tile_cells": tc.value, "hilbert_order": bool(ro.value), "ms_per_residual": ms.value}
 
     def device_bytes(self) -> int:
         b = C.c_size_t()

@@ -112,6 +112,9 @@ def _load():
         "ccfd_get_profile": (c_int, [C.c_void_p, P(c_double), P(c_long), c_int]),
         "ccfd_global_residual_noalloc": (c_int, [C.c_void_p, C.c_void_p, c_long, c_double,
                                                  C.c_void_p, C.c_void_p]),
+        "ccfd_autotune": (c_int, [C.c_void_p, P(Mesh), P(BC), c_int, P(Exact), P(c_double), P(c_int),
+                                  P(c_int), P(c_double)]),
+        "ccfd_write_output": (c_int, [C.c_void_p, P(c_double), c_double, c_long, C.c_char_p, C.c_size_t]),
         "ccfd_batch_create": (c_int, [c_int, P(C.c_void_p)]),
         "ccfd_batch_destroy": (None, [C.c_void_p]),
         "ccfd_batch_add": (c_int, [C.c_void_p, C.c_void_p, c_long]),

@@ -66,7 +66,10 @@ def _compile(src: str, force: bool) -> str:
         return obj
     inc = ["-I", INC, "-I", CSRC, "-I", os.path.join(CSRC, "host")]
     if src.endswith(".cu"):
-        cmd = [_nvcc(), *ARCH, "-lineinfo", "-O3", "-std=c++17", "-fmad=false",
+        # FP64 code keeps every multiply and add separately rounded (as the
+        # reference); the mixed-precision kernels may contract them
+        fmad = "-fmad=true" if src.endswith("_mixed.cu") else "-fmad=false"
+        cmd = [_nvcc(), *ARCH, "-lineinfo", "-O3", "-std=c++17", fmad,
                "--expt-relaxed-constexpr", "-Xcompiler", "-fPIC,-ffp-contract=off",
                *inc, "-c", src, "-o", obj]
     elif src.endswith(".cpp"):

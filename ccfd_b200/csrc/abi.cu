@@ -625,6 +625,60 @@ extern "C" int ccfd_residual(ccfd_ctx* ctx, double time, double* u_t_out, double
     return check_flags(ctx);
 }
 
+// Autotuner of the stage kernel's launch shape: cells per tile (which sets
+// the CTA's faces and gradient cells per thread) and the cell ordering
+// (Hilbert curve or the reference's numbering).  Every candidate is uploaded
+// and timed over a few residual evaluations of the given state; the context
+// keeps the fastest.  Results do not depend on the choice (the arithmetic
+// and the summation order per cell are the same for every tiling).
+extern "C" int ccfd_autotune(ccfd_ctx* ctx, const ccfd_mesh* m, const ccfd_bc* bc, int n_bc,
+                             const ccfd_exact* ex, const double* prim, int* tile_cells_out,
+                             int* reorder_out, double* ms_out) {
+    if (!ctx || !m || !ex || !prim) return CCFD_ERR_ARG;
+    if (ctx->batch) return CCFD_ERR_BUSY;
+    CK(cudaSetDevice(ctx->device));
+    static const int kTiles[] = {128, 192, 256, 320, 384};
+    const int kReps = 5;
+    cudaEvent_t e0, e1;
+    CK(cudaEventCreate(&e0));
+    CK(cudaEventCreate(&e1));
+    double best = 1e300;
+    int best_tile = ctx->tile_cells, best_order = 1;
+    for (int order = 1; order >= 0; --order)
+        for (int tc : kTiles) {
+            ctx->tile_cells = tc;
+            int st = ccfd_upload_case(ctx, m, bc, n_bc, ex, order);
+            if (st == CCFD_ERR_ARG) continue;  // tile too large for shared memory
+            if (st || (st = ccfd_set_state(ctx, prim, CCFD_PRIMITIVE))) {
+                cudaEventDestroy(e0);
+                cudaEventDestroy(e1);
+                return st;
+            }
+            if ((st = ccfd_residual_device(ctx, 0.0))) return st;  // warm-up
+            CK(cudaEventRecord(e0, ctx->stream));
+            for (int r = 0; r < kReps; ++r)
+                if ((st = ccfd_residual_device(ctx, 0.0))) return st;
+            CK(cudaEventRecord(e1, ctx->stream));
+            CK(cudaEventSynchronize(e1));
+            float ms = 0.0f;
+            CK(cudaEventElapsedTime(&ms, e0, e1));
+            if (ms / kReps < best) {
+                best = ms / kReps;
+                best_tile = tc;
+                best_order = order;
+            }
+        }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    ctx->tile_cells = best_tile;
+    int st = ccfd_upload_case(ctx, m, bc, n_bc, ex, best_order);
+    if (!st) st = ccfd_set_state(ctx, prim, CCFD_PRIMITIVE);
+    if (tile_cells_out) *tile_cells_out = best_tile;
+    if (reorder_out) *reorder_out = best_order;
+    if (ms_out) *ms_out = best;
+    return st;
+}
+
 extern "C" int ccfd_global_residual(ccfd_ctx* ctx, double res[4]) {
     if (!ctx || !res || !ctx->uploaded) return CCFD_ERR_ARG;
     CK(cudaSetDevice(ctx->device));

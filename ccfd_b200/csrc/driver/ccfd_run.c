@@ -1,0 +1,91 @@
+/*
+ * ccfd_run: command-line driver in the manner of the reference's main
+ * (src/main.c:53-130): reads a case .ini, sets the case up, runs the time
+ * loop on the GPU (explicit Runge-Kutta or implicit Newton / GMRES / LU-SGS
+ * as the .ini selects) and writes the final solution in the reference's
+ * output format.
+ *
+ *   ccfd_run case.ini [--steps N] [--device D] [--no-output]
+ *
+ * --steps N runs at most N time steps.  Exit status 0 on success, 1 on an
+ * error (the message is printed, as the reference prints before exit(1)).
+ */
+#include <stdio.h>
+#include <stdlib.h>
+#include <string.h>
+
+#include "ccfd_b200.h"
+
+static int fail(const char *what, int st)
+{
+	printf("| ERROR: %s: %s\n", what, ccfd_strerror(st));
+	return 1;
+}
+
+int main(int argc, char **argv)
+{
+	const char *ini = NULL;
+	long steps = 0;
+	int device = 0, output = 1;
+	for (int i = 1; i < argc; ++i) {
+		if (!strcmp(argv[i], "--steps") && i + 1 < argc)
+			steps = atol(argv[++i]);
+		else if (!strcmp(argv[i], "--device") && i + 1 < argc)
+			device = atoi(argv[++i]);
+		else if (!strcmp(argv[i], "--no-output"))
+			output = 0;
+		else if (!ini)
+			ini = argv[i];
+		else {
+			fprintf(stderr, "usage: %s case.ini [--steps N] [--device D] [--no-output]\n", argv[0]);
+			return 2;
+		}
+	}
+	if (!ini) {
+		fprintf(stderr, "usage: %s case.ini [--steps N] [--device D] [--no-output]\n", argv[0]);
+		return 2;
+	}
+	int st;
+	ccfd_case *c = NULL;
+	ccfd_ctx *ctx = NULL;
+	if ((st = ccfd_set_device(device)))
+		return fail("device", st);
+	if ((st = ccfd_case_load(ini, &c)))
+		return fail(ini, st);
+	printf("case %s: %ld cells, %ld faces, %ld boundary faces\n", ini, c->mesh.n_cells,
+	       c->mesh.n_faces, c->mesh.n_bc);
+	if ((st = ccfd_create(&c->params, &ctx)))
+		return fail("create", st);
+	if ((st = ccfd_upload_case(ctx, &c->mesh, c->bc_table, c->n_bc_table, &c->exact, 1)))
+		return fail("upload", st);
+	if ((st = ccfd_set_state(ctx, c->prim0, CCFD_PRIMITIVE)))
+		return fail("initial state", st);
+	ccfd_report rep;
+	st = c->params.implicit ? ccfd_run_implicit(ctx, steps, &rep) : ccfd_run_explicit(ctx, steps, &rep);
+	if (st)
+		return fail("time loop", st);
+	printf("iterations %ld  t %.9g  dt %.6g  residual %.6e %.6e %.6e %.6e  device %.3f ms\n",
+	       rep.iterations, rep.t, rep.dt, rep.residual[0], rep.residual[1], rep.residual[2],
+	       rep.residual[3], rep.device_ms);
+	if (c->params.calc_wing)
+		printf("cl %.12g  cd %.12g\n", rep.cl, rep.cd);
+	if (c->params.implicit)
+		printf("newton %ld  gmres %ld\n", rep.newton_iterations, rep.gmres_iterations);
+	if (output) {
+		double *prim = malloc(sizeof(double) * 4 * (size_t)c->mesh.n_cells);
+		if (!prim)
+			return fail("output", CCFD_ERR_NOMEM);
+		if ((st = ccfd_get_state(ctx, prim, CCFD_PRIMITIVE)))
+			return fail("state", st);
+		char path[600];
+		st = ccfd_write_output(c, prim, rep.t, rep.iterations, path, sizeof(path));
+		if (st == CCFD_OK)
+			printf("wrote %s\n", path);
+		else if (st != CCFD_ERR_UNSUPPORTED)
+			return fail("output", st);
+		free(prim);
+	}
+	ccfd_destroy(ctx);
+	ccfd_case_free(c);
+	return 0;
+}

@@ -1,0 +1,85 @@
+/*
+ * Solution output in the reference's formats (src/output.c).
+ *
+ * Only the tabular CSV format (outputFormat = 3, csvOutput,
+ * src/output.c:53-112) is written: cell barycentre x, density, x-velocity
+ * and pressure, rows sorted by x with a stable sort (the reference's bubble
+ * sort is stable too), "%15.9f" columns.  File names follow dataOutput
+ * (src/output.c:348-353): <fileName>_<iter %09ld>.csv for stationary runs,
+ * <fileName>_<time %015.7f>.csv otherwise.  CGNS and curve output are not
+ * built (CCFD_ERR_UNSUPPORTED).
+ */
+#include <stdio.h>
+#include <stdlib.h>
+#include <string.h>
+
+#include "ccfd_b200.h"
+
+static void merge_sort_by_x(long *idx, long *tmp, const double *x, long n)
+{
+	/* bottom-up stable merge sort of indices by x */
+	for (long w = 1; w < n; w *= 2) {
+		for (long lo = 0; lo < n; lo += 2 * w) {
+			long mid = lo + w < n ? lo + w : n;
+			long hi = lo + 2 * w < n ? lo + 2 * w : n;
+			long a = lo, b = mid, k = lo;
+			while (a < mid && b < hi)
+				tmp[k++] = (x[idx[b]] < x[idx[a]]) ? idx[b++] : idx[a++];
+			while (a < mid)
+				tmp[k++] = idx[a++];
+			while (b < hi)
+				tmp[k++] = idx[b++];
+		}
+		memcpy(idx, tmp, sizeof(long) * n);
+	}
+}
+
+int ccfd_write_output(const ccfd_case *c, const double *prim, double time, long iter,
+		      char *path, size_t path_len)
+{
+	if (!c || !prim)
+		return CCFD_ERR_ARG;
+	if (c->output_format != 3)
+		return CCFD_ERR_UNSUPPORTED;
+	char name[600];
+	if (c->params.stationary)
+		snprintf(name, sizeof(name), "%s_%09ld.csv", c->file_name, iter);
+	else
+		snprintf(name, sizeof(name), "%s_%015.7f.csv", c->file_name, time);
+	if (path && path_len) {
+		strncpy(path, name, path_len - 1);
+		path[path_len - 1] = '\0';
+	}
+	const long n = c->mesh.n_cells;
+	long *idx = malloc(sizeof(long) * (size_t)(n > 0 ? n : 1));
+	long *tmp = malloc(sizeof(long) * (size_t)(n > 0 ? n : 1));
+	double *x = malloc(sizeof(double) * (size_t)(n > 0 ? n : 1));
+	if (!idx || !tmp || !x) {
+		free(idx);
+		free(tmp);
+		free(x);
+		return CCFD_ERR_NOMEM;
+	}
+	for (long i = 0; i < n; ++i) {
+		idx[i] = i;
+		x[i] = c->mesh.cell_bary[2 * i];
+	}
+	merge_sort_by_x(idx, tmp, x, n);
+	FILE *f = fopen(name, "w");
+	if (!f) {
+		free(idx);
+		free(tmp);
+		free(x);
+		return CCFD_ERR_ARG;
+	}
+	fprintf(f, "CoordinateX, Density, Velocity, Pressure\n");
+	for (long k = 0; k < n; ++k) {
+		long i = idx[k];
+		fprintf(f, "%15.9f,%15.9f,%15.9f,%15.9f\n", x[i], prim[4 * i], prim[4 * i + 1], prim[4 * i + 3]);
+	}
+	fclose(f);
+	free(idx);
+	free(tmp);
+	free(x);
+	return CCFD_OK;
+}

@@ -1,0 +1,4 @@
+// Mixed-precision stage kernels of convective flux 1 (fluxFunction = 1).
+#define CCFD_FLUX_ID 1
+#define CCFD_FLUX_FP32 1
+#include "stage_flux.inc"

@@ -1,0 +1,4 @@
+// Mixed-precision stage kernels of convective flux 5 (fluxFunction = 5).
+#define CCFD_FLUX_ID 5
+#define CCFD_FLUX_FP32 1
+#include "stage_flux.inc"

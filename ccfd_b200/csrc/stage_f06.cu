@@ -1,3 +1,4 @@
-// Stage kernels of convective flux 6 (fluxFunction = 6).
+// FP64 stage kernels of convective flux 6 (fluxFunction = 6).
 #define CCFD_FLUX_ID 6
+#define CCFD_FLUX_FP32 0
 #include "stage_flux.inc"

@@ -1,0 +1,4 @@
+// Mixed-precision stage kernels of convective flux 7 (fluxFunction = 7).
+#define CCFD_FLUX_ID 7
+#define CCFD_FLUX_FP32 1
+#include "stage_flux.inc"

@@ -282,6 +282,24 @@ int ccfd_get_profile(ccfd_ctx *ctx, double *residual_ms, long *residual_count,
 /* Drop-in for globalResidual on the last residual (src/analyze.c:521-539). */
 int ccfd_global_residual(ccfd_ctx *ctx, double res[4]);
 
+/* Autotuner (no counterpart in the reference): re-uploads the case with
+ * each candidate launch shape of the stage kernel (cells per tile 128..384,
+ * Hilbert or reference cell order), times residual evaluations of state prim
+ * ([n_cells][4] primitive, reference order) and keeps the fastest; the
+ * context ends uploaded with that shape and with prim as its state.  Results
+ * are independent of the shape.  Outputs may be NULL. */
+int ccfd_autotune(ccfd_ctx *ctx, const ccfd_mesh *m, const ccfd_bc *bc, int n_bc,
+		  const ccfd_exact *ex, const double *prim, int *tile_cells, int *reorder,
+		  double *ms_per_residual);
+
+/* Final-solution output in the reference's format (dataOutput / csvOutput,
+ * src/output.c:53-112, 348-372): only outputFormat = 3 (CSV) is written,
+ * named <fileName>_<iter %09ld>.csv (stationary) or <fileName>_<time
+ * %015.7f>.csv; prim is [n_cells][4] in reference order; the file name is
+ * returned in path (may be NULL).  CCFD_ERR_UNSUPPORTED for CGNS / curve. */
+int ccfd_write_output(const ccfd_case *c, const double *prim, double time, long iter,
+		      char *path, size_t path_len);
+
 /* ------------------------------------------------------------- batching
  * Many contexts stepped together on one GPU (no counterpart in the
  * reference, which runs one case per process).  A member is an uploaded

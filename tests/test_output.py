@@ -1,0 +1,66 @@
+"""Solution output in the reference's CSV format and the command-line
+driver.
+
+The writer is checked on the CPU with the oracle's state of the reference's
+own regression cases (check/*.ini): the written file must reproduce the
+golden CSV within the reference's tolerance (Frobenius norm of the
+differences of x, density and velocity <= 1e-5, check/check.py:33-42).  The
+driver (ccfd_run) runs the same cases on the GPU.
+"""
+import os
+import re
+import subprocess
+import tempfile
+
+import numpy as np
+import pytest
+
+import ccfd_b200 as cc
+from oracle import restated
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+DRIVER = os.path.join(ROOT, "ccfd_b200", "lib", "ccfd_run")
+
+
+def _frobenius_vs_golden(path, g):
+    data = np.genfromtxt(path, skip_header=1, delimiter=",")
+    gold = np.stack([g["x"], g["rho"], g["u"]], 1)
+    return float(np.linalg.norm(data[:, 0:3] - gold))
+
+
+def test_csv_writer_reproduces_golden_output(sod_check):
+    for name in ("sod_FF02", "sod_SO2_VK", "sod_TO2_4RK"):
+        g = sod_check[name]
+        case = cc.CaseData.from_text(g["ini"])
+        prim, info = restated.run_explicit(case)
+        cwd = os.getcwd()
+        with tempfile.TemporaryDirectory() as tmp:
+            os.chdir(tmp)
+            try:
+                path = case.write_output(prim, info["t"], info["iterations"])
+                assert path == g["target"]
+                assert _frobenius_vs_golden(path, g) < 1e-5
+            finally:
+                os.chdir(cwd)
+
+
+def test_writer_refuses_formats_it_does_not_build(sod_check):
+    g = sod_check["sod_FF02"]
+    ini = re.sub(r"(?im)^(\s*outputformat\s*=\s*)3", r"\g<1>1", g["ini"])
+    case = cc.CaseData.from_text(ini)
+    assert case.c.output_format == 1
+    with pytest.raises(cc.CcfdError):
+        case.write_output(case.prim0(), 0.0, 0)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name", ["sod_FF05", "sod_SO2_BJ", "sod_TO2_3RK"])
+def test_driver_runs_regression_case(sod_check, name):
+    g = sod_check[name]
+    with tempfile.TemporaryDirectory() as tmp:
+        with open(os.path.join(tmp, "case.ini"), "w") as f:
+            f.write(g["ini"])
+        r = subprocess.run([DRIVER, "case.ini"], cwd=tmp, capture_output=True, text=True, timeout=300)
+        assert r.returncode == 0, r.stdout + r.stderr
+        assert f"wrote {g['target']}" in r.stdout
+        assert _frobenius_vs_golden(os.path.join(tmp, g["target"]), g) < 1e-5
