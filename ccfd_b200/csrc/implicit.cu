@@ -40,6 +40,7 @@
 
 #include <algorithm>
 #include <map>
+#include <thread>
 #include <tuple>
 #include <vector>
 
@@ -112,7 +113,7 @@ struct ImpState {
     int* color_cells = nullptr;
     int* twin = nullptr;         // [H] half-side of the neighbour that points back
     // LU-SGS level schedules
-    int n_lev_f = 0, n_lev_b = 0;
+    int n_lev_f = 0, n_lev_b = 0, max_level = 0;
     int *lev_f_off = nullptr, *fw_cell = nullptr, *lev_b_off = nullptr, *bw_cell = nullptr;
     int4 *fw_nb = nullptr, *fw_h = nullptr, *bw_nb = nullptr, *bw_h = nullptr;
     bool ready = false;
@@ -730,8 +731,11 @@ __device__ __forceinline__ void sweep(int nl, const int* __restrict__ off, const
 }
 
 // One CTA per member: the forward sweep, then the backward sweep
-// (src/linearSolver.c:261-333): Z_m = LU-SGS(V_m).
-__global__ void __launch_bounds__(kSweepThreads) kb_lusgs(const ImpDev* __restrict__ I, int m) {
+// (src/linearSolver.c:261-333): Z_m = LU-SGS(V_m); THREADS / 4 cells of a
+// level per pass.  512 threads: 1024 would take wide levels in one pass,
+// but the register cap they impose spills and is slower (measured).
+template <int THREADS>
+__global__ void __launch_bounds__(THREADS) kb_lusgs(const ImpDev* __restrict__ I, int m) {
     const ImpDev& d = I[blockIdx.x];
     if (!d.precond || !gmres_on(d)) return;
     const double* B = reinterpret_cast<const double*>(d.V + (long)m * d.N);
@@ -841,35 +845,51 @@ int ccfd_implicit_setup(ccfd_ctx* ctx, const std::vector<int>& hs_off, const std
                     }
             }
         // distance-3 greedy colouring: a cell's colour differs from every
-        // cell within three face-neighbour steps
-        std::vector<int> color(N, -1), mark(N, -1), frontier, next, seen;
-        int ncol = 0;
-        std::vector<int> used;
-        for (long d = 0; d < N; ++d) {
-            seen.clear();
-            frontier.assign(1, (int)d);
-            mark[d] = (int)d;
-            seen.push_back((int)d);
-            for (int r = 0; r < 3; ++r) {
-                next.clear();
-                for (int c : frontier)
-                    for (int h = hs_off[c]; h < hs_off[c + 1]; ++h) {
-                        int e = hs_nb[h];
-                        if (e >= 0 && mark[e] != (int)d) {
-                            mark[e] = (int)d;
-                            next.push_back(e);
-                            seen.push_back(e);
+        // cell within three face-neighbour steps.  The colour count depends
+        // on the order the greedy pass visits the cells; the Jacobian does
+        // not (any valid colouring gives the same entries), so the fewest
+        // colours of a few visiting orders win.
+        auto greedy = [&](const std::vector<int>& order, std::vector<int>& color) {
+            color.assign(N, -1);
+            std::vector<int> mark(N, -1), frontier, next, seen, used;
+            int ncol = 0;
+            for (long k = 0; k < N; ++k) {
+                const int d = order[k];
+                seen.clear();
+                frontier.assign(1, d);
+                mark[d] = d;
+                seen.push_back(d);
+                for (int r = 0; r < 3; ++r) {
+                    next.clear();
+                    for (int c : frontier)
+                        for (int h = hs_off[c]; h < hs_off[c + 1]; ++h) {
+                            int e = hs_nb[h];
+                            if (e >= 0 && mark[e] != d) {
+                                mark[e] = d;
+                                next.push_back(e);
+                                seen.push_back(e);
+                            }
                         }
-                    }
-                frontier.swap(next);
+                    frontier.swap(next);
+                }
+                used.assign(ncol + 1, 0);
+                for (int e : seen)
+                    if (color[e] >= 0) used[color[e]] = 1;
+                int c = 0;
+                while (c < ncol && used[c]) ++c;
+                color[d] = c;
+                if (c == ncol) ++ncol;
             }
-            used.assign(ncol + 1, 0);
-            for (int e : seen)
-                if (color[e] >= 0) used[color[e]] = 1;
-            int c = 0;
-            while (c < ncol && used[c]) ++c;
-            color[d] = c;
-            if (c == ncol) ++ncol;
+            return ncol;
+        };
+        std::vector<int> color, trial, order(N);
+        for (long d = 0; d < N; ++d) order[d] = (int)d;
+        int ncol = greedy(order, color);
+        for (long i = 0; i < N; ++i) order[i] = ctx->dev_of_cell[i];  // reference numbering
+        int nc2 = greedy(order, trial);
+        if (nc2 < ncol) {
+            ncol = nc2;
+            color.swap(trial);
         }
         std::vector<int> coff(ncol + 1, 0), ccells(N);
         for (long d = 0; d < N; ++d) coff[color[d] + 1]++;
@@ -943,6 +963,8 @@ int ccfd_implicit_setup(ccfd_ctx* ctx, const std::vector<int>& hs_off, const std
         pack(lbc, up_off, up_nb, up_h, bwn, bwh);
         S->n_lev_f = nlf;
         S->n_lev_b = nlb;
+        for (int l = 0; l < nlf; ++l) S->max_level = std::max(S->max_level, lfo[l + 1] - lfo[l]);
+        for (int l = 0; l < nlb; ++l) S->max_level = std::max(S->max_level, lbo[l + 1] - lbo[l]);
         if ((st = iupload(ctx, &S->twin, twin)) || (st = iupload(ctx, &S->color_cells, ccells)) ||
             (st = iupload(ctx, &S->color_off_d, coff)) ||
             (st = iupload(ctx, &S->lev_f_off, lfo)) || (st = iupload(ctx, &S->fw_cell, lfc)) ||
@@ -976,6 +998,7 @@ struct ImpSet {
     ImpDev* dev = nullptr;
     std::vector<ImpGroup> groups;
     int n = 0, max_nb = 0, max_col = 0, max_colsize = 0, max_K = 0, max_newton = 0;
+    int max_level = 0;  // widest LU-SGS level (cells) over the members
     bool any_precond = false;
     int* d_count = nullptr;
     int* h_count = nullptr;
@@ -1060,6 +1083,7 @@ static int set_build(const std::vector<ccfd_ctx*>& members, cudaStream_t stream,
             M->max_col = std::max(M->max_col, ncol);
             for (int c = 0; c < ncol; ++c)
                 M->max_colsize = std::max(M->max_colsize, S->color_off[c + 1] - S->color_off[c]);
+            M->max_level = std::max(M->max_level, S->max_level);
         }
         StageLaunch probe;
         ccfd_fill_stage(ctx, probe);
@@ -1188,7 +1212,7 @@ static int set_step(ImpSet* M) {
             kb_jac_check<<<g1, 32, 0, st>>>(M->dev);
         }
         for (int m = 0; m < M->max_K; ++m) {
-            if (M->any_precond) kb_lusgs<<<M->n, kSweepThreads, 0, st>>>(M->dev, m);
+            if (M->any_precond) kb_lusgs<kSweepThreads><<<M->n, kSweepThreads, 0, st>>>(M->dev, m);
             kb_copy_vz<<<gv, kB, 0, st>>>(M->dev, m);
             // matrixVector: epsFD = sqrt(eps) / |Z|
             kb_dot_zz<<<gv, kB, 0, st>>>(M->dev, m);
@@ -1314,14 +1338,30 @@ extern "C" int ccfd_run_implicit(ccfd_ctx* ctx, long nsteps, ccfd_report* report
 // ---------------------------------------------------------------- batching
 // The implicit members of a batch form one lockstep set on the batch stream
 // (rebuilt when the membership changes).
+// The implicit members of a batch are split into a few lockstep sets, each
+// driven by its own host thread on its own stream: the latency-bound work of
+// one set (LU-SGS sweeps, reductions) overlaps on the device with the
+// throughput-bound residual evaluations of the others.  Rebuilt when the
+// membership changes.
 struct BatchImp {
-    ImpSet* set = nullptr;
+    std::vector<ImpSet*> sets;
+    std::vector<cudaStream_t> streams;
     std::vector<ccfd_ctx*> key;
 };
 static std::map<const ccfd_batch*, BatchImp> g_batch_imp;
 
+static void batch_imp_free(BatchImp& bi) {
+    for (ImpSet* M : bi.sets) set_free(M);
+    for (cudaStream_t st : bi.streams) {
+        cudaStreamSynchronize(st);
+        cudaStreamDestroy(st);
+    }
+    bi.sets.clear();
+    bi.streams.clear();
+    bi.key.clear();
+}
+
 cudaStream_t ccfd_batch_stream(ccfd_batch* b);
-cudaStream_t ccfd_batch_implicit_stream(ccfd_batch* b);
 
 int ccfd_implicit_batch_join(ccfd_batch* b, ccfd_ctx* ctx) {
     ImpState* S = (ImpState*)ctx->implicit_state;
@@ -1337,10 +1377,8 @@ int ccfd_implicit_batch_join(ccfd_batch* b, ccfd_ctx* ctx) {
 int ccfd_implicit_batch_leave(ccfd_batch* b, ccfd_ctx* ctx) {
     auto it = g_batch_imp.find(b);
     if (it != g_batch_imp.end()) {
-        if (it->second.set) {
-            set_pull_counts(it->second.set);
-            set_free(it->second.set);
-        }
+        for (ImpSet* M : it->second.sets) set_pull_counts(M);
+        batch_imp_free(it->second);
         g_batch_imp.erase(it);
     }
     (void)ctx;
@@ -1350,31 +1388,62 @@ int ccfd_implicit_batch_leave(ccfd_batch* b, ccfd_ctx* ctx) {
 void ccfd_implicit_batch_release(ccfd_batch* b) {
     auto it = g_batch_imp.find(b);
     if (it == g_batch_imp.end()) return;
-    if (it->second.set) set_free(it->second.set);
+    batch_imp_free(it->second);
     g_batch_imp.erase(it);
 }
 
-int ccfd_implicit_batch_steps(ccfd_batch* b, const std::vector<ccfd_ctx*>& members, int steps) {
-    BatchImp& bi = g_batch_imp[b];
-    if (bi.key != members) {
-        if (bi.set) set_free(bi.set);
-        bi.set = nullptr;
-        bi.key = members;
-        int s = set_build(members, ccfd_batch_implicit_stream(b), &bi.set);
-        if (s) return s;
-    }
-    ImpSet* M = bi.set;
+// up to `steps` implicit time steps of one lockstep set
+static int set_steps(ImpSet* M, int device, int steps) {
+    if (cudaSetDevice(device) != cudaSuccess) return CCFD_ERR_CUDA;
     for (int k = 0; k < steps; ++k) {
         // members that can still step
         int any = 0;
-        for (ccfd_ctx* ctx : members) {
+        for (ccfd_ctx* ctx : M->members)
             CKM(cudaMemcpyAsync(ctx->h_ctrl, ctx->ctrl, sizeof(Ctrl), cudaMemcpyDeviceToHost, M->stream));
-        }
         CKM(cudaStreamSynchronize(M->stream));
-        for (ccfd_ctx* ctx : members) any |= ctx->h_ctrl->active && !ctx->h_ctrl->done;
+        for (ccfd_ctx* ctx : M->members) any |= ctx->h_ctrl->active && !ctx->h_ctrl->done;
         if (!any) break;
         int s = set_step(M);
         if (s) return s;
     }
     return set_pull_counts(M);
+}
+
+int ccfd_implicit_batch_steps(ccfd_batch* b, const std::vector<ccfd_ctx*>& members, int steps) {
+    BatchImp& bi = g_batch_imp[b];
+    if (bi.key != members) {
+        batch_imp_free(bi);
+        bi.key = members;
+        // sets balanced by cell count (largest first onto the lightest set)
+        const int nsets = std::max(1, std::min(4, (int)members.size() / 4));
+        std::vector<int> idx(members.size());
+        for (size_t k = 0; k < idx.size(); ++k) idx[k] = (int)k;
+        std::stable_sort(idx.begin(), idx.end(), [&](int a, int c) { return members[a]->N > members[c]->N; });
+        std::vector<std::vector<ccfd_ctx*>> parts(nsets);
+        std::vector<long> load(nsets, 0);
+        for (int k : idx) {
+            int j = (int)(std::min_element(load.begin(), load.end()) - load.begin());
+            parts[j].push_back(members[k]);
+            load[j] += members[k]->N;
+        }
+        for (int j = 0; j < nsets; ++j) {
+            cudaStream_t st;
+            if (cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking) != cudaSuccess) return CCFD_ERR_CUDA;
+            bi.streams.push_back(st);
+            ImpSet* M = nullptr;
+            int s = set_build(parts[j], st, &M);
+            bi.sets.push_back(M);
+            if (s) return s;
+        }
+    }
+    int device = members[0]->device;
+    std::vector<int> status(bi.sets.size(), CCFD_OK);
+    std::vector<std::thread> threads;
+    for (size_t j = 1; j < bi.sets.size(); ++j)
+        threads.emplace_back([&, j] { status[j] = set_steps(bi.sets[j], device, steps); });
+    status[0] = set_steps(bi.sets[0], device, steps);
+    for (auto& t : threads) t.join();
+    for (int s : status)
+        if (s) return s;
+    return CCFD_OK;
 }

@@ -85,12 +85,31 @@ def _main(argv=None) -> int:
     """python -m ccfd_b200.workloads airfoil NI NJ STEPS [CFL]: one steady
     airfoil (m 0.02, p 0.4, t 0.12, Mach 0.5, 1 degree) through the implicit
     solver on device 0; prints cells, steps, Newton / GMRES iterations and
-    device milliseconds."""
+    device milliseconds.
+    python -m ccfd_b200.workloads batch N STEPS [CFL]: the first N airfoils
+    of the batched distribution stepped together in one batch; prints the
+    total cells, Newton / GMRES iterations and batch device milliseconds."""
     import sys
     import tempfile
 
     import ccfd_b200 as cc
     args = sys.argv[1:] if argv is None else argv
+    if len(args) >= 3 and args[0] == "batch":
+        n, steps = int(args[1]), int(args[2])
+        cfl = float(args[3]) if len(args) > 3 else 1.0
+        cc.set_device(0)
+        with tempfile.TemporaryDirectory() as tmp:
+            cases = [airfoil_case(sp, tmp, f"af{k}", cfl=cfl) for k, sp in enumerate(airfoil_specs(n))]
+        b = cc.Batch(0)
+        members = [cc.Solver(c) for c in cases]
+        for s in members:
+            b.add(s, steps)
+        b.step(steps)
+        reps = [b.report(s) for s in members]
+        print(sum(c.n_cells for c in cases), sum(r["newton_iterations"] for r in reps),
+              sum(r["gmres_iterations"] for r in reps), f"{reps[0]['device_ms']:.3f}")
+        b.close()
+        return 0
     if len(args) < 4 or args[0] != "airfoil":
         print(_main.__doc__)
         return 2
