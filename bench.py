@@ -157,50 +157,69 @@ def run_mixed(tmpdir: str, steps: int, warmup: int, prim_fp64, nrk: int, bytes_s
 def run_batched_airfoils(n_cases: int, steps: int, cfl: float) -> dict:
     """Steady-Euler airfoils of the batched distribution: the plain FP64 GPU
     solver looping over the cases one at a time vs all cases in one batch
-    (lockstep Newton / GMRES / LU-SGS launches over every member).  A solve
-    is `steps` implicit time steps of one airfoil; both forms do the same
-    iterations and give bit-identical states (checked)."""
+    (lockstep Newton / GMRES / LU-SGS sets over all members), in FP64 and in
+    mixed precision (FP32 Krylov basis and LU-SGS).  A solve is `steps`
+    implicit time steps of one airfoil.  The FP64 batch gives states
+    bit-identical to the loop (checked); the mixed batch states its error
+    against the FP64 loop."""
     import ccfd_b200 as cc
     from ccfd_b200 import workloads
     specs = workloads.airfoil_specs(n_cases)
     with tempfile.TemporaryDirectory() as tmp:
         cases = [workloads.airfoil_case(sp, tmp, f"af{k}", cfl=cfl) for k, sp in enumerate(specs)]
+        mixed = [workloads.airfoil_case(sp, tmp, f"af{k}", cfl=cfl, precision=1) for k, sp in enumerate(specs)]
     cells = [c.n_cells for c in cases]
-    loop_ms, loop_states, t0 = 0.0, [], time.perf_counter()
+    loop_ms, loop_states, loop_reps, t0 = 0.0, [], [], time.perf_counter()
     for c in cases:
         s = cc.Solver(c)
         rep = s.run(steps)
         loop_ms += rep["device_ms"]
         loop_states.append(s.get_state())
+        loop_reps.append(rep)
         s.close()
     loop_wall = time.perf_counter() - t0
-    b = cc.Batch(0)
-    members = [cc.Solver(c) for c in cases]
-    for s in members:
-        b.add(s, steps)
-    t0 = time.perf_counter()
-    b.step(steps)
-    batch_wall = time.perf_counter() - t0
-    reps = [b.report(s) for s in members]
-    batch_ms = reps[0]["device_ms"]
-    diff = max(float(np.abs(s.get_state() - ls).max()) for s, ls in zip(members, loop_states))
-    b.close()
-    for s in members:
-        s.close()
+
+    def batched(cs):
+        b = cc.Batch(0)
+        members = [cc.Solver(c) for c in cs]
+        for s in members:
+            b.add(s, steps)
+        t1 = time.perf_counter()
+        b.step(steps)
+        wall = time.perf_counter() - t1
+        reps = [b.report(s) for s in members]
+        states = [s.get_state() for s in members]
+        b.close()
+        for s in members:
+            s.close()
+        return reps, states, reps[0]["device_ms"], wall
+
+    reps, states, batch_ms, batch_wall = batched(cases)
+    diff = max(float(np.abs(st - ls).max()) for st, ls in zip(states, loop_states))
+    mreps, mstates, mixed_ms, mixed_wall = batched(mixed)
+    merr = max(float((np.abs(st - ls).max(axis=0) / np.abs(ls).max(axis=0)).max())
+               for st, ls in zip(mstates, loop_states))
+    mcl = max(abs(a["cl"] - b["cl"]) for a, b in zip(mreps, loop_reps))
+    mcd = max(abs(a["cd"] - b["cd"]) for a, b in zip(mreps, loop_reps))
     return {
         "workload": f"{n_cases} NACA airfoils of the batched distribution (seed 20260004), O-grids "
                     f"{min(cells)}..{max(cells)} cells, steady Euler, Roe, 2nd order VK K=5, JFNK-GMRES "
-                    f"(Krylov 30) + LU-SGS, CFL {cfl}, {steps} implicit steps per solve, FP64",
+                    f"(Krylov 30) + LU-SGS, CFL {cfl}, {steps} implicit steps per solve",
         "cells_total": int(sum(cells)), "solves": n_cases,
-        "loop": {"device_s": loop_ms / 1e3, "wall_s": loop_wall,
-                 "solves_per_s": n_cases / (loop_ms / 1e3)},
-        "batched": {"device_s": batch_ms / 1e3, "wall_s": batch_wall,
-                    "solves_per_s": n_cases / (batch_ms / 1e3)},
-        "speedup": loop_ms / batch_ms,
-        "max_state_diff_batched_vs_loop": diff,
+        "loop_fp64": {"device_s": loop_ms / 1e3, "wall_s": loop_wall,
+                      "solves_per_s": n_cases / (loop_ms / 1e3)},
+        "batched_fp64": {"device_s": batch_ms / 1e3, "wall_s": batch_wall,
+                         "solves_per_s": n_cases / (batch_ms / 1e3),
+                         "max_state_diff_vs_loop": diff},
+        "batched_mixed": {"device_s": mixed_ms / 1e3, "wall_s": mixed_wall,
+                          "solves_per_s": n_cases / (mixed_ms / 1e3),
+                          "state_rel_err_vs_fp64_loop": merr, "cl_err": mcl, "cd_err": mcd,
+                          "gmres_iterations": sum(r["gmres_iterations"] for r in mreps)},
+        "speedup_batched_fp64": loop_ms / batch_ms,
+        "speedup_batched_mixed": loop_ms / mixed_ms,
         "newton_iterations": sum(r["newton_iterations"] for r in reps),
         "gmres_iterations": sum(r["gmres_iterations"] for r in reps),
-        "failed": sum(1 for r in reps if r["status"] != 0),
+        "failed": sum(1 for r in reps + mreps if r["status"] != 0),
     }
 
 

@@ -81,6 +81,12 @@ struct ImpDev {
     double gam1, eps_gmres, eps2newton;
     double4 *XK, *Q, *RXK, *F, *dX, *W, *V, *Z, *ptmp, *ut, *dxs, *cons, *prim, *pert;
     double *D, *Dinv, *O, *sc, *partial;
+    // mixed precision (fp32 = 1): Krylov basis V, Z, the sweep vector and the
+    // LU-SGS blocks D^-1, O in FP32 (Vf, Zf, dxsf, Dinvf, Of instead of the
+    // FP64 arrays); residuals, W, the Newton update and GMRES scalars FP64
+    int fp32;
+    float4 *Vf, *Zf, *dxsf;
+    float *Dinvf, *Of;
     int* flag;  // [0] GMRES cycle done, [1] final m, [2] singular, [3] non-finite
     int* ctl;   // Ctl words
     Ctrl* ctrl;
@@ -102,6 +108,9 @@ struct ImpState {
     double4 *W = nullptr, *V = nullptr, *Z = nullptr, *ptmp = nullptr, *ut = nullptr;
     double4 *dxs = nullptr;
     double *D = nullptr, *Dinv = nullptr, *O = nullptr;  // [N][16], [N][16], [H][16]
+    bool fp32 = false;           // mixed precision: the FP32 arrays below instead
+    float4 *Vf = nullptr, *Zf = nullptr, *dxsf = nullptr;
+    float *Dinvf = nullptr, *Of = nullptr;
     double* sc = nullptr;        // device scalars
     int* flag = nullptr;         // [0] gmres done, [1] m_final, [2] singular, [3] non-finite
     int* ctl = nullptr;          // Ctl words
@@ -148,6 +157,30 @@ __device__ __forceinline__ void block_partial(double v, double* partial) {
         for (int o = 16; o > 0; o >>= 1) x += __shfl_down_sync(0xffffffffu, x, o);
         if (lane == 0) partial[blockIdx.x] = x;
     }
+}
+
+// Krylov basis access in the member's precision (FP64 arithmetic outside)
+__device__ __forceinline__ double4 getV(const ImpDev& d, long k) {
+    if (d.fp32) {
+        float4 v = d.Vf[k];
+        return make_double4(v.x, v.y, v.z, v.w);
+    }
+    return d.V[k];
+}
+__device__ __forceinline__ double4 getZ(const ImpDev& d, long k) {
+    if (d.fp32) {
+        float4 v = d.Zf[k];
+        return make_double4(v.x, v.y, v.z, v.w);
+    }
+    return d.Z[k];
+}
+__device__ __forceinline__ void putV(const ImpDev& d, long k, double4 v) {
+    if (d.fp32) d.Vf[k] = make_float4((float)v.x, (float)v.y, (float)v.z, (float)v.w);
+    else d.V[k] = v;
+}
+__device__ __forceinline__ void putZ(const ImpDev& d, long k, double4 v) {
+    if (d.fp32) d.Zf[k] = make_float4((float)v.x, (float)v.y, (float)v.z, (float)v.w);
+    else d.Z[k] = v;
 }
 
 __device__ __forceinline__ bool newton_on(const ImpDev& d) { return d.ctl[CTL_NEWTON] != 0; }
@@ -292,7 +325,7 @@ __global__ void kb_gmres_init(const ImpDev* __restrict__ I) {
     ld(d.F[i], b);
 #pragma unroll
     for (int k = 0; k < 4; ++k) v[k] = -b[k] / nr;
-    d.V[i] = mk(v);
+    putV(d, i, mk(v));
     d.dX[i] = make_double4(0.0, 0.0, 0.0, 0.0);
 }
 
@@ -311,7 +344,7 @@ __global__ void kb_copy_vz(const ImpDev* __restrict__ I, int m) {
     MEMBER;
     if (d.precond || !gmres_on(d)) return;
     CELL_INDEX;
-    if (i < d.N) d.Z[(long)m * d.N + i] = d.V[(long)m * d.N + i];
+    if (i < d.N) putZ(d, (long)m * d.N + i, getV(d, (long)m * d.N + i));
 }
 
 __global__ void kb_dot_zz(const ImpDev* __restrict__ I, int m) {
@@ -320,7 +353,7 @@ __global__ void kb_dot_zz(const ImpDev* __restrict__ I, int m) {
     CELL_INDEX;
     double v = 0.0;
     if (i < d.N) {
-        double4 z = d.Z[(long)m * d.N + i];
+        double4 z = getZ(d, (long)m * d.N + i);
         v = cell_dot(z, z);
     }
     block_partial(v, d.partial);
@@ -334,7 +367,7 @@ __global__ void kb_mv_prep(const ImpDev* __restrict__ I, int m) {
     if (i >= d.N) return;
     double x[4], z[4], c[4], p[4];
     ld(d.XK[i], x);
-    ld(d.Z[(long)m * d.N + i], z);
+    ld(getZ(d, (long)m * d.N + i), z);
     double e = d.sc[SC_EPSFD];
 #pragma unroll
     for (int k = 0; k < 4; ++k) c[k] = x[k] + e * z[k];
@@ -352,7 +385,7 @@ __global__ void kb_mv_finish(const ImpDev* __restrict__ I, int m) {
     if (i < d.N) {
         const double adt = 1.0 * d.ctrl->dt;
         double z[4], u[4], r[4], w[4];
-        ld(d.Z[(long)m * d.N + i], z);
+        ld(getZ(d, (long)m * d.N + i), z);
         ld(d.ut[i], u);
         ld(d.RXK[i], r);
         double e = d.sc[SC_EPSFD];
@@ -360,7 +393,7 @@ __global__ void kb_mv_finish(const ImpDev* __restrict__ I, int m) {
         for (int k = 0; k < 4; ++k) w[k] = z[k] - adt * (u[k] - r[k]) / e;
         double4 wv = mk(w);
         d.W[i] = wv;
-        dd = cell_dot(d.V[i], wv);
+        dd = cell_dot(getV(d, i), wv);
     }
     block_partial(dd, d.partial);
 }
@@ -375,13 +408,13 @@ __global__ void kb_mgs(const ImpDev* __restrict__ I, int nn, int m) {
     if (i < d.N) {
         double w[4], p[4];
         ld(d.W[i], w);
-        ld(d.V[(long)nn * d.N + i], p);
+        ld(getV(d, (long)nn * d.N + i), p);
         double hh = d.sc[SC_H + nn * (d.K + 1) + m];
 #pragma unroll
         for (int k = 0; k < 4; ++k) w[k] -= hh * p[k];
         double4 wv = mk(w);
         d.W[i] = wv;
-        dd = nn < m ? cell_dot(d.V[(long)(nn + 1) * d.N + i], wv) : cell_dot(wv, wv);
+        dd = nn < m ? cell_dot(getV(d, (long)(nn + 1) * d.N + i), wv) : cell_dot(wv, wv);
     }
     block_partial(dd, d.partial);
 }
@@ -434,7 +467,7 @@ __global__ void kb_vnext(const ImpDev* __restrict__ I, int m) {
     double hh = d.sc[SC_H + (m + 1) * (d.K + 1) + m];
 #pragma unroll
     for (int k = 0; k < 4; ++k) w[k] = w[k] / hh;
-    d.V[(long)(m + 1) * d.N + i] = mk(w);
+    putV(d, (long)(m + 1) * d.N + i, mk(w));
 }
 
 // end of a GMRES cycle: iteration count, breakdown test
@@ -459,7 +492,7 @@ __global__ void kb_newton_update(const ImpDev* __restrict__ I) {
     ld(d.dX[i], x);
     for (int nn = 0; nn <= m; ++nn) {
         double z[4];
-        ld(d.Z[(long)nn * d.N + i], z);
+        ld(getZ(d, (long)nn * d.N + i), z);
         double a = alp[nn];
 #pragma unroll
         for (int k = 0; k < 4; ++k) x[k] += a * z[k];
@@ -549,7 +582,11 @@ __global__ void kb_jac_collect(const ImpDev* __restrict__ I, int c, int v) {
         ld(d.RXK[e], r);
         long t = d.twin[h];
 #pragma unroll
-        for (int j = 0; j < 4; ++j) d.O[16 * t + 4 * j + v] = 0.0 + (u[j] - r[j]) * sreps;
+        for (int j = 0; j < 4; ++j) {
+            const double o = 0.0 + (u[j] - r[j]) * sreps;
+            if (d.fp32) d.Of[16 * t + 4 * j + v] = (float)o;
+            else d.O[16 * t + 4 * j + v] = o;
+        }
     }
 }
 
@@ -610,11 +647,19 @@ __global__ void kb_jac_finish(const ImpDev* __restrict__ I) {
 #pragma unroll
         for (int k = 0; k < 16; ++k) r[k] = 0.0;
     }
+    if (d.fp32) {
 #pragma unroll
-    for (int k = 0; k < 16; ++k) d.Dinv[16 * i + k] = r[k];
-    for (long h = d.hs_off[i]; h < d.hs_off[i + 1]; ++h)
+        for (int k = 0; k < 16; ++k) d.Dinvf[16 * i + k] = (float)r[k];
+        for (long h = d.hs_off[i]; h < d.hs_off[i + 1]; ++h)
 #pragma unroll
-        for (int k = 0; k < 16; ++k) d.O[16 * h + k] = d.O[16 * h + k] * -dt;
+            for (int k = 0; k < 16; ++k) d.Of[16 * h + k] = (float)((double)d.Of[16 * h + k] * -dt);
+    } else {
+#pragma unroll
+        for (int k = 0; k < 16; ++k) d.Dinv[16 * i + k] = r[k];
+        for (long h = d.hs_off[i]; h < d.hs_off[i + 1]; ++h)
+#pragma unroll
+            for (int k = 0; k < 16; ++k) d.O[16 * h + k] = d.O[16 * h + k] * -dt;
+    }
 }
 
 // a singular diagonal block ends the member's step
@@ -634,36 +679,38 @@ __global__ void kb_jac_check(const ImpDev* __restrict__ I) {
 // are exchanged by shuffles for the product with Dinv_i.  All loads of a
 // cell depend only on its indices (prefetched one level ahead) and on
 // results of earlier levels, so they are issued together.
-template <bool FWD>
+template <typename T> struct Vec4;
+template <> struct Vec4<double> { using t = double4; };
+template <> struct Vec4<float> { using t = float4; };
+
+template <bool FWD, typename T>
 __device__ __forceinline__ void sweep_row(int i, int4 nb, int4 hh, int a, unsigned mask, int lane0,
-                                          const double* __restrict__ B, const double* src, double* dst,
-                                          const double* dxs, const double* __restrict__ Dinv,
-                                          const double* __restrict__ O) {
+                                          const T* __restrict__ B, const T* src, T* dst, const T* dxs,
+                                          const T* __restrict__ Dinv, const T* __restrict__ O) {
+    using V4 = typename Vec4<T>::t;
     const int nbv[4] = {nb.x, nb.y, nb.z, nb.w};
     const int hv[4] = {hh.x, hh.y, hh.z, hh.w};
     // component a of each neighbour state and row a of each block
-    double xa[4];
-    double4 orow[4];
+    T xa[4];
+    V4 orow[4];
 #pragma unroll
     for (int q = 0; q < 4; ++q)
         if (nbv[q] >= 0) {
             xa[q] = src[4 * (long)nbv[q] + a];
-            orow[q] = reinterpret_cast<const double4*>(O + 16 * (long)hv[q])[a];
+            orow[q] = reinterpret_cast<const V4*>(O + 16 * (long)hv[q])[a];
         }
-    const double4 drow = reinterpret_cast<const double4*>(Dinv + 16 * (long)i)[a];
-    const double own_a = FWD ? B[4 * (long)i + a] : dxs[4 * (long)i + a];
-    double t1a = 0.0;
+    const V4 drow = reinterpret_cast<const V4*>(Dinv + 16 * (long)i)[a];
+    const T own_a = FWD ? B[4 * (long)i + a] : dxs[4 * (long)i + a];
+    T t1a = T(0.0);
 #pragma unroll
     for (int q = 0; q < 4; ++q)
         if (nbv[q] >= 0) {
-            double o[4];
-            ld(orow[q], o);
+            const T o[4] = {orow[q].x, orow[q].y, orow[q].z, orow[q].w};
 #pragma unroll
             for (int b = 0; b < 4; ++b) t1a += o[b] * __shfl_sync(mask, xa[q], lane0 + b);
         }
-    double di[4];
-    ld(drow, di);
-    double t2 = 0.0;
+    const T di[4] = {drow.x, drow.y, drow.z, drow.w};
+    T t2 = T(0.0);
     if (FWD) {
 #pragma unroll
         for (int c = 0; c < 4; ++c)
@@ -676,12 +723,11 @@ __device__ __forceinline__ void sweep_row(int i, int4 nb, int4 hh, int a, unsign
     }
 }
 
-template <bool FWD>
+template <bool FWD, typename T>
 __device__ __forceinline__ void sweep(int nl, const int* __restrict__ off, const int* __restrict__ cell,
                                       const int4* __restrict__ nbs, const int4* __restrict__ hs,
-                                      const double* __restrict__ B, const double* src, double* dst,
-                                      const double* dxs, const double* __restrict__ Dinv,
-                                      const double* __restrict__ O) {
+                                      const T* __restrict__ B, const T* src, T* dst, const T* dxs,
+                                      const T* __restrict__ Dinv, const T* __restrict__ O) {
     // the cell count per pass is a multiple of 8, so the four threads of a
     // cell always sit in one aligned quarter of a warp
     const int g = threadIdx.x >> 2, a = threadIdx.x & 3, ng = blockDim.x >> 2;
@@ -712,7 +758,7 @@ __device__ __forceinline__ void sweep(int nl, const int* __restrict__ off, const
         if (have) {
             int q = p;
             while (true) {
-                sweep_row<FWD>(ci, nb, hh, a, mask, lane0, B, src, dst, dxs, Dinv, O);
+                sweep_row<FWD, T>(ci, nb, hh, a, mask, lane0, B, src, dst, dxs, Dinv, O);
                 q += ng;
                 if (q >= end) break;
                 ci = cell[q];
@@ -731,18 +777,32 @@ __device__ __forceinline__ void sweep(int nl, const int* __restrict__ off, const
 }
 
 // One CTA per member: the forward sweep, then the backward sweep
-// (src/linearSolver.c:261-333): Z_m = LU-SGS(V_m); THREADS / 4 cells of a
-// level per pass.  512 threads: 1024 would take wide levels in one pass,
-// but the register cap they impose spills and is slower (measured).
-template <int THREADS>
+// (src/linearSolver.c:261-333): Z_m = LU-SGS(V_m), in the member's precision
+// (members of the other precision are left to the other instantiation);
+// THREADS / 4 cells of a level per pass.  512 threads: 1024 would take wide
+// levels in one pass, but the register cap they impose spills and is slower
+// (measured).
+template <int THREADS, typename T>
 __global__ void __launch_bounds__(THREADS) kb_lusgs(const ImpDev* __restrict__ I, int m) {
     const ImpDev& d = I[blockIdx.x];
-    if (!d.precond || !gmres_on(d)) return;
-    const double* B = reinterpret_cast<const double*>(d.V + (long)m * d.N);
-    double* dxs = reinterpret_cast<double*>(d.dxs);
-    double* dx = reinterpret_cast<double*>(d.Z + (long)m * d.N);
-    sweep<true>(d.n_lev_f, d.lev_f_off, d.fw_cell, d.fw_nb, d.fw_h, B, dxs, dxs, dxs, d.Dinv, d.O);
-    sweep<false>(d.n_lev_b, d.lev_b_off, d.bw_cell, d.bw_nb, d.bw_h, B, dx, dx, dxs, d.Dinv, d.O);
+    if (!d.precond || !gmres_on(d) || d.fp32 != (sizeof(T) == 4)) return;
+    const T *B, *Dinv, *O;
+    T *dxs, *dx;
+    if constexpr (sizeof(T) == 8) {
+        B = reinterpret_cast<const T*>(d.V + (long)m * d.N);
+        dxs = reinterpret_cast<T*>(d.dxs);
+        dx = reinterpret_cast<T*>(d.Z + (long)m * d.N);
+        Dinv = reinterpret_cast<const T*>(d.Dinv);
+        O = reinterpret_cast<const T*>(d.O);
+    } else {
+        B = reinterpret_cast<const T*>(d.Vf + (long)m * d.N);
+        dxs = reinterpret_cast<T*>(d.dxsf);
+        dx = reinterpret_cast<T*>(d.Zf + (long)m * d.N);
+        Dinv = reinterpret_cast<const T*>(d.Dinvf);
+        O = reinterpret_cast<const T*>(d.Of);
+    }
+    sweep<true, T>(d.n_lev_f, d.lev_f_off, d.fw_cell, d.fw_nb, d.fw_h, B, dxs, dxs, dxs, Dinv, O);
+    sweep<false, T>(d.n_lev_b, d.lev_b_off, d.bw_cell, d.bw_nb, d.bw_h, B, dx, dx, dxs, Dinv, O);
 }
 
 // number of members whose Newton loop (what = 0) / GMRES cycle (what = 1)
@@ -820,18 +880,30 @@ int ccfd_implicit_setup(ccfd_ctx* ctx, const std::vector<int>& hs_off, const std
     S->nb = (int)((N + kB - 1) / kB);
     const long H = hs_off[N];
     int st;
+    S->fp32 = ctx->params.precision == CCFD_MIXED;
+    if (S->fp32) {
+        if ((st = ialloc(ctx, &S->Vf, (size_t)(K + 1) * N)) || (st = ialloc(ctx, &S->Zf, (size_t)K * N)))
+            return st;
+    } else if ((st = ialloc(ctx, &S->V, (size_t)(K + 1) * N)) || (st = ialloc(ctx, &S->Z, (size_t)K * N))) {
+        return st;
+    }
     if ((st = ialloc(ctx, &S->XK, N)) || (st = ialloc(ctx, &S->Q, N)) || (st = ialloc(ctx, &S->RXK, N)) ||
         (st = ialloc(ctx, &S->F, N)) || (st = ialloc(ctx, &S->dX, N)) || (st = ialloc(ctx, &S->W, N)) ||
-        (st = ialloc(ctx, &S->V, (size_t)(K + 1) * N)) || (st = ialloc(ctx, &S->Z, (size_t)K * N)) ||
         (st = ialloc(ctx, &S->ptmp, N)) || (st = ialloc(ctx, &S->ut, N)) ||
         (st = ialloc(ctx, &S->sc, SC_H + (K + 1) * (K + 1) + 4 * (K + 1) + 8)) ||
         (st = ialloc(ctx, &S->flag, 8)) || (st = ialloc(ctx, &S->ctl, CTL_WORDS)) ||
         (st = ialloc(ctx, &S->partial, S->nb + 1)))
         return st;
     if (ctx->params.precond) {
-        if ((st = ialloc(ctx, &S->D, 16 * (size_t)N)) || (st = ialloc(ctx, &S->Dinv, 16 * (size_t)N)) ||
-            (st = ialloc(ctx, &S->O, 16 * (size_t)H)) || (st = ialloc(ctx, &S->dxs, N)))
+        if ((st = ialloc(ctx, &S->D, 16 * (size_t)N))) return st;
+        if (S->fp32) {
+            if ((st = ialloc(ctx, &S->Dinvf, 16 * (size_t)N)) || (st = ialloc(ctx, &S->Of, 16 * (size_t)H)) ||
+                (st = ialloc(ctx, &S->dxsf, N)))
+                return st;
+        } else if ((st = ialloc(ctx, &S->Dinv, 16 * (size_t)N)) || (st = ialloc(ctx, &S->O, 16 * (size_t)H)) ||
+                   (st = ialloc(ctx, &S->dxs, N))) {
             return st;
+        }
         // twins
         std::vector<int> twin(H, -1);
         for (long d = 0; d < N; ++d)
@@ -1000,6 +1072,7 @@ struct ImpSet {
     int n = 0, max_nb = 0, max_col = 0, max_colsize = 0, max_K = 0, max_newton = 0;
     int max_level = 0;  // widest LU-SGS level (cells) over the members
     bool any_precond = false;
+    bool pc64 = false, pc32 = false;  // preconditioned members in FP64 / FP32
     int* d_count = nullptr;
     int* h_count = nullptr;
     cudaStream_t stream = nullptr;
@@ -1047,6 +1120,8 @@ static ImpDev make_dev(ccfd_ctx* ctx) {
     d.prim = ctx->prim_buf[ctx->cur];
     d.pert = ctx->prim_buf[ctx->cur ^ 1];
     d.D = S->D; d.Dinv = S->Dinv; d.O = S->O; d.sc = S->sc; d.partial = S->partial;
+    d.fp32 = S->fp32;
+    d.Vf = S->Vf; d.Zf = S->Zf; d.dxsf = S->dxsf; d.Dinvf = S->Dinvf; d.Of = S->Of;
     d.flag = S->flag;
     d.ctl = S->ctl;
     d.ctrl = ctx->ctrl;
@@ -1079,6 +1154,8 @@ static int set_build(const std::vector<ccfd_ctx*>& members, cudaStream_t stream,
         M->max_newton = std::max(M->max_newton, ctx->params.n_newton_iter);
         if (ctx->params.precond) {
             M->any_precond = true;
+            if (S->fp32) M->pc32 = true;
+            else M->pc64 = true;
             int ncol = (int)S->color_off.size() - 1;
             M->max_col = std::max(M->max_col, ncol);
             for (int c = 0; c < ncol; ++c)
@@ -1212,7 +1289,8 @@ static int set_step(ImpSet* M) {
             kb_jac_check<<<g1, 32, 0, st>>>(M->dev);
         }
         for (int m = 0; m < M->max_K; ++m) {
-            if (M->any_precond) kb_lusgs<kSweepThreads><<<M->n, kSweepThreads, 0, st>>>(M->dev, m);
+            if (M->pc64) kb_lusgs<kSweepThreads, double><<<M->n, kSweepThreads, 0, st>>>(M->dev, m);
+            if (M->pc32) kb_lusgs<kSweepThreads, float><<<M->n, kSweepThreads, 0, st>>>(M->dev, m);
             kb_copy_vz<<<gv, kB, 0, st>>>(M->dev, m);
             // matrixVector: epsFD = sqrt(eps) / |Z|
             kb_dot_zz<<<gv, kB, 0, st>>>(M->dev, m);

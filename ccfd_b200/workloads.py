@@ -40,11 +40,14 @@ def airfoil_ini(spec: dict, mesh_name: str, cfl: float, precision: int = 0) -> s
                                                                           "epsNewton = 0.1")
 
 
-def airfoil_case(spec: dict, tmpdir: str, name: str, cfl: float = 1.0, h0: float = 2e-3):
+def airfoil_case(spec: dict, tmpdir: str, name: str, cfl: float = 1.0, h0: float = 2e-3,
+                 precision: int = 0):
     import ccfd_b200 as cc
-    meshgen.naca_ogrid(spec["m"], spec["p"], spec["t"], spec["ni"], spec["nj"], h0=h0,
-                       wall_code=101).write_gmsh(os.path.join(tmpdir, name + ".msh"))
-    return cc.CaseData.from_text(airfoil_ini(spec, name, cfl), tmpdir)
+    path = os.path.join(tmpdir, name + ".msh")
+    if not os.path.exists(path):
+        meshgen.naca_ogrid(spec["m"], spec["p"], spec["t"], spec["ni"], spec["nj"], h0=h0,
+                           wall_code=101).write_gmsh(path)
+    return cc.CaseData.from_text(airfoil_ini(spec, name, cfl, precision), tmpdir)
 
 
 def stream_specs(n: int, seed: int = 20260005, riemann_n=(256, 2048), cylinder_cells=(50_000, 400_000),

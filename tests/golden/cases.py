@@ -143,6 +143,11 @@ def implicit_cases() -> dict:
                                 "eqn": "euler", "steps": 4},
         "naca_ns_imp_pc": {"mesh": ("naca", 32, 12), "ini": ini(ns=True, cfl=10.0), "eqn": "navierstokes",
                            "steps": 3},
+        # a long run towards the steady state (relative residual 1.7e-2 after
+        # 200 steps; the reference's fixed-CFL backward Euler converges
+        # slowly, so 1e-8 is out of reach of the dense reference Jacobian)
+        "naca_euler_imp_pc_long": {"mesh": ("naca", 32, 12, 101), "ini": ini(steps=200), "eqn": "euler",
+                                   "steps": 200},
     }
 
 

@@ -112,7 +112,7 @@ def test_batch_join_and_leave_mid_run():
 
 def test_implicit_members_in_lockstep_equal_alone():
     # uneven implicit members (sizes, Krylov dimensions, preconditioner on /
-    # off, Euler / Navier-Stokes) advance in lockstep Newton / GMRES /
+    # off, Euler / Navier-Stokes, FP64 / mixed) advance in lockstep Newton / GMRES /
     # LU-SGS launches; each must match its own run alone exactly
     imp = CASES.implicit_cases()
     specs = {
@@ -121,6 +121,9 @@ def test_implicit_members_in_lockstep_equal_alone():
         "ns_pc": (dict(imp["naca_ns_imp_pc"]), 3),
         "pc_small": ({"mesh": ("naca", 24, 8, 101), "ini": imp["naca_euler_imp_pc"]["ini"],
                       "eqn": "euler"}, 5),
+        "pc_mixed": ({"mesh": ("naca", 32, 12, 101),
+                      "ini": imp["naca_euler_imp_pc"]["ini"].replace("precision = 0", "precision = 1"),
+                      "eqn": "euler"}, 4),
     }
     alone = {}
     for k, (spec, steps) in specs.items():

@@ -49,8 +49,15 @@ def test_writer_refuses_formats_it_does_not_build(sod_check):
     ini = re.sub(r"(?im)^(\s*outputformat\s*=\s*)3", r"\g<1>1", g["ini"])
     case = cc.CaseData.from_text(ini)
     assert case.c.output_format == 1
-    with pytest.raises(cc.CcfdError):
-        case.write_output(case.prim0(), 0.0, 0)
+    cwd = os.getcwd()
+    with tempfile.TemporaryDirectory() as tmp:
+        os.chdir(tmp)
+        try:
+            with pytest.raises(cc.CcfdError):
+                case.write_output(case.prim0(), 0.0, 0)
+            assert os.listdir(tmp) == []
+        finally:
+            os.chdir(cwd)
 
 
 @pytest.mark.gpu
