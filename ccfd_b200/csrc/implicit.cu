@@ -36,6 +36,7 @@
 #include <cuda_runtime.h>
 #include <float.h>
 #include <math.h>
+#include <stdlib.h>
 #include <string.h>
 
 #include <algorithm>
@@ -1492,8 +1493,11 @@ int ccfd_implicit_batch_steps(ccfd_batch* b, const std::vector<ccfd_ctx*>& membe
     if (bi.key != members) {
         batch_imp_free(bi);
         bi.key = members;
-        // sets balanced by cell count (largest first onto the lightest set)
-        const int nsets = std::max(1, std::min(4, (int)members.size() / 4));
+        // sets balanced by cell count (largest first onto the lightest set);
+        // at most CCFD_IMPLICIT_SETS (default 4) sets of at least 4 members
+        int max_sets = 4;
+        if (const char* e = getenv("CCFD_IMPLICIT_SETS")) max_sets = std::max(1, std::min(64, atoi(e)));
+        const int nsets = std::max(1, std::min(max_sets, (int)members.size() / 4));
         std::vector<int> idx(members.size());
         for (size_t k = 0; k < idx.size(); ++k) idx[k] = (int)k;
         std::stable_sort(idx.begin(), idx.end(), [&](int a, int c) { return members[a]->N > members[c]->N; });

@@ -89,9 +89,10 @@ def _main(argv=None) -> int:
     airfoil (m 0.02, p 0.4, t 0.12, Mach 0.5, 1 degree) through the implicit
     solver on device 0; prints cells, steps, Newton / GMRES iterations and
     device milliseconds.
-    python -m ccfd_b200.workloads batch N STEPS [CFL]: the first N airfoils
-    of the batched distribution stepped together in one batch; prints the
-    total cells, Newton / GMRES iterations and batch device milliseconds."""
+    python -m ccfd_b200.workloads batch N STEPS [CFL] [PRECISION]: the first
+    N airfoils of the batched distribution stepped together in one batch
+    (PRECISION 0: FP64, 1: mixed); prints the total cells, Newton / GMRES
+    iterations and batch device milliseconds."""
     import sys
     import tempfile
 
@@ -100,9 +101,11 @@ def _main(argv=None) -> int:
     if len(args) >= 3 and args[0] == "batch":
         n, steps = int(args[1]), int(args[2])
         cfl = float(args[3]) if len(args) > 3 else 1.0
+        prec = int(args[4]) if len(args) > 4 else 0
         cc.set_device(0)
         with tempfile.TemporaryDirectory() as tmp:
-            cases = [airfoil_case(sp, tmp, f"af{k}", cfl=cfl) for k, sp in enumerate(airfoil_specs(n))]
+            cases = [airfoil_case(sp, tmp, f"af{k}", cfl=cfl, precision=prec)
+                     for k, sp in enumerate(airfoil_specs(n))]
         b = cc.Batch(0)
         members = [cc.Solver(c) for c in cases]
         for s in members:
