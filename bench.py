@@ -113,7 +113,7 @@ def algorithmic_bytes_per_stage(m: dict, venk: bool) -> int:
 # DRAM bytes per launch of the stage kernel on this workload, from the ncu
 # capture summarised in profiles/k_stage_dmr500k_hllc_vk_fp64.md
 # (dram__bytes_read.sum + dram__bytes_write.sum)
-STAGE_TRAFFIC_BYTES = 151.7e6 + 13.0e6
+STAGE_TRAFFIC_BYTES = 151.42e6 + 12.26e6
 
 
 def make_case(tmpdir: str, precision: int = 0):

@@ -6,6 +6,7 @@
 #include <string.h>
 
 #include <algorithm>
+#include <string>
 #include <vector>
 
 #include "ccfd_b200.h"
@@ -113,8 +114,11 @@ extern "C" int ccfd_create(const ccfd_params* params, ccfd_ctx** out) {
         delete ctx;
         return CCFD_ERR_CUDA;
     }
-    if (cudaMallocHost((void**)&ctx->h_ctrl, sizeof(Ctrl)) != cudaSuccess ||
-        cudaEventCreate(&ctx->ev_run0) != cudaSuccess || cudaEventCreate(&ctx->ev_run1) != cudaSuccess) {
+    // host copy of the control block in ordinary memory: releasing pinned
+    // memory would wait for all work on the device (other contexts included)
+    ctx->h_ctrl = new Ctrl();
+    if (cudaEventCreate(&ctx->ev_run0) != cudaSuccess || cudaEventCreate(&ctx->ev_run1) != cudaSuccess) {
+        delete ctx->h_ctrl;
         cudaStreamDestroy(ctx->stream);
         delete ctx;
         return CCFD_ERR_CUDA;
@@ -149,7 +153,7 @@ extern "C" void ccfd_destroy(ccfd_ctx* ctx) {
     free_device(ctx);
     if (ctx->ev_run0) cudaEventDestroy(ctx->ev_run0);
     if (ctx->ev_run1) cudaEventDestroy(ctx->ev_run1);
-    if (ctx->h_ctrl) cudaFreeHost(ctx->h_ctrl);
+    delete ctx->h_ctrl;
     cudaStreamDestroy(ctx->stream);
     delete ctx;
 }
@@ -158,7 +162,7 @@ extern "C" void ccfd_destroy(ccfd_ctx* ctx) {
 // list then the suction-side list, each built by the insertion of initWing
 // (src/analyze.c:95-184), keyed on the face midpoint x
 static void build_wall_list(const ccfd_mesh* m, const ccfd_bc* bc, int wall_code,
-                            std::vector<int>& order) {
+                            std::vector<int>& order, int* n_pressure) {
     std::vector<int> pressure, suction;
     for (long g = 0; g < m->n_bc; ++g) {
         const ccfd_bc& b = bc[m->bc_index[g]];
@@ -177,6 +181,7 @@ static void build_wall_list(const ccfd_mesh* m, const ccfd_bc* bc, int wall_code
     }
     order = pressure;
     order.insert(order.end(), suction.begin(), suction.end());
+    *n_pressure = (int)pressure.size();
 }
 
 extern "C" int ccfd_upload_case(ccfd_ctx* ctx, const ccfd_mesh* m, const ccfd_bc* bc, int n_bc,
@@ -272,32 +277,6 @@ extern "C" int ccfd_upload_case(ccfd_ctx* ctx, const ccfd_mesh* m, const ccfd_bc
         counts[t] = make_int4(ts.counts[4 * t], ts.counts[4 * t + 1], ts.counts[4 * t + 2], ts.counts[4 * t + 3]);
         gl_off[t + 1] = gl_off[t] + ts.counts[4 * t + 1] + 1;
     }
-    // packed per-tile records of the gradient cells and faces
-    std::vector<int4> g_rec(gl_off[ts.n_tiles]);
-    for (int t = 0; t < ts.n_tiles; ++t) {
-        const int nG = ts.counts[4 * t + 1], e0 = ts.e_off[t], gb = gl_off[t];
-        for (int i = 0; i < nG; ++i) {
-            int d = ts.e_ref[e0 + i];
-            g_rec[gb + i] = make_int4(d, hs_off[d], hs_off[d + 1] - hs_off[d], ts.hs_loc[gb + i]);
-        }
-    }
-    const bool ns = p.eqn == CCFD_NAVIER_STOKES;
-    const size_t nTF = ts.f_id.size();
-    std::vector<int4> f_rec(nTF);
-    std::vector<double4> f_nl(nTF), f_bb(ns ? nTF : 1);
-    for (size_t j = 0; j < nTF; ++j) {
-        int fid = ts.f_id[j];
-        f_rec[j] = make_int4(fid, ts.f_lr[j], ts.f_hs[j], 0);
-        if (fid >= 0) {
-            f_nl[j] = face_nl[fid];
-            if (ns) f_bb[j] = face_bb[fid];
-        } else {
-            int g = -1 - fid;
-            f_nl[j] = make_double4(g_gn[g].z, g_gn[g].w, g_ml[g].z, 0.0);
-            if (ns) f_bb[j] = g_bb[g];
-        }
-    }
-
     int st;
     DevMesh& dm = ctx->mesh;
     memset(&dm, 0, sizeof(dm));
@@ -318,9 +297,7 @@ extern "C" int ccfd_upload_case(ccfd_ctx* ctx, const ccfd_mesh* m, const ccfd_bc
         (st = dupload_c(ctx, &td.gl_off, gl_off)) || (st = dupload_c(ctx, &td.hs_loc, hs_loc)) ||
         (st = dupload_c(ctx, &td.f_off, ts.f_off)) || (st = dupload_c(ctx, &td.f_id, ts.f_id)) ||
         (st = dupload_c(ctx, &td.f_lr, ts.f_lr)) || (st = dupload_c(ctx, &td.f_hs, ts.f_hs)) ||
-        (st = dupload_c(ctx, &td.u_code, ts.u_code)) || (st = dupload_c(ctx, &td.g_rec, g_rec)) ||
-        (st = dupload_c(ctx, &td.f_rec, f_rec)) || (st = dupload_c(ctx, &td.f_nl, f_nl)) ||
-        (st = dupload_c(ctx, &td.f_bb, f_bb))) {
+        (st = dupload_c(ctx, &td.u_code, ts.u_code))) {
         free_device(ctx);
         return st;
     }
@@ -377,9 +354,13 @@ extern "C" int ccfd_upload_case(ccfd_ctx* ctx, const ccfd_mesh* m, const ccfd_bc
     // wing surface list for CL / CD
     std::vector<int> wl;
     std::vector<double> wnl;
-    if (p.calc_wing) build_wall_list(m, bc, p.wall_id, wl);
+    ctx->n_wall_pressure = 0;
+    ctx->wall_xy.clear();
+    if (p.calc_wing) build_wall_list(m, bc, p.wall_id, wl, &ctx->n_wall_pressure);
     for (int g : wl) {
         long f = m->bc_face[g];
+        ctx->wall_xy.push_back(m->bc_x[2 * g]);
+        ctx->wall_xy.push_back(m->bc_x[2 * g + 1]);
         wnl.push_back(m->face_n[2 * f]);
         wnl.push_back(m->face_n[2 * f + 1]);
         wnl.push_back(m->face_len[f]);
@@ -882,6 +863,60 @@ extern "C" int ccfd_run_explicit(ccfd_ctx* ctx, long nsteps, ccfd_report* report
         report->device_ms = run_ms;
     }
     return ccfd_status_from_flags(c.flags | f);
+}
+
+// Pressure coefficient along the wing (the CP part of calcCoef,
+// src/analyze.c:296-367): for each wall face in calcCoef's order (pressure
+// side by increasing x, then suction side) its point x, y and
+// cp = (p_face - p_inf) / (rho_inf v_inf^2 / 2) of the last residual
+// evaluation.  Arrays of at least *n entries; with x == NULL only the counts
+// are returned.
+extern "C" int ccfd_wall_cp(ccfd_ctx* ctx, double* x, double* y, double* cp, int* n, int* n_pressure) {
+    if (!ctx || !ctx->uploaded || !n) return CCFD_ERR_ARG;
+    if (!ctx->params.calc_wing || ctx->n_wall == 0) return CCFD_ERR_ARG;
+    *n = ctx->n_wall;
+    if (n_pressure) *n_pressure = ctx->n_wall_pressure;
+    if (!x) return CCFD_OK;
+    if (!y || !cp) return CCFD_ERR_ARG;
+    CK(cudaSetDevice(ctx->device));
+    std::vector<double> pf(ctx->B + 1);
+    std::vector<int> wl(ctx->n_wall);
+    CK(cudaMemcpyAsync(pf.data(), ctx->ghost_pface, sizeof(double) * pf.size(), cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaMemcpyAsync(wl.data(), ctx->wall_ghost, sizeof(int) * wl.size(), cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    const double pi = acos(-1.0);
+    const double* ref = ctx->exact.ref_state[0];
+    const double v = ref[1] / cos(ctx->exact.alpha * pi / 180.0);
+    const double q_inf_q = 1.0 / (ref[0] * 0.5 * v * v);
+    const double p_inf = ref[3];
+    for (int k = 0; k < ctx->n_wall; ++k) {
+        x[k] = ctx->wall_xy[2 * k];
+        y[k] = ctx->wall_xy[2 * k + 1];
+        cp[k] = (pf[wl[k]] - p_inf) * q_inf_q;
+    }
+    return CCFD_OK;
+}
+
+// The reference's CP files: <base>_CP_pressureSide.csv and
+// <base>_CP_suctionSide.csv with rows x, y, phi = atan2(y, x), cp
+extern "C" int ccfd_write_cp(ccfd_ctx* ctx, const char* base) {
+    if (!base) return CCFD_ERR_ARG;
+    int n = 0, np = 0;
+    int st = ccfd_wall_cp(ctx, nullptr, nullptr, nullptr, &n, &np);
+    if (st) return st;
+    std::vector<double> x(n), y(n), cp(n);
+    if ((st = ccfd_wall_cp(ctx, x.data(), y.data(), cp.data(), &n, &np))) return st;
+    for (int side = 0; side < 2; ++side) {
+        const char* tag = side ? "suctionSide" : "pressureSide";
+        std::string name = std::string(base) + "_CP_" + tag + ".csv";
+        FILE* f = fopen(name.c_str(), "w");
+        if (!f) return CCFD_ERR_ARG;
+        fprintf(f, "x, y, phi, CP_%s\n", tag);
+        for (int k = side ? np : 0; k < (side ? n : np); ++k)
+            fprintf(f, "%15.7f,%15.7f,%15.7f,%15.7f\n", x[k], y[k], atan2(y[k], x[k]), cp[k]);
+        fclose(f);
+    }
+    return CCFD_OK;
 }
 
 extern "C" int ccfd_clcd(ccfd_ctx* ctx, double* cl, double* cd) {

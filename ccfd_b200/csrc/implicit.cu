@@ -1076,6 +1076,7 @@ struct ImpSet {
     bool pc64 = false, pc32 = false;  // preconditioned members in FP64 / FP32
     int* d_count = nullptr;
     int* h_count = nullptr;
+    int h_count_v = 0;  // ordinary memory: freeing pinned memory would wait for the device
     cudaStream_t stream = nullptr;
     int last_cuda_error = 0;
 };
@@ -1090,7 +1091,6 @@ static void set_free(ImpSet* M) {
     }
     if (M->dev) cudaFreeAsync(M->dev, M->stream);
     if (M->d_count) cudaFreeAsync(M->d_count, M->stream);
-    if (M->h_count) cudaFreeHost(M->h_count);
     delete M;
 }
 
@@ -1170,7 +1170,7 @@ static int set_build(const std::vector<ccfd_ctx*>& members, cudaStream_t stream,
     CKM(cudaMallocAsync(&M->dev, sizeof(ImpDev) * M->n, stream));
     CKM(cudaMemcpyAsync(M->dev, hd.data(), sizeof(ImpDev) * M->n, cudaMemcpyHostToDevice, stream));
     CKM(cudaMallocAsync(&M->d_count, sizeof(int), stream));
-    CKM(cudaMallocHost(&M->h_count, sizeof(int)));
+    M->h_count = &M->h_count_v;
     for (auto& kv : by_variant) {
         ImpGroup g;
         std::tie(g.flux, g.order, g.ns, g.fp32) = kv.first;

@@ -22,12 +22,6 @@ struct TileDev {
     const int* f_lr;      // packed local cell indices
     const int* f_hs;      // packed local half-side indices
     const int* u_code;    // [H] per device half-side: 2 * local face + neighbour flag, or -1-g
-    // packed records (one load each, independent of one another):
-    const int4* g_rec;    // per gradient cell (gl_off indexing): (device cell, first half-side,
-                          //   half-side count, local half-side start)
-    const int4* f_rec;    // per tile face: (f_id, f_lr, f_hs, 0)
-    const double4* f_nl;  // per tile face: (n.x, n.y, len, 0)
-    const double4* f_bb;  // per tile face: (baryBaryVec.x, .y, baryBaryDist, 0); Navier-Stokes only
 };
 
 // Per-ghost data of the boundary kernel (device order of ghosts = BCside order).

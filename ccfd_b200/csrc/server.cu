@@ -8,9 +8,9 @@
 // requests.  Each call of ccfd_server_poll moves the uploaded requests into
 // the running batch at the step boundary, so they overlap on the device with
 // the requests already running, advances the batch, and retires the
-// requests that stopped (end time, convergence, step budget, error): their
-// final state is copied to the host and their device memory is released for
-// the next admissions.  No counterpart in the reference, which runs one case
+// requests that stopped (end time, convergence, step budget, error): the
+// workers copy their final state to the host and release their device
+// memory for the next admissions, again while the GPU keeps stepping.  No counterpart in the reference, which runs one case
 // per process.
 #include <cuda_runtime.h>
 #include <string.h>
@@ -33,7 +33,7 @@ double now_s() {
     return duration<double>(steady_clock::now().time_since_epoch()).count();
 }
 
-enum ReqState { QUEUED = 0, UPLOADING, READY, RUNNING, DONE };
+enum ReqState { QUEUED = 0, UPLOADING, READY, RUNNING, RETIRING, DONE };
 
 struct Request {
     long id = 0;
@@ -59,6 +59,7 @@ struct ccfd_server {
     std::deque<long> queue;
     std::map<long, Request> reqs;
     std::vector<long> ready;      // uploaded, waiting for the next step boundary
+    std::deque<long> retiring;    // left the batch, state to copy back and memory to release
     long next_id = 1;
     double t_admit = 0, t_step = 0, t_retire = 0;  // host seconds per phase
     std::mutex mu;
@@ -109,11 +110,34 @@ static void worker_main(ccfd_server* s) {
     std::unique_lock<std::mutex> lk(s->mu);
     for (;;) {
         s->cv.wait(lk, [s] {
-            if (s->stop) return true;
+            if (s->stop || !s->retiring.empty()) return true;
             if (s->queue.empty() || s->slots >= s->max_running) return false;
             return s->used + s->reqs[s->queue.front()].est <= s->budget;
         });
         if (s->stop) return;
+        if (!s->retiring.empty()) {
+            // retire first: it frees memory for the next admissions
+            long rid = s->retiring.front();
+            s->retiring.pop_front();
+            Request& q = s->reqs[rid];
+            lk.unlock();
+            double t0 = now_s();
+            q.prim.resize(4 * (size_t)q.c->mesh.n_cells);
+            int gs = ccfd_get_state(q.ctx, q.prim.data(), CCFD_PRIMITIVE);
+            if (gs) q.prim.clear();
+            ccfd_destroy(q.ctx);
+            double t1 = now_s();
+            lk.lock();
+            s->t_retire += t1 - t0;
+            if (!q.status) q.status = gs;
+            q.ctx = nullptr;
+            s->used -= q.bytes;
+            s->slots--;
+            q.state = DONE;
+            q.t_done = now_s();
+            s->cv.notify_all();
+            continue;
+        }
         long id = s->queue.front();
         s->queue.pop_front();
         Request& r = s->reqs[id];  // std::map references stay valid
@@ -204,19 +228,13 @@ extern "C" int ccfd_server_submit(ccfd_server* s, const ccfd_case* c, long nstep
     return CCFD_OK;
 }
 
-// retire a request that left the batch (server lock held)
+// hand a request that left the batch to the workers, which copy its state
+// back and release its context while the GPU keeps stepping (lock held)
 static void retire(ccfd_server* s, Request& r, int status) {
     r.status = status;
-    r.prim.resize(4 * (size_t)r.c->mesh.n_cells);
-    int gs = ccfd_get_state(r.ctx, r.prim.data(), CCFD_PRIMITIVE);
-    if (gs) r.prim.clear();
-    if (!r.status) r.status = gs;
-    ccfd_destroy(r.ctx);
-    r.ctx = nullptr;
-    s->used -= r.bytes;
-    s->slots--;
-    r.state = DONE;
-    r.t_done = now_s();
+    r.state = RETIRING;
+    s->retiring.push_back(r.id);
+    s->cv.notify_all();
 }
 
 // Move uploaded requests into the batch, advance the running requests by up
@@ -274,7 +292,6 @@ extern "C" int ccfd_server_poll(ccfd_server* s, int steps, int* n_queued, int* n
             retire(s, *r, r->rep.status);
         }
         std::lock_guard<std::mutex> lk(s->mu);
-        s->t_retire += now_s() - t2;
         s->cv.notify_all();
     }
     std::lock_guard<std::mutex> lk(s->mu);
@@ -282,7 +299,7 @@ extern "C" int ccfd_server_poll(ccfd_server* s, int steps, int* n_queued, int* n
     for (auto& kv : s->reqs) {
         int stt = kv.second.state;
         q += stt == QUEUED || stt == UPLOADING || stt == READY;
-        run += stt == RUNNING;
+        run += stt == RUNNING || stt == RETIRING;
         d += stt == DONE;
     }
     if (n_queued) *n_queued = q;

@@ -33,7 +33,13 @@
 
 namespace ccfd {
 
-constexpr int kThreads = 256;
+// CTA shape per arithmetic type (one CTA per tile; measured): FP64 stages
+// run 384 threads, 2 CTAs per SM (gradient cells and faces of a 256-cell
+// tile in about one pass each); the FP32 kernels need half the shared
+// memory and run 256 threads, 3 CTAs per SM.
+template <typename FT> struct StageShape;
+template <> struct StageShape<double> { static constexpr int threads = 384, min_blocks = 2; };
+template <> struct StageShape<float> { static constexpr int threads = 256, min_blocks = 3; };
 
 __device__ __forceinline__ double stage_time(const Ctrl* ctrl, double tfix, double a_time) {
     return ctrl ? ctrl->t + a_time * ctrl->dt : tfix;
@@ -410,6 +416,7 @@ __device__ __forceinline__ void stage_body(const StageLaunch& L, const int t) {
     const TileDev& T = L.tiles;
     const Phys& P = L.phys;
     const int tid = threadIdx.x;
+    constexpr int kThreads = StageShape<FT>::threads;
     const int4 cnt = T.counts[t];
     const int nT = cnt.x, nG = cnt.y, nEc = cnt.z, nE = cnt.w;
     const int e0 = T.e_off[t];
@@ -438,8 +445,9 @@ __device__ __forceinline__ void stage_body(const StageLaunch& L, const int t) {
     const int hb = T.hs_off[t], gb = T.gl_off[t];
     if (ORDER == 2) {
         for (int i = tid; i < nG; i += kThreads) {
-            const int4 gr = T.g_rec[gb + i];
-            const int d = gr.x, h0 = gr.y, nh = gr.z, lo = gr.w;
+            int d = T.e_ref[e0 + i];
+            int h0 = m.hs_off[d], nh = m.hs_off[d + 1] - h0;
+            int lo = T.hs_loc[gb + i];
             FT q[4], ux[4], uy[4];
             ld4(ps[i], q);
             FT eps2 = L.limiter == 2 ? FT(m.venk_eps2[d]) : FT(0.0);
@@ -459,15 +467,14 @@ __device__ __forceinline__ void stage_body(const StageLaunch& L, const int t) {
     // C: fluxes of the tile's faces (interior faces, then boundary faces)
     const int f0 = T.f_off[t], nF = T.f_off[t + 1] - f0;
     for (int j = tid; j < nF; j += kThreads) {
-        const int4 fr = T.f_rec[f0 + j];
-        const double4 nlj = T.f_nl[f0 + j];
-        const int fid = fr.x, lr = fr.y;
+        int fid = T.f_id[f0 + j];
+        int lr = T.f_lr[f0 + j];
         int il = lr & 0xffff, ir = lr >> 16;
         FT q0[4], q1[4], Lf[4], Rf[4];
         FT g0x[4] = {0, 0, 0, 0}, g0y[4] = {0, 0, 0, 0}, g1x[4] = {0, 0, 0, 0}, g1y[4] = {0, 0, 0, 0};
         ld4(ps[il], q0);
         ld4(ps[ir], q1);
-        int hh = fr.z;
+        int hh = T.f_hs[f0 + j];
         if (ORDER == 2) {
             V2 gpl = hgp[hh & 0xffff];
             ld4(gs[2 * il], g0x);
@@ -491,16 +498,18 @@ __device__ __forceinline__ void stage_body(const StageLaunch& L, const int t) {
 #pragma unroll
                 for (int v = 0; v < 4; ++v) Rf[v] = q1[v];
             }
-            nx = FT(nlj.x); ny = FT(nlj.y); len = FT(nlj.z);
-            if (NS) bb = T.f_bb[f0 + j];
+            double4 nl = m.face_nl[fid];
+            nx = FT(nl.x); ny = FT(nl.y); len = FT(nl.z);
+            if (NS) bb = m.face_bb[fid];
         } else {
             int g = -1 - fid;
             double4 Rd = ghost_face(L.ghosts.bc, L.ghosts.gn, L.ghosts.ml, L.phys_g, g, time,
                                     to_d4(mk4(Lf)), L.flags);
             ld4(cvt4<FT>(Rd), Rf);
             if (L.ghost_pface) L.ghost_pface[g] = double(Lf[3]);
-            nx = FT(nlj.x); ny = FT(nlj.y); len = FT(nlj.z);
-            if (NS) bb = T.f_bb[f0 + j];
+            double4 gn = L.ghosts.gn[g];
+            nx = FT(gn.z); ny = FT(gn.w); len = FT(L.ghosts.ml[g].z);
+            if (NS) bb = L.ghosts.bb[g];
         }
         FT F[4];
         face_flux<FLUX, NS, FT>(P, nx, ny, len, Lf, Rf, q0, q1, g0x, g0y, g1x, g1y, bb, F, L.flags);
@@ -514,8 +523,8 @@ __device__ __forceinline__ void stage_body(const StageLaunch& L, const int t) {
     int bad = 0;
     const bool rk = L.mode == 1;
     for (int i = tid; i < nT; i += kThreads) {
-        const int4 gr = T.g_rec[gb + i];  // tile cells lead the gradient-cell list
-        const int d = gr.x, h0 = gr.y, h1 = gr.y + gr.z;
+        int d = T.e_ref[e0 + i];
+        int h0 = m.hs_off[d], h1 = m.hs_off[d + 1];
         double s[4] = {0.0, 0.0, 0.0, 0.0};
         for (int h = h0; h < h1; ++h) {
             int code = T.u_code[h];
@@ -587,13 +596,10 @@ __device__ __forceinline__ void stage_body(const StageLaunch& L, const int t) {
     }
 }
 
-#ifndef CCFD_STAGE_MIN_BLOCKS
-#define CCFD_STAGE_MIN_BLOCKS 3
-#endif
 
 // one instance: one tile per CTA, launch parameters in the parameter space
 template <int FLUX, int ORDER, int NS, typename FT>
-__global__ void __launch_bounds__(kThreads, CCFD_STAGE_MIN_BLOCKS) k_stage(StageLaunch L) {
+__global__ void __launch_bounds__(StageShape<FT>::threads, StageShape<FT>::min_blocks) k_stage(StageLaunch L) {
     if (inactive(L.ctrl)) return;
     stage_body<FLUX, ORDER, NS, FT>(L, blockIdx.x);
 }
@@ -604,7 +610,7 @@ __global__ void __launch_bounds__(kThreads, CCFD_STAGE_MIN_BLOCKS) k_stage(Stage
 // (Ls[inst][par][stage]); a residual evaluation (stride 1) takes
 // Ls[inst] and is skipped while *skip is nonzero.
 template <int FLUX, int ORDER, int NS, typename FT>
-__global__ void __launch_bounds__(kThreads, CCFD_STAGE_MIN_BLOCKS)
+__global__ void __launch_bounds__(StageShape<FT>::threads, StageShape<FT>::min_blocks)
     k_stage_batch(const StageLaunch* __restrict__ Ls, const int2* __restrict__ tmap, int rk_mode,
                   int stage) {
     const int2 tm = tmap[blockIdx.x];
