@@ -252,6 +252,19 @@ class Solver:
         _check(N.lib.ccfd_device_bytes(self._ctx, C.byref(b)), "ccfd_device_bytes")
         return b.value
 
+    def wall_cp(self):
+        """(x, y, cp, n_pressure_side) along the wing (ccfd_wall_cp)."""
+        n, npres = C.c_int(), C.c_int()
+        _check(N.lib.ccfd_wall_cp(self._ctx, None, None, None, C.byref(n), C.byref(npres)), "ccfd_wall_cp")
+        x, y, cp = np.empty(n.value), np.empty(n.value), np.empty(n.value)
+        _check(N.lib.ccfd_wall_cp(self._ctx, _dptr(x), _dptr(y), _dptr(cp), C.byref(n), C.byref(npres)),
+               "ccfd_wall_cp")
+        return x, y, cp, npres.value
+
+    def write_cp(self, base: str) -> None:
+        """The reference's CP files <base>_CP_pressureSide.csv / _CP_suctionSide.csv."""
+        _check(N.lib.ccfd_write_cp(self._ctx, os.fsencode(base)), "ccfd_write_cp")
+
     def clcd(self):
         cl, cd = C.c_double(), C.c_double()
         _check(N.lib.ccfd_clcd(self._ctx, C.byref(cl), C.byref(cd)), "ccfd_clcd")

@@ -50,6 +50,8 @@ struct ccfd_ctx {
     int* wall_ghost = nullptr;
     double* wall_nl = nullptr;
     int n_wall = 0;
+    int n_wall_pressure = 0;       // pressure-side entries lead the wall list
+    std::vector<double> wall_xy;   // wall face points (x, y) in wall-list order
     // step graphs per start buffer parity: [parity][0: one step, 1: many]
     cudaGraphExec_t graph[2][2] = {{nullptr, nullptr}, {nullptr, nullptr}};
     std::vector<cudaEvent_t> prof_ev[2][2];

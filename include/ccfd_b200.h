@@ -282,6 +282,16 @@ int ccfd_get_profile(ccfd_ctx *ctx, double *residual_ms, long *residual_count,
 /* Drop-in for globalResidual on the last residual (src/analyze.c:521-539). */
 int ccfd_global_residual(ccfd_ctx *ctx, double res[4]);
 
+/* Pressure coefficient along the wall params.wall_id (the CP part of
+ * calcCoef, src/analyze.c:296-367), from the last residual evaluation: per
+ * wall face in calcCoef's order (pressure side by increasing x, then suction
+ * side) its point x, y and cp.  *n receives the face count, *n_pressure
+ * (may be NULL) the pressure-side count; with x == NULL only the counts. */
+int ccfd_wall_cp(ccfd_ctx *ctx, double *x, double *y, double *cp, int *n, int *n_pressure);
+/* The reference's CP files <base>_CP_pressureSide.csv / _CP_suctionSide.csv
+ * (rows x, y, phi, cp). */
+int ccfd_write_cp(ccfd_ctx *ctx, const char *base);
+
 /* Autotuner (no counterpart in the reference): re-uploads the case with
  * each candidate launch shape of the stage kernel (cells per tile 128..384,
  * Hilbert or reference cell order), times residual evaluations of state prim

@@ -83,4 +83,12 @@ def run_ref(ini_text: str, mode: str, *args, eqn: str = "euler",
         if r.returncode != 0:
             raise RuntimeError(f"reference driver failed ({r.returncode}):\n"
                                f"{r.stdout[-3000:]}\n{r.stderr[-3000:]}")
-        return read_dump(dump)
+        out = read_dump(dump)
+        # pressure-coefficient files written by calcCoef (src/analyze.c:
+        # 302-367), as arrays of (x, y, phi, cp) rows
+        for name in sorted(os.listdir(tmp)):
+            if "_CP_" in name and name.endswith(".csv"):
+                side = "cp_pressure" if "pressureSide" in name else "cp_suction"
+                out[side] = np.genfromtxt(os.path.join(tmp, name), delimiter=",",
+                                          skip_header=1).reshape(-1, 4)
+        return out

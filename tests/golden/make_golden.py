@@ -74,6 +74,8 @@ def ref_small() -> dict:
             arrays[f"{key}/info"] = d["run_info"]
             arrays[f"{key}/history"] = d["history"]
             arrays[f"{key}/clcd"] = d["clcd"]
+            arrays[f"{key}/cp_pressure"] = d["cp_pressure"]
+            arrays[f"{key}/cp_suction"] = d["cp_suction"]
     return arrays
 
 
