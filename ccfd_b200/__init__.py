@@ -265,6 +265,14 @@ class Solver:
         """The reference's CP files <base>_CP_pressureSide.csv / _CP_suctionSide.csv."""
         _check(N.lib.ccfd_write_cp(self._ctx, os.fsencode(base)), "ccfd_write_cp")
 
+    def errors(self, exact_func: int | None = None) -> dict:
+        """calcErrors at the current time (ccfd_errors): L1, L2 and Linf of
+        the primitive variables against the case's exact function."""
+        which = self.case.c.exact_func if exact_func is None else exact_func
+        e = np.empty(12)
+        _check(N.lib.ccfd_errors(self._ctx, int(which), _dptr(e)), "ccfd_errors")
+        return {"L1": e[0:4].copy(), "L2": e[4:8].copy(), "Linf": e[8:12].copy()}
+
     def clcd(self):
         cl, cd = C.c_double(), C.c_double()
         _check(N.lib.ccfd_clcd(self._ctx, C.byref(cl), C.byref(cd)), "ccfd_clcd")

@@ -31,6 +31,7 @@ class Params(C.Structure):
         ("eps_newton", c_double), ("eps_gmres", c_double), ("gamma_ew", c_double),
         ("calc_wing", c_int), ("wall_id", c_int), ("ref_length", c_double),
         ("precision", c_int), ("rel_abort_residual", c_double),
+        ("source_func", c_int), ("exact_solution", c_int),
     ]
 
 
@@ -55,7 +56,7 @@ class Mesh(C.Structure):
         ("face_cells", P(c_long)), ("face_hs", P(c_long)), ("face_n", P(c_double)),
         ("face_len", P(c_double)), ("face_bb", P(c_double)), ("ghost_gp", P(c_double)),
         ("bc_face", P(c_long)), ("bc_index", P(c_int)), ("bc_ghost_bary", P(c_double)),
-        ("bc_x", P(c_double)),
+        ("bc_x", P(c_double)), ("cell_gp5", P(c_double)),
         ("total_area_q", c_double), ("dx_ref", c_double), ("x_min", c_double),
         ("x_max", c_double), ("y_min", c_double), ("y_max", c_double),
     ]
@@ -116,6 +117,7 @@ def _load():
                                   P(c_int), P(c_double)]),
         "ccfd_wall_cp": (c_int, [C.c_void_p, P(c_double), P(c_double), P(c_double), P(c_int), P(c_int)]),
         "ccfd_write_cp": (c_int, [C.c_void_p, C.c_char_p]),
+        "ccfd_errors": (c_int, [C.c_void_p, c_int, P(c_double)]),
         "ccfd_write_output": (c_int, [C.c_void_p, P(c_double), c_double, c_long, C.c_char_p, C.c_size_t]),
         "ccfd_batch_create": (c_int, [c_int, P(C.c_void_p)]),
         "ccfd_batch_destroy": (None, [C.c_void_p]),

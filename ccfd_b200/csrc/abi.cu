@@ -100,7 +100,8 @@ extern "C" int ccfd_create(const ccfd_params* params, ccfd_ctx** out) {
     if (p.flux < 1 || p.flux > 11 || p.spatial_order < 1 || p.spatial_order > 2 ||
         (p.spatial_order == 2 && p.limiter != 1 && p.limiter != 2) || p.time_order < 1 ||
         p.time_order > 3 ||
-        (!(p.n_rk_stages == 1 && p.time_order == 1) && (p.n_rk_stages < 3 || p.n_rk_stages > 5)))
+        (!(p.n_rk_stages == 1 && p.time_order == 1) && (p.n_rk_stages < 3 || p.n_rk_stages > 5)) ||
+        p.source_func < 0 || p.source_func > 1)
         return CCFD_ERR_ARG;
     if (p.time_step_1d && p.mu > 1e-10 && p.eqn == CCFD_NAVIER_STOKES)
         return CCFD_ERR_ARG; /* src/timeDiscretization.c:264-267 */
@@ -225,7 +226,7 @@ extern "C" int ccfd_upload_case(ccfd_ctx* ctx, const ccfd_mesh* m, const ccfd_bc
 
     // per-cell CSR in device order
     std::vector<int> hs_off(N + 1), hs_nb;
-    std::vector<double4> hs_gw, cell_geo(N);
+    std::vector<double4> hs_gw, cell_geo(N), cell_xq(N);
     std::vector<int> hs_dev_of_ref(m->n_half_sides);
     hs_nb.reserve(m->n_half_sides);
     hs_gw.reserve(m->n_half_sides);
@@ -240,6 +241,9 @@ extern "C" int ccfd_upload_case(ccfd_ctx* ctx, const ccfd_mesh* m, const ccfd_bc
         }
         cell_geo[d] = make_double4(m->cell_geo[4 * c], m->cell_geo[4 * c + 1], m->cell_geo[4 * c + 2],
                                    m->cell_geo[4 * c + 3]);
+        const double* b = &m->cell_bary[2 * c];
+        const double* q5 = m->cell_gp5 ? &m->cell_gp5[2 * c] : b;
+        cell_xq[d] = make_double4(b[0], b[1], q5[0], q5[1]);
     }
     hs_off[N] = (int)hs_nb.size();
     std::vector<double> venk(N, 0.0);
@@ -297,9 +301,16 @@ extern "C" int ccfd_upload_case(ccfd_ctx* ctx, const ccfd_mesh* m, const ccfd_bc
         (st = dupload_c(ctx, &td.gl_off, gl_off)) || (st = dupload_c(ctx, &td.hs_loc, hs_loc)) ||
         (st = dupload_c(ctx, &td.f_off, ts.f_off)) || (st = dupload_c(ctx, &td.f_id, ts.f_id)) ||
         (st = dupload_c(ctx, &td.f_lr, ts.f_lr)) || (st = dupload_c(ctx, &td.f_hs, ts.f_hs)) ||
-        (st = dupload_c(ctx, &td.u_code, ts.u_code))) {
+        (st = dupload_c(ctx, &td.u_code, ts.u_code)) || (st = dupload_c(ctx, &ctx->cell_xq, cell_xq))) {
         free_device(ctx);
         return st;
+    }
+    if (p.source_func) {
+        dm.cell_src = ctx->cell_xq;
+        if ((st = dalloc(ctx, &dm.src_buf, (size_t)N))) {
+            free_device(ctx);
+            return st;
+        }
     }
     dm.N = (int)N;
     dm.F = (int)FI;
@@ -331,6 +342,7 @@ extern "C" int ccfd_upload_case(ccfd_ctx* ctx, const ccfd_mesh* m, const ccfd_bc
     P.nbc = n_bc;
     P.order = p.spatial_order;
     P.eqn = p.eqn;
+    P.source_func = p.source_func;
     for (int i = 0; i < n_bc; ++i) {
         P.bc[i].type = bc[i].type;
         P.bc[i].exact_func = bc[i].exact_func;
@@ -602,6 +614,61 @@ extern "C" int ccfd_residual(ccfd_ctx* ctx, double time, double* u_t_out, double
             s[0] = h[2 * d].x; s[1] = h[2 * d].y; s[2] = h[2 * d].z; s[3] = h[2 * d].w;
             s[4] = h[2 * d + 1].x; s[5] = h[2 * d + 1].y; s[6] = h[2 * d + 1].z; s[7] = h[2 * d + 1].w;
         }
+    }
+    return check_flags(ctx);
+}
+
+// calcErrors (src/analyze.c:445-514) at the current time: the limited
+// gradients of the current state (spatialReconstruction, as one residual
+// evaluation that writes only the gradients), then the per-cell quadrature
+// errors against exact function `exact_func` and the CTA partials summed
+// here in CTA order.
+extern "C" int ccfd_errors(ccfd_ctx* ctx, int exact_func, double out[12]) {
+    if (!ctx || !out || !ctx->uploaded || exact_func < 1 || exact_func > 6) return CCFD_ERR_ARG;
+    if (ctx->batch) return CCFD_ERR_BUSY;
+    CK(cudaSetDevice(ctx->device));
+    double t = 0.0;
+    int st = ccfd_get_time(ctx, &t);
+    if (st) return st;
+    const bool second = ctx->params.spatial_order == 2;
+    if (second) {
+        StageLaunch L;
+        ccfd_fill_stage(ctx, L);
+        L.ctrl = nullptr;
+        L.tfix = t;
+        L.mode = 0;
+        L.prim_in = cur_prim(ctx);
+        L.u_t = nullptr;
+        L.grad_out = ctx->grad;
+        L.res_partial = nullptr;
+        L.ghost_pface = nullptr;
+        launch_stage(L, ctx->stream);
+        CK(cudaGetLastError());
+    }
+    const int nb = error_blocks((int)ctx->N);
+    double* part = nullptr;
+    CK(cudaMallocAsync((void**)&part, sizeof(double) * 12 * nb, ctx->stream));
+    launch_errors(ctx->mesh, ctx->cell_xq, cur_prim(ctx), second ? ctx->grad : nullptr, ctx->phys_g, exact_func, t,
+                  part, ctx->flags, ctx->stream);
+    cudaError_t le = cudaGetLastError();
+    std::vector<double> h(12 * (size_t)nb);
+    cudaError_t ce = le == cudaSuccess ? cudaMemcpyAsync(h.data(), part, sizeof(double) * h.size(),
+                                                         cudaMemcpyDeviceToHost, ctx->stream)
+                                       : le;
+    cudaFreeAsync(part, ctx->stream);
+    CK(ce);
+    CK(cudaStreamSynchronize(ctx->stream));
+    double l1[4] = {0, 0, 0, 0}, l2[4] = {0, 0, 0, 0}, li[4] = {0, 0, 0, 0};
+    for (int b = 0; b < nb; ++b)
+        for (int v = 0; v < 4; ++v) {
+            l1[v] += h[12 * b + v];
+            l2[v] += h[12 * b + 4 + v];
+            li[v] = fmax(li[v], h[12 * b + 8 + v]);
+        }
+    for (int v = 0; v < 4; ++v) {
+        out[v] = l1[v] * ctx->total_area_q;
+        out[4 + v] = sqrt(l2[v] * ctx->total_area_q);
+        out[8 + v] = li[v];
     }
     return check_flags(ctx);
 }

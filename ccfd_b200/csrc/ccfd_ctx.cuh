@@ -36,6 +36,7 @@ struct ccfd_ctx {
     double4* cons0 = nullptr;
     double4* u_t = nullptr;
     double4* grad = nullptr;
+    const double4* cell_xq = nullptr;  // [N] (bary, fifth quad point): source term and error norms
     unsigned* ticket = nullptr;
     ccfd::Phys* phys_g = nullptr;
     double* ghost_pface = nullptr;

@@ -71,6 +71,18 @@ int main(int argc, char **argv)
 		printf("cl %.12g  cd %.12g\n", rep.cl, rep.cd);
 	if (c->params.implicit)
 		printf("newton %ld  gmres %ld\n", rep.newton_iterations, rep.gmres_iterations);
+	if (c->params.exact_solution && c->exact_func > 0) {
+		/* the error analysis printed at the end of timeDisc
+		 * (src/analyze.c:506-513) */
+		double e[12];
+		if ((st = ccfd_errors(ctx, c->exact_func, e)))
+			return fail("errors", st);
+		printf("\nError Analysis at t = %g\n", rep.t);
+		printf("|                RHO           VX           VY            P\n");
+		printf("| L1  :  %7.5e  %7.5e  %7.5e  %7.5e\n", e[0], e[1], e[2], e[3]);
+		printf("| L2  :  %7.5e  %7.5e  %7.5e  %7.5e\n", e[4], e[5], e[6], e[7]);
+		printf("| Linf:  %7.5e  %7.5e  %7.5e  %7.5e\n", e[8], e[9], e[10], e[11]);
+	}
 	if (output) {
 		double *prim = malloc(sizeof(double) * 4 * (size_t)c->mesh.n_cells);
 		if (!prim)

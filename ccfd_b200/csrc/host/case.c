@@ -231,9 +231,14 @@ int ccfd_case_load_text(const char *text, const char *base_dir, ccfd_case **out)
 	}
 	P->flux = (int)lv;
 	TRY(ccfd_ini_bool(ini, "calcSource", "F", &bv));
+	P->source_func = 0;
 	if (bv) {
-		st = CCFD_ERR_UNSUPPORTED; /* manufactured source, src/source.c */
-		goto fail;
+		TRY(ccfd_ini_int(ini, "sourceFunction", NULL, &lv));
+		if (lv != 1) {
+			st = CCFD_ERR_INI; /* src/source.c knows source 1 only */
+			goto fail;
+		}
+		P->source_func = (int)lv;
 	}
 
 	/* initBoundary */
@@ -510,6 +515,7 @@ int ccfd_case_load_text(const char *text, const char *base_dir, ccfd_case **out)
 	/* initAnalyze */
 	int has_exact;
 	TRY(ccfd_ini_bool(ini, "exactSolution", "F", &has_exact));
+	P->exact_solution = has_exact;
 	TRY(ccfd_ini_bool(ini, "calcWing", "F", &P->calc_wing));
 	P->ref_length = 1.0;
 	if (P->calc_wing) {

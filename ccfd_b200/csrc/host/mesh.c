@@ -91,6 +91,7 @@ void ccfd_mesh_free(ccfd_mesh *m)
 	free(m->face_len); free(m->face_bb); free(m->ghost_gp);
 	free(m->bc_face); free(m->bc_index); free(m->bc_ghost_bary);
 	free(m->bc_x);
+	free(m->cell_gp5);
 	memset(m, 0, sizeof(*m));
 }
 
@@ -363,6 +364,7 @@ int ccfd_mesh_build(const double *nodes, long n_nodes,
 	m->cell_type = malloc(sizeof(int) * N);
 	m->cell_domain = malloc(sizeof(int) * N);
 	m->cell_bary = malloc(sizeof(double) * 2 * N);
+	m->cell_gp5 = malloc(sizeof(double) * 2 * N);
 	m->cell_geo = malloc(sizeof(double) * 4 * N);
 	m->hs_offset = malloc(sizeof(long) * (N + 1));
 	m->hs_face = malloc(sizeof(long) * H);
@@ -382,7 +384,7 @@ int ccfd_mesh_build(const double *nodes, long n_nodes,
 	m->bc_x = malloc(sizeof(double) * 2 * (B + 1));
 	long *hs_face_of = malloc(sizeof(long) * n_created);
 	long *hs_pos = malloc(sizeof(long) * n_created);
-	if (!m->cell_type || !m->cell_domain || !m->cell_bary || !m->cell_geo ||
+	if (!m->cell_type || !m->cell_domain || !m->cell_bary || !m->cell_geo || !m->cell_gp5 ||
 	    !m->hs_offset || !m->hs_face || !m->hs_sign || !m->hs_nb ||
 	    !m->hs_gp || !m->hs_w || !m->face_cells || !m->face_hs ||
 	    !m->face_n || !m->face_len || !m->face_bb || !m->ghost_gp ||
@@ -404,6 +406,14 @@ int ccfd_mesh_build(const double *nodes, long n_nodes,
 		m->cell_domain[e] = edom[e];
 		m->cell_bary[2 * e] = bary[2 * e];
 		m->cell_bary[2 * e + 1] = bary[2 * e + 1];
+		if (etype[e] == 4) {
+			const double *x0 = &nodes[2 * enode[4 * e]], *x2 = &nodes[2 * enode[4 * e + 2]];
+			m->cell_gp5[2 * e] = 0.5 * (x0[0] + x2[0]);
+			m->cell_gp5[2 * e + 1] = 0.5 * (x0[1] + x2[1]);
+		} else {
+			m->cell_gp5[2 * e] = bary[2 * e];
+			m->cell_gp5[2 * e + 1] = bary[2 * e + 1];
+		}
 		memcpy(&m->cell_geo[4 * e], &geo[4 * e], sizeof(double) * 4);
 		m->hs_offset[e] = k;
 		for (int j = etype[e] - 1; j >= 0; --j, ++k) {

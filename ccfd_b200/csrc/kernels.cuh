@@ -87,6 +87,10 @@ void launch_dt(const DevMesh& m, const Phys& P, const Ctrl* ctrl, const StepPara
                const double4* prim, double2* partial, int* bad_partial, cudaStream_t st);
 void launch_step_begin(Ctrl* ctrl, const StepParams& sp, const double2* partial,
                        const int* bad_partial, int nb, cudaStream_t st);
+int error_blocks(int n_cells);
+void launch_errors(const DevMesh& m, const double4* xq, const double4* prim, const double4* grad,
+                   const Phys* phys_g, int which, double time, double* partial, unsigned* flags,
+                   cudaStream_t st);
 void imp_step_end_launch(Ctrl* ctrl, const StepParams& sp, const double* res_partial, int nres,
                          const double2* dt_partial, const int* dt_bad, int ndt, const int* wall_ghost,
                          const double* wall_nl, const double* ghost_pface, cudaStream_t st);

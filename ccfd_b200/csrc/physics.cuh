@@ -37,6 +37,7 @@ struct Phys {
     int nbc;
     int order;      // spatial order 1 / 2
     int eqn;        // 0 Euler, 1 Navier-Stokes
+    int source_func;  // calcSource / sourceFunction, 0: no source term
     DevBC bc[kMaxBC];
     DevExact ex;
 };
@@ -55,6 +56,50 @@ template <typename T>
 struct V4 {
     T v[4];
 };
+
+// evalSource, source function 1 (src/source.c:22-60): the source of the
+// manufactured sine-wave solution (exact function 3); adds source * w to q.
+// The operation order is the reference's; cos / sin are CUDA's and may
+// differ from the C library's in the last bit.
+__device__ __forceinline__ void add_source(const Phys& P, double x, double y, double time, double w,
+                                           double q[4]) {
+    const double freq = 1.0, amp = 0.1;
+    const double om = P.pi * freq;
+    const double a = 2.0 * P.pi;
+    const double tmp1 = cos(om * (x + y) - a * time);
+    const double tmp2 = sin(2.0 * (om * (x + y) - a * time));
+    double s0 = (-a + 2.0 * om) * tmp1;
+    double s1 = (-a + om * (P.gam * 3.0 - 1.0)) * tmp1 + amp * om * P.gam1 * tmp2;
+    double s3 = ((2.0 + P.gam * 6.0) * om - 4.0 * a) * tmp1 + amp * (2.0 * om * P.gam - a) * tmp2;
+    if (P.eqn == 1) {
+        const double tmp3 = sin(om * (x + y) - a * time);
+        s3 = s3 + 2.0 * P.mu * P.gam * om * om / P.Pr * tmp3;
+    }
+    s0 *= amp;
+    s1 *= amp;
+    s3 *= amp;
+    q[0] += s0 * w;
+    q[1] += s1 * w;
+    q[2] += s1 * w;
+    q[3] += s3 * w;
+}
+
+// calcSource (src/source.c:66-85) for one cell: side quadrature points
+// bary + GP in side order (weight area/3 for triangles, area/6 for quads),
+// then the quad's fifth point, the midpoint of its nodes 0 and 2
+// (src/mesh.c:117-161).  xq = (bary.x, bary.y, gp5.x, gp5.y).
+__device__ __forceinline__ double4 cell_source(const Phys& P, const double4* __restrict__ hs_gw, int h0, int h1,
+                                               double4 xq, double area, double time) {
+    double q[4] = {0.0, 0.0, 0.0, 0.0};
+    const bool quad = h1 - h0 == 4;
+    const double w = quad ? area / 6.0 : area / 3.0;
+    for (int h = h0; h < h1; ++h) {
+        double4 gw = hs_gw[h];
+        add_source(P, xq.x + gw.x, xq.y + gw.y, time, w, q);
+    }
+    if (quad) add_source(P, xq.z, xq.w, time, area / 3.0, q);
+    return make_double4(q[0], q[1], q[2], q[3]);
+}
 
 // primCons, src/equationOfState.c:19-26
 __device__ __forceinline__ void prim_cons(double gam1q, const double p[4], double c[4]) {

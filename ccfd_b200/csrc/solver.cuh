@@ -19,6 +19,8 @@ struct DevMesh {
     const double* venk_eps2;  // [N] Venkatakrishnan epsilon^2
     const double4* face_nl;   // [F] (n.x, n.y, len, 0) of interior faces
     const double4* face_bb;   // [F] (baryBaryVec.x, .y, baryBaryDist, 0)
+    const double4* cell_src;  // [N] (bary, fifth quad point) when the source term is on, else nullptr
+    double4* src_buf;         // [N] the cells' source term of the running evaluation (with cell_src)
 };
 
 // Time-loop control block in device memory.  The time step, simulation time,

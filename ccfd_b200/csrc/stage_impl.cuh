@@ -426,6 +426,16 @@ __device__ __forceinline__ void stage_body(const StageLaunch& L, const int t) {
     V2* hgp = reinterpret_cast<V2*>(gs + 2 * T.max_g);  // [max_hs] GP
     V4* fs = reinterpret_cast<V4*>(hgp + T.max_hs + (T.max_hs & 1));  // [max_f]
 
+    // source term of the tile's cells (calcSource), evaluated first, while
+    // few registers are live, into a per-cell buffer that the same thread
+    // reads back in D (same cell-to-thread mapping)
+    if (m.cell_src)
+        for (int i = tid; i < nT; i += kThreads) {
+            const int d = T.e_ref[e0 + i];
+            m.src_buf[d] = cell_source(P, m.hs_gw, m.hs_off[d], m.hs_off[d + 1], m.cell_src[d],
+                                       m.cell_geo[d].x, time);
+        }
+
     // A: stage the states of the tile and its rings; ghost cells get the
     // boundary state at their mirrored barycentre (second order only: the
     // reference sets ghost cell states in its second-order reconstruction
@@ -539,9 +549,11 @@ __device__ __forceinline__ void stage_body(const StageLaunch& L, const int t) {
             }
         }
         double4 geo = m.cell_geo[d];
+        const double4 sv = m.cell_src ? m.src_buf[d] : make_double4(0.0, 0.0, 0.0, 0.0);
+        const double src[4] = {sv.x, sv.y, sv.z, sv.w};
         double ut[4];
 #pragma unroll
-        for (int v = 0; v < 4; ++v) ut[v] = (0.0 - s[v]) * geo.y;
+        for (int v = 0; v < 4; ++v) ut[v] = (src[v] - s[v]) * geo.y;
         if (L.u_t) L.u_t[d] = mk4(ut);
         if (!rk && L.grad_out) {
             L.grad_out[2 * d] = ORDER == 2 ? to_d4(gs[2 * i]) : make_double4(0, 0, 0, 0);

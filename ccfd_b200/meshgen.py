@@ -168,6 +168,85 @@ outputFormat = 3
 """
 
 
+def sinewave_mesh(n: int, jitter: float = 0.15, seed: int = 20260005) -> RawMesh:
+    """Square [-1,1]^2 for the manufactured sine-wave solution: n x n cells,
+    interior nodes moved by U(-jitter, jitter) * h (PCG64, ``seed``) so that
+    the quads are general quadrilaterals, every cell whose (i + j) is odd
+    split along its diagonal into two triangles (both quadrature rules in one
+    mesh); all boundary faces 601 (exact solution)."""
+    nodes = _grid_nodes(n, n, -1.0, 1.0, -1.0, 1.0)
+    rng = np.random.Generator(np.random.PCG64(seed))
+    h = 2.0 / n
+    jj, ii = np.meshgrid(np.arange(n + 1), np.arange(n + 1), indexing="ij")
+    interior = ((ii > 0) & (ii < n) & (jj > 0) & (jj < n)).ravel()
+    d = rng.uniform(-jitter, jitter, size=(int(interior.sum()), 2))
+    nodes[interior] += d * h
+    a, b, c, dd = _quad_conn(n, n)
+    j, i = np.meshgrid(np.arange(n), np.arange(n), indexing="ij")
+    odd = ((i + j).ravel() % 2) == 1
+    one = np.ones(int((~odd).sum()), dtype=np.int64)
+    quad = np.stack([a[~odd], b[~odd], c[~odd], dd[~odd], one], axis=1)
+    t1 = np.stack([a[odd], b[odd], c[odd], np.ones_like(a[odd])], axis=1)
+    t2 = np.stack([a[odd], c[odd], dd[odd], np.ones_like(a[odd])], axis=1)
+    tria = np.concatenate([t1, t2])
+    bc = []
+    for k in range(n):
+        bc.append((k, k + 1, 601))
+        bc.append(((k + 1) * (n + 1) - 1, (k + 2) * (n + 1) - 1, 601))
+        bc.append((n * (n + 1) + k, n * (n + 1) + k + 1, 601))
+        bc.append((k * (n + 1), (k + 1) * (n + 1), 601))
+    return RawMesh(nodes, tria=tria, quad=quad, bc=np.array(bc))
+
+
+def sinewave_ini(mesh_file: str | None, n: int = 16, order: int = 2, limiter: int = 1,
+                 flux: int = 2, navier_stokes: bool = False, mu: float = 0.01,
+                 source: bool = True, t_end: float = 0.05, cfl: float = 0.9,
+                 time_order: int = 2, rk_stages: int = 3) -> str:
+    """Manufactured sine-wave solution (exact function 3 with source
+    function 1), the convergence case of the reference's calc/sinewave.
+    ``mesh_file`` None: the reference's own Cartesian n x n mesh on
+    [-1,1]^2."""
+    if mesh_file is None:
+        mesh = f"""meshType = 1
+nElemsX = {n}
+nElemsY = {n}
+X0 = (/-1.0, -1.0/)
+Xmax = (/1.0, 1.0/)
+nBCsegments = (/1, 1, 1, 1/)
+meshBCtype = 601
+meshBCtype = 601
+meshBCtype = 601
+meshBCtype = 601
+"""
+    else:
+        base = mesh_file[:-4] if mesh_file.endswith(".msh") else mesh_file
+        mesh = f"meshType = 0\nmeshFormat = .msh\nmeshFile = {base}\n"
+    ns = f"navierStokes = T\nmu = {mu}\nPr = 0.72\n" if navier_stokes else ""
+    src = "calcSource = T\nsourceFunction = 1\n" if source else "calcSource = F\n"
+    return f"""! manufactured sine-wave solution
+{ns}{mesh}nBC = 1
+BCtype = 601
+BCexactFunc = 3
+icType = 2
+exactFunc = 3
+{src}exactSolution = T
+fluxFunction = {flux}
+spatialOrder = {order}
+limiter = {limiter}
+venk_k = 5.0
+timeOrder = {time_order}
+nRKstages = {rk_stages}
+CFL = {cfl}
+stationary = F
+tEnd = {t_end}
+maxIter = 1000000
+fileName = sinewave
+IOtimeInterval = {t_end}
+IOiterInterval = 100000000
+outputFormat = 3
+"""
+
+
 def riemann2d_mesh(n: int) -> RawMesh:
     """Unit square, n x n quads, four quadrant domains (physical groups 1..4
     counter-clockwise from the upper right), outflow (401) on all sides."""

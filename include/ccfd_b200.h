@@ -102,6 +102,8 @@ typedef struct ccfd_params {
 	double ref_length;     /* referenceLength                               */
 	int precision;         /* enum ccfd_precision                           */
 	double rel_abort_residual; /* >0: stop when res/res_first <= this (extension) */
+	int source_func;       /* calcSource / sourceFunction (0: none), src/source.c */
+	int exact_solution;    /* exactSolution (error norms at the end of a run) */
 } ccfd_params;
 
 /* one boundary condition, src/boundary.h:19-46, parsed by initBoundary
@@ -159,6 +161,9 @@ typedef struct ccfd_mesh {
 	int *bc_index;         /* [B] index into the BC table                   */
 	double *bc_ghost_bary; /* [B][2] mirrored ghost barycentre              */
 	double *bc_x;          /* [B][2] face midpoint, side->GP + elem->bary   */
+	double *cell_gp5;      /* [N][2] fifth quadrature point of a quad (midpoint
+				  of its nodes 0 and 2, src/mesh.c:157-160);
+				  the barycentre for triangles                */
 	double total_area_q, dx_ref, x_min, x_max, y_min, y_max;
 } ccfd_mesh;
 
@@ -291,6 +296,14 @@ int ccfd_wall_cp(ccfd_ctx *ctx, double *x, double *y, double *cp, int *n, int *n
 /* The reference's CP files <base>_CP_pressureSide.csv / _CP_suctionSide.csv
  * (rows x, y, phi, cp). */
 int ccfd_write_cp(ccfd_ctx *ctx, const char *base);
+
+/* Drop-in for calcErrors (src/analyze.c:445-514) at the current time: L1,
+ * L2 and Linf norms of the primitive variables against exact function
+ * exact_func (the case's exactFunc), over the element quadrature points
+ * with the solution expanded by the limited gradients of the current
+ * state.  out = {L1[4], L2[4], Linf[4]}.  Allocates a per-call partial-sum
+ * buffer (stream-ordered). */
+int ccfd_errors(ccfd_ctx *ctx, int exact_func, double out[12]);
 
 /* Autotuner (no counterpart in the reference): re-uploads the case with
  * each candidate launch shape of the stage kernel (cells per tile 128..384,

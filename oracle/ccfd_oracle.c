@@ -603,6 +603,67 @@ static void o_init(orc *o, const ccfd_case *cs, const double *eps2)
 	o->vacuum = 0;
 }
 
+/* evalSource, source function 1 (src/source.c:22-60): source of the
+ * manufactured sine-wave solution (exactFunc 3) */
+static void o_source(const orc *o, const double x[2], double t, double s[4])
+{
+	double freq = 1.0, amp = 0.1;
+	double om = o->pi * freq;
+	double a = 2.0 * o->pi;
+	double tmp1 = cos(om * (x[0] + x[1]) - a * t);
+	double tmp2 = sin(2.0 * (om * (x[0] + x[1]) - a * t));
+	s[0] = (-a + 2.0 * om) * tmp1;
+	s[1] = (-a + om * (o->gam * 3.0 - 1.0)) * tmp1 + amp * om * o->gam1 * tmp2;
+	s[2] = s[1];
+	if (o->eqn == CCFD_NAVIER_STOKES) {
+		double tmp3 = sin(om * (x[0] + x[1]) - a * t);
+		s[3] = ((2.0 + o->gam * 6.0) * om - 4.0 * a) * tmp1 + amp * (2.0 * om * o->gam - a) * tmp2 +
+		       2.0 * o->mu * o->gam * om * om / o->Pr * tmp3;
+	} else {
+		s[3] = ((2.0 + o->gam * 6.0) * om - 4.0 * a) * tmp1 + amp * (2.0 * om * o->gam - a) * tmp2;
+	}
+	for (int v = 0; v < NV; ++v)
+		s[v] *= amp;
+}
+
+/* element quadrature points and weights (createReconstructionInfo,
+ * src/mesh.c:114-161): bary + side GP in side order (area/3 for triangles,
+ * area/6 for quads), then a quad's fifth point, the midpoint of nodes 0 and
+ * 2, with area/3; returns the point count */
+static int o_elem_gp(const ccfd_mesh *m, long c, double x[5][2], double w[5])
+{
+	long h0 = m->hs_offset[c], h1 = m->hs_offset[c + 1];
+	int ns = (int)(h1 - h0);
+	double area = m->cell_geo[4 * c];
+	const double *b = &m->cell_bary[2 * c];
+	for (int k = 0; k < ns; ++k) {
+		x[k][0] = b[0] + m->hs_gp[2 * (h0 + k)];
+		x[k][1] = b[1] + m->hs_gp[2 * (h0 + k) + 1];
+		w[k] = ns == 4 ? area / 6.0 : area / 3.0;
+	}
+	if (ns == 4) {
+		x[4][0] = m->cell_gp5[2 * c];
+		x[4][1] = m->cell_gp5[2 * c + 1];
+		w[4] = area / 3.0;
+		return 5;
+	}
+	return ns;
+}
+
+/* calcSource (src/source.c:66-85) for element c */
+static void o_cell_source(const orc *o, const ccfd_mesh *m, long c, double t, double src[4])
+{
+	double x[5][2], w[5], s[4];
+	int n = o_elem_gp(m, c, x, w);
+	for (int v = 0; v < NV; ++v)
+		src[v] = 0.0;
+	for (int k = 0; k < n; ++k) {
+		o_source(o, x[k], t, s);
+		for (int v = 0; v < NV; ++v)
+			src[v] += s[v] * w[k];
+	}
+}
+
 /* ghost-cell state at the mirrored barycentre of ghost b (setBCatBarys) */
 static void o_ghost_bary(orc *o, long b, double t, const double *prim, double out[4])
 {
@@ -772,8 +833,11 @@ int oracle_residual(const ccfd_case *cs, const double *prim, double t, double *u
 			for (int v = 0; v < NV; ++v)
 				s[v] += m->hs_sign[h] > 0 ? F4[v] : -F4[v];
 		}
+		double src[4] = {0.0, 0.0, 0.0, 0.0};
+		if (cs->params.source_func)
+			o_cell_source(&o, m, c, t, src);
 		for (int v = 0; v < NV; ++v)
-			u_t[4 * c + v] = (0.0 - s[v]) * m->cell_geo[4 * c + 1];
+			u_t[4 * c + v] = (src[v] - s[v]) * m->cell_geo[4 * c + 1];
 	}
 	if (grad)
 		memcpy(grad, g, sizeof(double) * 8 * N);
@@ -782,6 +846,51 @@ int oracle_residual(const ccfd_case *cs, const double *prim, double t, double *u
 	int vac = o.vacuum;
 	free(g); free(gb); free(ff); free(eps2);
 	return vac ? CCFD_ERR_VACUUM : CCFD_OK;
+}
+
+/* calcErrors (src/analyze.c:445-514) of primitive state prim at time t
+ * against exact function `which`: out = {L1[4], L2[4], Linf[4]}, summed in
+ * element order */
+int oracle_errors(const ccfd_case *cs, const double *prim, double t, int which, double out[12])
+{
+	const ccfd_mesh *m = &cs->mesh;
+	const long N = m->n_cells;
+	double *ut = malloc(sizeof(double) * 4 * N);
+	double *g = calloc(8 * N, sizeof(double));
+	if (!ut || !g) {
+		free(ut); free(g);
+		return CCFD_ERR_NOMEM;
+	}
+	int st = CCFD_OK;
+	if (cs->params.spatial_order == 2)
+		st = oracle_residual(cs, prim, t, ut, g, NULL, NULL);
+	orc o;
+	o_init(&o, cs, NULL);
+	double L1[4] = {0, 0, 0, 0}, L2[4] = {0, 0, 0, 0}, Li[4] = {0, 0, 0, 0};
+	for (long c = 0; c < N && st == CCFD_OK; ++c) {
+		double x[5][2], w[5];
+		int n = o_elem_gp(m, c, x, w);
+		const double *b = &m->cell_bary[2 * c];
+		for (int k = 0; k < n; ++k) {
+			double ex[4];
+			o_exact(&o, which, x[k], t, ex);
+			double dx[2] = {x[k][0] - b[0], x[k][1] - b[1]};
+			for (int v = 0; v < NV; ++v) {
+				double q = prim[4 * c + v] + dx[0] * g[8 * c + v] + dx[1] * g[8 * c + 4 + v];
+				double err = fabs(ex[v] - q);
+				Li[v] = fmax(Li[v], err);
+				L1[v] += err * w[k];
+				L2[v] += err * err * w[k];
+			}
+		}
+	}
+	for (int v = 0; v < NV; ++v) {
+		out[v] = L1[v] * m->total_area_q;
+		out[4 + v] = sqrt(L2[v] * m->total_area_q);
+		out[8 + v] = Li[v];
+	}
+	free(ut); free(g);
+	return st;
 }
 
 /* ---------------- time loop, src/timeDiscretization.c:249-731 ----------- */

@@ -16,6 +16,8 @@
  *                        559-732) without file output, at most nsteps
  *                        iterations (<=0: until tEnd / convergence)
  *   coef                 like run, plus calcCoef (src/analyze.c:292) per step
+ *                        run / coef end with calcErrors (src/analyze.c:445)
+ *                        when the case has an exact solution
  *
  * The initialisation order mirrors main() (src/main.c:53-118).  Output format
  * is forced to CSV so that the CGNS stand-in is never reached.
@@ -345,6 +347,23 @@ int main(int argc, char *argv[])
 		}
 		double tEnd = omp_get_wtime();
 		dump_state();
+		if (hasExactSolution) {
+			/* the error analysis that ends timeDisc (src/analyze.c:
+			 * 445-514) prints the norms; the gradients it reconstructs
+			 * are dumped for a full-precision check */
+			calcErrors(t);
+			double *ux = malloc(sizeof(double) * 4 * nElems);
+			double *uy = malloc(sizeof(double) * 4 * nElems);
+			for (long i = 0; i < nElems; ++i)
+				for (int v = 0; v < 4; ++v) {
+					ux[4 * i + v] = elem[i]->u_x[v];
+					uy[4 * i + v] = elem[i]->u_y[v];
+				}
+			dump_f64("err_u_x", ux, 4 * nElems);
+			dump_f64("err_u_y", uy, 4 * nElems);
+			free(ux);
+			free(uy);
+		}
 		dump_f64("history", hist, 8 * nhist);
 		dump_f64("step_wall", wall, nhist);
 		double info[8] = {t, (double)nhist, tEnd - tStart,

@@ -84,6 +84,11 @@ def run_ref(ini_text: str, mode: str, *args, eqn: str = "euler",
             raise RuntimeError(f"reference driver failed ({r.returncode}):\n"
                                f"{r.stdout[-3000:]}\n{r.stderr[-3000:]}")
         out = read_dump(dump)
+        # error norms printed by calcErrors (src/analyze.c:506-513)
+        rows = [ln.split(":", 1)[1].split() for ln in r.stdout.splitlines()
+                if ln.startswith(("| L1  :", "| L2  :", "| Linf:"))]
+        if len(rows) >= 3:
+            out["errors_printed"] = np.array(rows[-3:], dtype=np.float64)
         # pressure-coefficient files written by calcCoef (src/analyze.c:
         # 302-367), as arrays of (x, y, phi, cp) rows
         for name in sorted(os.listdir(tmp)):

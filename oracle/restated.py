@@ -45,6 +45,8 @@ def lib():
         L.oracle_time_step.argtypes = [C.c_void_p, dp, C.c_double, C.c_double, dp]
         L.oracle_run_explicit.restype = C.c_int
         L.oracle_run_explicit.argtypes = [C.c_void_p, dp, C.c_long, dp]
+        L.oracle_errors.restype = C.c_int
+        L.oracle_errors.argtypes = [C.c_void_p, dp, C.c_double, C.c_int, dp]
         _lib = L
     return _lib
 
@@ -72,6 +74,17 @@ def residual(case, prim: np.ndarray, time: float = 0.0, with_extras: bool = Fals
     if st != 0:
         raise RuntimeError(f"oracle_residual status {st}")
     return (ut, gr, ff, wp[:m.n_bc]) if with_extras else ut
+
+
+def errors(case, prim: np.ndarray, time: float, exact_func: int | None = None) -> dict:
+    """calcErrors restated: L1, L2, Linf of the primitive variables."""
+    which = case.c.exact_func if exact_func is None else exact_func
+    prim = np.ascontiguousarray(prim, dtype=np.float64).reshape(case.n_cells, 4)
+    e = np.zeros(12)
+    st = lib().oracle_errors(_case_ptr(case), _dp(prim), float(time), int(which), _dp(e))
+    if st != 0:
+        raise RuntimeError(f"oracle_errors status {st}")
+    return {"L1": e[0:4], "L2": e[4:8], "Linf": e[8:12]}
 
 
 def time_step(case, prim: np.ndarray, t: float, print_time: float) -> float:

@@ -108,6 +108,13 @@ def residual_cases() -> dict:
                                      "eqn": "euler", "time": 0.02, "seed": 77 + order + lim}
         cases[f"zoo_ns_{tag}"] = {"mesh": None, "ini": zoo_ini(5, order, lim, ns=True),
                                   "eqn": "navierstokes", "time": 0.02, "seed": 88 + order + lim}
+    # manufactured sine-wave solution with the source term (triangles and
+    # general quads in one mesh)
+    cases["sine_euler_bj"] = {"mesh": ("sine", 12), "ini": meshgen.sinewave_ini("sine", order=2, limiter=1),
+                              "eqn": "euler", "time": 0.13, "seed": 515}
+    cases["sine_ns_vk"] = {"mesh": ("sine", 12),
+                           "ini": meshgen.sinewave_ini("sine", order=2, limiter=2, flux=5, navier_stokes=True),
+                           "eqn": "navierstokes", "time": 0.37, "seed": 516}
     cases["naca_ns_vk"] = {
         "mesh": ("naca", 32, 12),
         "ini": meshgen.airfoil_ini("naca", navier_stokes=True, reynolds=500.0, implicit=False,
@@ -126,6 +133,16 @@ def run_cases() -> dict:
                           "eqn": "euler", "steps": 0},
         "zoo_ns_run": {"mesh": None, "ini": zoo_ini(2, 2, 1, ns=True).replace("tEnd = 10.0", "tEnd = 0.02"),
                        "eqn": "navierstokes", "steps": 0},
+        # manufactured solution runs ending with the error analysis
+        "sine_euler_run": {"mesh": ("sine", 16), "ini": meshgen.sinewave_ini("sine", order=2, limiter=2,
+                                                                             t_end=0.2),
+                           "eqn": "euler", "steps": 0},
+        "sine_ns_run": {"mesh": ("sine", 16), "ini": meshgen.sinewave_ini("sine", order=2, limiter=1, flux=5,
+                                                                          navier_stokes=True, t_end=0.2),
+                        "eqn": "navierstokes", "steps": 0},
+        "sine_cart_o1_run": {"mesh": None, "ini": meshgen.sinewave_ini(None, n=16, order=1, time_order=1,
+                                                                       rk_stages=1, t_end=0.2),
+                             "eqn": "euler", "steps": 0},
     }
 
 
@@ -157,6 +174,8 @@ def make_mesh(spec):
         return None
     if kind[0] == "dmr":
         return "dmr", meshgen.dmr_mesh(kind[1], kind[2])
+    if kind[0] == "sine":
+        return "sine", meshgen.sinewave_mesh(kind[1])
     if kind[0] == "naca":
         wall = kind[3] if len(kind) > 3 else 201
         return "naca", meshgen.naca_ogrid(0.0, 0.0, 0.12, kind[1], kind[2], r_far=5.0, h0=1e-2,

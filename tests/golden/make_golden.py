@@ -49,10 +49,13 @@ def sod_check(ref: str) -> dict:
     return out
 
 
-def ref_small() -> dict:
+def ref_small(only: str | None = None) -> dict:
+    """Reference outputs of every case, or of the cases whose key starts
+    with ``only``."""
     arrays = {}
+    pick = lambda d: {k: v for k, v in d.items() if only is None or k.startswith(only)}
     with tempfile.TemporaryDirectory() as tmp:
-        for key, spec in CASES.residual_cases().items():
+        for key, spec in pick(CASES.residual_cases()).items():
             ini, files = CASES.materialise(spec, tmp)
             prim = CASES.random_state(spec, tmp)
             d = refdump.run_ref(ini, "residual", spec["time"], state=prim, eqn=spec["eqn"],
@@ -61,13 +64,17 @@ def ref_small() -> dict:
             arrays[f"{key}/u_x"] = d["u_x"]
             arrays[f"{key}/u_y"] = d["u_y"]
             arrays[f"{key}/prim"] = prim.ravel()
-        for key, spec in CASES.run_cases().items():
+        for key, spec in pick(CASES.run_cases()).items():
             ini, files = CASES.materialise(spec, tmp)
             d = refdump.run_ref(ini, "run", spec["steps"], eqn=spec["eqn"], files=files)
             arrays[f"{key}/pvar"] = d["pvar"]
             arrays[f"{key}/info"] = d["run_info"]
             arrays[f"{key}/history"] = d["history"]
-        for key, spec in CASES.implicit_cases().items():
+            if "errors_printed" in d:
+                arrays[f"{key}/errors_printed"] = d["errors_printed"]
+                arrays[f"{key}/err_u_x"] = d["err_u_x"]
+                arrays[f"{key}/err_u_y"] = d["err_u_y"]
+        for key, spec in pick(CASES.implicit_cases()).items():
             ini, files = CASES.materialise(spec, tmp)
             d = refdump.run_ref(ini, "coef", spec["steps"], eqn=spec["eqn"], files=files)
             arrays[f"{key}/pvar"] = d["pvar"]
@@ -82,13 +89,24 @@ def ref_small() -> dict:
 def main() -> int:
     ap = argparse.ArgumentParser()
     ap.add_argument("--ref", default="/root/reference")
+    ap.add_argument("--only", default=None,
+                    help="regenerate only the cases whose key starts with this prefix and "
+                         "merge them into the existing ref_small.npz")
     a = ap.parse_args()
     if not refdump.have_ref("euler") or not refdump.have_ref("navierstokes"):
         print("compiled reference missing: run `make -C oracle` first", file=sys.stderr)
         return 1
+    npz = os.path.join(HERE, "ref_small.npz")
+    if a.only:
+        with np.load(npz) as old:
+            arrays = {k: old[k] for k in old.files}
+        arrays.update(ref_small(a.only))
+        np.savez_compressed(npz, **arrays)
+        print(f"updated ref_small.npz ({a.only}*)")
+        return 0
     with open(os.path.join(HERE, "sod_check.json"), "w") as f:
         json.dump(sod_check(a.ref), f)
-    np.savez_compressed(os.path.join(HERE, "ref_small.npz"), **ref_small())
+    np.savez_compressed(npz, **ref_small())
     print("wrote sod_check.json, ref_small.npz")
     return 0
 

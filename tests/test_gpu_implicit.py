@@ -36,3 +36,27 @@ def test_implicit_steps_match_reference(ref_small, key):
     assert abs(rep["cl"] - clcd[0]) <= TOL and abs(rep["cd"] - clcd[1]) <= TOL
     hist = ref_small[f"{key}/history"].reshape(-1, 8)
     np.testing.assert_allclose(rep["residual"][:4], hist[-1, 2:6], rtol=1e-6)
+
+
+@pytest.mark.parametrize("key", ["naca_euler_imp_pc", "naca_ns_imp_pc"])
+def test_wall_pressure_coefficient_matches_reference_files(ref_small, key, tmp_path):
+    # the reference writes CP along the wing with "%15.7f" (calcCoef,
+    # src/analyze.c:302-367); the state agrees to 1e-8, so the files agree to
+    # their printed precision
+    spec = CASES.implicit_cases()[key]
+    with tempfile.TemporaryDirectory() as tmp:
+        case, _, _ = CASES.load_case(spec, tmp)
+    s = cc.Solver(case, reorder=True)
+    s.run(spec["steps"])
+    x, y, cp, npres = s.wall_cp()
+    base = str(tmp_path / "naca")
+    s.write_cp(base)
+    s.close()
+    for side, lo, hi in (("pressure", 0, npres), ("suction", npres, len(cp))):
+        want = ref_small[f"{key}/cp_{side}"].reshape(-1, 4)
+        assert hi - lo == len(want)
+        np.testing.assert_allclose(x[lo:hi], want[:, 0], atol=1e-7, rtol=0)
+        np.testing.assert_allclose(y[lo:hi], want[:, 1], atol=1e-7, rtol=0)
+        np.testing.assert_allclose(cp[lo:hi], want[:, 3], atol=2e-7, rtol=0)
+        got = np.genfromtxt(f"{base}_CP_{side}Side.csv", delimiter=",", skip_header=1).reshape(-1, 4)
+        np.testing.assert_allclose(got, want, atol=2e-7, rtol=0)

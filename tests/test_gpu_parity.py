@@ -148,3 +148,51 @@ def test_nonfinite_time_step_is_reported_not_fatal():
     rep = s.run(3)
     assert rep["iterations"] >= 3
     s.close()
+
+
+SINE_RUNS = ["sine_euler_run", "sine_ns_run", "sine_cart_o1_run"]
+
+
+@pytest.mark.parametrize("key", SINE_RUNS)
+def test_error_norms_match_oracle_and_reference(ref_small, key):
+    # manufactured solution with the source term, then calcErrors
+    # (ccfd_errors) against the oracle on the same state and against the
+    # norms the reference printed
+    spec = CASES.run_cases()[key]
+    with tempfile.TemporaryDirectory() as tmp:
+        case, _, _ = CASES.load_case(spec, tmp)
+        s = cc.Solver(case, reorder=True)
+        rep = s.run(spec["steps"])
+        prim = s.get_state()
+        e = s.errors()
+        s.close()
+        eo = restated.errors(case, prim, rep["t"])
+    for k in ("L1", "L2", "Linf"):
+        np.testing.assert_allclose(e[k], eo[k], rtol=1e-12, atol=0)
+    printed = ref_small[f"{key}/errors_printed"]
+    got = np.stack([e["L1"], e["L2"], e["Linf"]])
+    np.testing.assert_allclose(got, printed, rtol=6e-6, atol=0)
+
+
+def test_driver_prints_error_analysis():
+    import re
+    import subprocess
+    driver = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))),
+                          "ccfd_b200", "lib", "ccfd_run")
+    with tempfile.TemporaryDirectory() as tmp:
+        meshgen.sinewave_mesh(16).write_gmsh(os.path.join(tmp, "sine.msh"))
+        ini = os.path.join(tmp, "sine.ini")
+        with open(ini, "w") as f:
+            f.write(meshgen.sinewave_ini("sine", order=2, limiter=2, t_end=0.2))
+        r = subprocess.run([driver, ini, "--no-output"], capture_output=True, text=True, timeout=300)
+        assert r.returncode == 0, r.stdout + r.stderr
+        case = cc.CaseData.from_text(open(ini).read(), tmp)
+        s = cc.Solver(case)
+        s.run(0)
+        e = s.errors()
+        s.close()
+    rows = {m.group(1): [float(v) for v in m.group(2).split()]
+            for m in re.finditer(r"^\| (L1  |L2  |Linf):\s+(.*)$", r.stdout, re.M)}
+    assert set(rows) == {"L1  ", "L2  ", "Linf"}
+    np.testing.assert_allclose(rows["L1  "], e["L1"], rtol=6e-6)
+    np.testing.assert_allclose(rows["Linf"], e["Linf"], rtol=6e-6)

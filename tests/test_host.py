@@ -2,6 +2,7 @@
 import ctypes as C
 import os
 import re
+import tempfile
 
 import numpy as np
 import pytest
@@ -108,3 +109,32 @@ def test_gmsh_roundtrip(tmp_path):
     assert mm["n_bc"] == 18 and mm["n_faces"] == (3 * 36 + 18) // 2
     # cell areas sum to the domain area
     assert abs(mm["cell_geo"][:, 0].sum() - 4.0) < 1e-12
+
+
+def test_source_term_keys_and_quadrature_points():
+    # calcSource / sourceFunction (src/equation.c:120-123): the function is
+    # mandatory once the source is on; the reference knows function 1 only
+    src = SOD + "calcSource = T\nsourceFunction = 1\nexactSolution = T\n"
+    case = cc.CaseData.from_text(src)
+    assert case.params.source_func == 1 and case.params.exact_solution == 1
+    with pytest.raises(cc.CcfdError) as e:
+        cc.CaseData.from_text(SOD + "calcSource = T\n")
+    assert e.value.status == 9
+    with pytest.raises(cc.CcfdError):
+        cc.CaseData.from_text(SOD + "calcSource = T\nsourceFunction = 2\n")
+    assert cc.CaseData.from_text(SOD).params.source_func == 0
+    # fifth quadrature point of a quad: midpoint of its nodes 0 and 2
+    # (src/mesh.c:157-160); triangles carry their barycentre
+    m = meshgen.sinewave_mesh(4)
+    with tempfile.TemporaryDirectory() as tmp:
+        m.write_gmsh(os.path.join(tmp, "sine.msh"))
+        sc = cc.CaseData.from_text(meshgen.sinewave_ini("sine"), tmp)
+        mesh = sc.c.mesh
+        n = sc.n_cells
+        gp5 = np.ctypeslib.as_array(mesh.cell_gp5, shape=(n * 2,)).reshape(n, 2)
+        bary = sc.mesh()["cell_bary"]
+        ctype = np.ctypeslib.as_array(mesh.cell_type, shape=(n,))
+    assert set(np.unique(ctype)) == {3, 4}
+    tri = ctype == 3
+    assert np.array_equal(gp5[tri], bary[tri])
+    assert np.abs(gp5[~tri] - bary[~tri]).max() > 1e-4  # jittered quads

@@ -83,3 +83,44 @@ def test_mesh_builder_bit_identical_to_reference():
     assert np.array_equal(M["face_n"], fg[:, :2]) and np.array_equal(M["face_len"], fg[:, 2])
     assert (M["total_area_q"], M["dx_ref"]) == tuple(d["mesh_scalars"][:2])
     assert np.array_equal(case.prim0().ravel(), d["pvar"])
+
+
+SINE_RUNS = ["sine_euler_run", "sine_ns_run", "sine_cart_o1_run"]
+
+
+@pytest.mark.parametrize("key", SINE_RUNS)
+def test_oracle_error_norms_match_reference(ref_small, key):
+    # calcErrors restated on the reference's final state: its printed norms
+    # (%7.5e) and, at full precision, the same sums formed from the
+    # gradients the reference reconstructed for them
+    spec = CASES.run_cases()[key]
+    info = ref_small[f"{key}/info"]
+    prim = ref_small[f"{key}/pvar"].reshape(-1, 4)
+    with tempfile.TemporaryDirectory() as tmp:
+        case, _, _ = CASES.load_case(spec, tmp)
+        assert case.c.params.source_func == 1 and case.c.params.exact_solution == 1
+        assert case.c.exact_func == 3
+        e = restated.errors(case, prim, float(info[0]))
+        if case.c.params.spatial_order == 2:
+            _, gr, _, _ = restated.residual(case, prim, float(info[0]), with_extras=True)
+            assert np.array_equal(gr[:, :4].ravel(), ref_small[f"{key}/err_u_x"])
+            assert np.array_equal(gr[:, 4:].ravel(), ref_small[f"{key}/err_u_y"])
+    printed = ref_small[f"{key}/errors_printed"]
+    got = np.stack([e["L1"], e["L2"], e["Linf"]])
+    np.testing.assert_allclose(got, printed, rtol=6e-6, atol=0)
+
+
+@pytest.mark.skipif(not refdump.have_ref(), reason="compiled reference not built")
+@pytest.mark.parametrize("key", ["sine_euler_bj", "sine_ns_vk"])
+def test_oracle_source_term_bit_identical_to_live_reference(key):
+    spec = CASES.residual_cases()[key]
+    with tempfile.TemporaryDirectory() as tmp:
+        case, ini, files = CASES.load_case(spec, tmp)
+        prim = CASES.random_state(spec, tmp)
+        d = refdump.run_ref(ini, "residual", spec["time"], state=prim, eqn=spec["eqn"], files=files)
+        ut = restated.residual(case, prim, spec["time"])
+        # the same state without the source term: the source is what differs
+        case0 = cc.CaseData.from_text(ini.replace("calcSource = T", "calcSource = F"), tmp)
+        ut0 = restated.residual(case0, prim, spec["time"])
+    assert np.array_equal(ut.ravel(), d["u_t"])
+    assert np.abs(ut - ut0).max() > 1e-3
