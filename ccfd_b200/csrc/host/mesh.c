@@ -19,7 +19,9 @@
  *     (src/mesh.c:250-289, ghost barycentre mirrored across the face),
  *     createReconstructionInfo (src/mesh.c:80-114, least-squares weights from
  *     a Gram-Schmidt factorisation of the barycentre-to-barycentre vectors).
- * Periodic boundaries (connectPeriodicBC, src/mesh.c:172-244) are not built.
+ *   - periodic boundaries: connectPeriodicBC (src/mesh.c:172-244) joins the
+ *     matched boundary faces into interior faces before the least-squares
+ *     weights are formed.
  *
  * Also here: the Cartesian generator (src/mesh.c:385-486) and a gmsh 2.2
  * reader / writer (the format src/mesh.c:498-742 reads).
@@ -194,10 +196,6 @@ int ccfd_mesh_build(const double *nodes, long n_nodes,
 			st = CCFD_ERR_MESH; /* BC missing from the parameter file */
 			goto done;
 		}
-		if (bc_table[bi].type == CCFD_BC_PERIODIC) {
-			st = CCFD_ERR_UNSUPPORTED;
-			goto done;
-		}
 		hs[ns].node[0] = a;
 		hs[ns].node[1] = b;
 		hs[ns].key0 = a < b ? a : b;
@@ -328,6 +326,81 @@ int ccfd_mesh_build(const double *nodes, long n_nodes,
 		B->len = len;
 	}
 
+	/* connectPeriodicBC (src/mesh.c:172-244): in BC-list order, the ghost of
+	 * a periodic BC whose id ends in 1 is matched with the first ghost of
+	 * the periodic BC with the same id / 10 and an id ending in 2 whose face
+	 * midpoint is its own plus the BC's connection vector (within 1e-7 in
+	 * the 1-norm).  The two interior half-sides then face each other across
+	 * one interior face, owned by the first; the second one's face and both
+	 * ghosts leave the face and BC lists (src/mesh.c:1834-1841). */
+	long *gpair = malloc(sizeof(long) * (n_ghost + 1));  /* ghost -> face pair */
+	long *gside = malloc(sizeof(long) * (n_ghost + 1));  /* ghost -> its half-side */
+	long *gnew = malloc(sizeof(long) * (n_ghost + 1));   /* ghost -> BC-list index or -1 */
+	char *removed = calloc(n_sides + 1, 1);
+	char *matched = calloc(n_ghost + 1, 1);
+	long *face_new = malloc(sizeof(long) * (n_sides + 1));
+	if (!gpair || !gside || !gnew || !removed || !matched || !face_new) {
+		free(gpair); free(gside); free(gnew); free(removed); free(matched); free(face_new);
+		free(ghost_bary);
+		st = CCFD_ERR_NOMEM;
+		goto done;
+	}
+	for (long p = 0; p < n_sides; ++p)
+		if (hs[pair_b[p]].is_bc) {
+			gpair[hs[pair_b[p]].ghost] = p;
+			gside[hs[pair_b[p]].ghost] = pair_b[p];
+		}
+	for (long g = 0; g < n_ghost && st == CCFD_OK; ++g) {
+		const hside *G = &hs[gside[g]];
+		const ccfd_bc *bc = &bc_table[G->bc];
+		if (bc->type != CCFD_BC_PERIODIC || bc->id % 10 != 1)
+			continue;
+		double ax = G->gp[0] + ghost_bary[2 * g], ay = G->gp[1] + ghost_bary[2 * g + 1];
+		long hit = -1;
+		for (long g2 = 0; g2 < n_ghost && hit < 0; ++g2) {
+			const hside *S = &hs[gside[g2]];
+			const ccfd_bc *sb = &bc_table[S->bc];
+			if (sb->type != CCFD_BC_PERIODIC || sb->id % 10 != 2 || sb->id / 10 != bc->id / 10)
+				continue;
+			double sx = S->gp[0] + ghost_bary[2 * g2], sy = S->gp[1] + ghost_bary[2 * g2 + 1];
+			if ((fabs(ax + bc->connection[0] - sx) + fabs(ay + bc->connection[1] - sy)) <= 1e-7)
+				hit = g2;
+		}
+		if (hit < 0) {
+			st = CCFD_ERR_MESH; /* "No connection found" */
+			break;
+		}
+		long p = gpair[g], p2 = gpair[hit];
+		long ur = pair_a[p], target = pair_a[p2];
+		hs[ur].conn = target;
+		hs[target].conn = ur;
+		pair_b[p] = target;
+		removed[p2] = 1;
+		matched[hit] = 1;
+	}
+	/* a periodic ghost with an id ending in 2 that no ghost connected would
+	 * stay a ghost whose state is never set: rejected */
+	for (long g = 0; g < n_ghost && st == CCFD_OK; ++g) {
+		const ccfd_bc *bc = &bc_table[hs[gside[g]].bc];
+		if (bc->type == CCFD_BC_PERIODIC && bc->id % 10 != 1 && !matched[g])
+			st = CCFD_ERR_MESH;
+	}
+	if (st == CCFD_OK) {
+		long gn = 0;
+		for (long g = 0; g < n_ghost; ++g)
+			gnew[g] = bc_table[hs[gside[g]].bc].type == CCFD_BC_PERIODIC ? -1 : gn++;
+		long fn = 0;
+		for (long p = n_sides - 1; p >= 0; --p)  /* face list order */
+			face_new[p] = removed[p] ? -1 : fn++;
+	}
+	free(gpair);
+	free(gside);
+	free(matched);
+	if (st != CCFD_OK) {
+		free(gnew); free(removed); free(face_new); free(ghost_bary);
+		goto done;
+	}
+
 	/* createReconstructionInfo per element (src/mesh.c:80-114) */
 	for (long e = 0; e < n_elem; ++e) {
 		int t = etype[e];
@@ -355,7 +428,11 @@ int ccfd_mesh_build(const double *nodes, long n_nodes,
 	}
 
 	/* flatten, faces in side[] order = reverse pairing order */
-	long F = n_sides, N = n_elem, H = 3 * n_tria + 4 * n_quad, B = n_ghost;
+	long F = 0, N = n_elem, H = 3 * n_tria + 4 * n_quad, B = 0;
+	for (long p = 0; p < n_sides; ++p)
+		F += !removed[p];
+	for (long g = 0; g < n_ghost; ++g)
+		B += gnew[g] >= 0;
 	m->n_cells = N;
 	m->n_faces = F;
 	m->n_bc = B;
@@ -391,14 +468,16 @@ int ccfd_mesh_build(const double *nodes, long n_nodes,
 	    !m->bc_face || !m->bc_index || !m->bc_ghost_bary || !m->bc_x ||
 	    !hs_face_of || !hs_pos) {
 		free(hs_face_of); free(hs_pos); free(ghost_bary);
+		free(gnew); free(removed); free(face_new);
 		ccfd_mesh_free(m);
 		st = CCFD_ERR_NOMEM;
 		goto done;
 	}
 	for (long p = 0; p < n_sides; ++p) {
-		long f = n_sides - 1 - p;
-		hs_face_of[pair_a[p]] = f;
-		hs_face_of[pair_b[p]] = f;
+		if (removed[p])
+			continue;
+		hs_face_of[pair_a[p]] = face_new[p];
+		hs_face_of[pair_b[p]] = face_new[p];
 	}
 	long k = 0;
 	for (long e = 0; e < N; ++e) {
@@ -422,7 +501,7 @@ int ccfd_mesh_build(const double *nodes, long n_nodes,
 			hs_pos[s] = k;
 			m->hs_face[k] = hs_face_of[s];
 			m->hs_sign[k] = 0;
-			m->hs_nb[k] = C->is_bc ? -1 - C->ghost : C->elem;
+			m->hs_nb[k] = C->is_bc ? -1 - gnew[C->ghost] : C->elem;
 			m->hs_gp[2 * k] = S->gp[0];
 			m->hs_gp[2 * k + 1] = S->gp[1];
 			m->hs_w[2 * k] = S->w[0];
@@ -431,19 +510,21 @@ int ccfd_mesh_build(const double *nodes, long n_nodes,
 	}
 	m->hs_offset[N] = k;
 	for (long p = 0; p < n_sides; ++p) {
-		long f = n_sides - 1 - p;
+		if (removed[p])
+			continue;
+		long f = face_new[p];
 		hside *A = &hs[pair_a[p]], *Bs = &hs[pair_b[p]];
 		m->hs_sign[hs_pos[pair_a[p]]] = 1;
 		m->face_cells[2 * f] = A->elem;
 		m->face_hs[2 * f] = hs_pos[pair_a[p]];
 		if (Bs->is_bc) {
-			m->face_cells[2 * f + 1] = -1 - Bs->ghost;
+			long g = gnew[Bs->ghost];
+			m->face_cells[2 * f + 1] = -1 - g;
 			m->face_hs[2 * f + 1] = -1;
-			long g = Bs->ghost;
 			m->bc_face[g] = f;
 			m->bc_index[g] = Bs->bc;
-			m->bc_ghost_bary[2 * g] = ghost_bary[2 * g];
-			m->bc_ghost_bary[2 * g + 1] = ghost_bary[2 * g + 1];
+			m->bc_ghost_bary[2 * g] = ghost_bary[2 * Bs->ghost];
+			m->bc_ghost_bary[2 * g + 1] = ghost_bary[2 * Bs->ghost + 1];
 			m->ghost_gp[2 * g] = Bs->gp[0];
 			m->ghost_gp[2 * g + 1] = Bs->gp[1];
 			m->bc_x[2 * g] = A->gp[0] + bary[2 * A->elem];
@@ -465,6 +546,9 @@ int ccfd_mesh_build(const double *nodes, long n_nodes,
 	free(hs_face_of);
 	free(hs_pos);
 	free(ghost_bary);
+	free(gnew);
+	free(removed);
+	free(face_new);
 done:
 	free(hs); free(elem_first); free(etype); free(edom); free(enode);
 	free(bary); free(geo); free(idx); free(pair_a); free(pair_b);

@@ -168,12 +168,14 @@ outputFormat = 3
 """
 
 
-def sinewave_mesh(n: int, jitter: float = 0.15, seed: int = 20260005) -> RawMesh:
+def sinewave_mesh(n: int, jitter: float = 0.15, seed: int = 20260005,
+                  periodic: bool = False) -> RawMesh:
     """Square [-1,1]^2 for the manufactured sine-wave solution: n x n cells,
     interior nodes moved by U(-jitter, jitter) * h (PCG64, ``seed``) so that
     the quads are general quadrilaterals, every cell whose (i + j) is odd
     split along its diagonal into two triangles (both quadrature rules in one
-    mesh); all boundary faces 601 (exact solution)."""
+    mesh); all boundary faces 601 (exact solution), or with ``periodic``
+    the periodic pairs bottom 701 / top 702 and right 711 / left 712."""
     nodes = _grid_nodes(n, n, -1.0, 1.0, -1.0, 1.0)
     rng = np.random.Generator(np.random.PCG64(seed))
     h = 2.0 / n
@@ -189,23 +191,29 @@ def sinewave_mesh(n: int, jitter: float = 0.15, seed: int = 20260005) -> RawMesh
     t1 = np.stack([a[odd], b[odd], c[odd], np.ones_like(a[odd])], axis=1)
     t2 = np.stack([a[odd], c[odd], dd[odd], np.ones_like(a[odd])], axis=1)
     tria = np.concatenate([t1, t2])
+    codes = (701, 711, 702, 712) if periodic else (601, 601, 601, 601)
     bc = []
     for k in range(n):
-        bc.append((k, k + 1, 601))
-        bc.append(((k + 1) * (n + 1) - 1, (k + 2) * (n + 1) - 1, 601))
-        bc.append((n * (n + 1) + k, n * (n + 1) + k + 1, 601))
-        bc.append((k * (n + 1), (k + 1) * (n + 1), 601))
+        bc.append((k, k + 1, codes[0]))
+        bc.append(((k + 1) * (n + 1) - 1, (k + 2) * (n + 1) - 1, codes[1]))
+        bc.append((n * (n + 1) + k, n * (n + 1) + k + 1, codes[2]))
+        bc.append((k * (n + 1), (k + 1) * (n + 1), codes[3]))
     return RawMesh(nodes, tria=tria, quad=quad, bc=np.array(bc))
 
 
 def sinewave_ini(mesh_file: str | None, n: int = 16, order: int = 2, limiter: int = 1,
                  flux: int = 2, navier_stokes: bool = False, mu: float = 0.01,
                  source: bool = True, t_end: float = 0.05, cfl: float = 0.9,
-                 time_order: int = 2, rk_stages: int = 3) -> str:
+                 time_order: int = 2, rk_stages: int = 3, periodic: bool = False,
+                 implicit: bool = False) -> str:
     """Manufactured sine-wave solution (exact function 3 with source
     function 1), the convergence case of the reference's calc/sinewave.
     ``mesh_file`` None: the reference's own Cartesian n x n mesh on
-    [-1,1]^2."""
+    [-1,1]^2.  ``periodic``: periodic boundaries (pairs 701 / 702 bottom to
+    top, 711 / 712 right to left, as in calc/sinewave/sinewave_1D.ini)
+    instead of the exact solution.  ``implicit``: backward Euler with
+    JFNK-GMRES and LU-SGS (time-accurate, fixed CFL)."""
+    codes = ("701", "711", "702", "712") if periodic else ("601",) * 4
     if mesh_file is None:
         mesh = f"""meshType = 1
 nElemsX = {n}
@@ -213,21 +221,33 @@ nElemsY = {n}
 X0 = (/-1.0, -1.0/)
 Xmax = (/1.0, 1.0/)
 nBCsegments = (/1, 1, 1, 1/)
-meshBCtype = 601
-meshBCtype = 601
-meshBCtype = 601
-meshBCtype = 601
+meshBCtype = {codes[0]}
+meshBCtype = {codes[1]}
+meshBCtype = {codes[2]}
+meshBCtype = {codes[3]}
 """
     else:
         base = mesh_file[:-4] if mesh_file.endswith(".msh") else mesh_file
         mesh = f"meshType = 0\nmeshFormat = .msh\nmeshFile = {base}\n"
     ns = f"navierStokes = T\nmu = {mu}\nPr = 0.72\n" if navier_stokes else ""
     src = "calcSource = T\nsourceFunction = 1\n" if source else "calcSource = F\n"
+    if periodic:
+        bcs = """nBC = 4
+BCtype = 701
+connection = (/0.0, 2.0/)
+BCtype = 711
+connection = (/-2.0, 0.0/)
+BCtype = 702
+connection = (/0.0, -2.0/)
+BCtype = 712
+connection = (/2.0, 0.0/)
+"""
+    else:
+        bcs = "nBC = 1\nBCtype = 601\nBCexactFunc = 3\n"
+    imp = ("implicit = T\nprecond = T\nnKdim = 10\nnNewtonIter = 100\nepsNewton = 0.001\n"
+           "epsGMRES = 0.001\n") if implicit else ""
     return f"""! manufactured sine-wave solution
-{ns}{mesh}nBC = 1
-BCtype = 601
-BCexactFunc = 3
-icType = 2
+{ns}{mesh}{bcs}{imp}icType = 2
 exactFunc = 3
 {src}exactSolution = T
 fluxFunction = {flux}

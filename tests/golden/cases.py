@@ -115,6 +115,9 @@ def residual_cases() -> dict:
     cases["sine_ns_vk"] = {"mesh": ("sine", 12),
                            "ini": meshgen.sinewave_ini("sine", order=2, limiter=2, flux=5, navier_stokes=True),
                            "eqn": "navierstokes", "time": 0.37, "seed": 516}
+    cases["sine_periodic_vk"] = {"mesh": ("sine_periodic", 12),
+                                 "ini": meshgen.sinewave_ini("sine", order=2, limiter=2, flux=5, periodic=True),
+                                 "eqn": "euler", "time": 0.21, "seed": 517}
     cases["naca_ns_vk"] = {
         "mesh": ("naca", 32, 12),
         "ini": meshgen.airfoil_ini("naca", navier_stokes=True, reynolds=500.0, implicit=False,
@@ -140,6 +143,13 @@ def run_cases() -> dict:
         "sine_ns_run": {"mesh": ("sine", 16), "ini": meshgen.sinewave_ini("sine", order=2, limiter=1, flux=5,
                                                                           navier_stokes=True, t_end=0.2),
                         "eqn": "navierstokes", "steps": 0},
+        "sine_periodic_run": {"mesh": ("sine_periodic", 16),
+                              "ini": meshgen.sinewave_ini("sine", order=2, limiter=1, periodic=True, t_end=0.2),
+                              "eqn": "euler", "steps": 0},
+        "sine_periodic_ns_cart_run": {"mesh": None,
+                                      "ini": meshgen.sinewave_ini(None, n=16, order=2, limiter=2, flux=3,
+                                                                  navier_stokes=True, periodic=True, t_end=0.2),
+                                      "eqn": "navierstokes", "steps": 0},
         "sine_cart_o1_run": {"mesh": None, "ini": meshgen.sinewave_ini(None, n=16, order=1, time_order=1,
                                                                        rk_stages=1, t_end=0.2),
                              "eqn": "euler", "steps": 0},
@@ -165,6 +175,14 @@ def implicit_cases() -> dict:
         # slowly, so 1e-8 is out of reach of the dense reference Jacobian)
         "naca_euler_imp_pc_long": {"mesh": ("naca", 32, 12, 101), "ini": ini(steps=200), "eqn": "euler",
                                    "steps": 200},
+        # time-accurate implicit steps of the sine wave on a periodic mesh
+        # (with the source term or the exact-solution boundary the
+        # reference's Newton iteration stalls at a relative residual of
+        # 0.5-0.9 in its first step, at CFL 0.5 to 4)
+        "sine_periodic_imp": {"mesh": ("sine_periodic", 8),
+                              "ini": meshgen.sinewave_ini("sine", order=2, limiter=2, periodic=True, implicit=True,
+                                                          cfl=4.0, t_end=1.0, source=False),
+                              "eqn": "euler", "steps": 5},
     }
 
 
@@ -176,6 +194,8 @@ def make_mesh(spec):
         return "dmr", meshgen.dmr_mesh(kind[1], kind[2])
     if kind[0] == "sine":
         return "sine", meshgen.sinewave_mesh(kind[1])
+    if kind[0] == "sine_periodic":
+        return "sine", meshgen.sinewave_mesh(kind[1], periodic=True)
     if kind[0] == "naca":
         wall = kind[3] if len(kind) > 3 else 201
         return "naca", meshgen.naca_ogrid(0.0, 0.0, 0.12, kind[1], kind[2], r_far=5.0, h0=1e-2,

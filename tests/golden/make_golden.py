@@ -80,9 +80,9 @@ def ref_small(only: str | None = None) -> dict:
             arrays[f"{key}/pvar"] = d["pvar"]
             arrays[f"{key}/info"] = d["run_info"]
             arrays[f"{key}/history"] = d["history"]
-            arrays[f"{key}/clcd"] = d["clcd"]
-            arrays[f"{key}/cp_pressure"] = d["cp_pressure"]
-            arrays[f"{key}/cp_suction"] = d["cp_suction"]
+            for name in ("clcd", "cp_pressure", "cp_suction"):
+                if name in d:  # cases with calcWing
+                    arrays[f"{key}/{name}"] = d[name]
     return arrays
 
 

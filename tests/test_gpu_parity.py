@@ -150,7 +150,8 @@ def test_nonfinite_time_step_is_reported_not_fatal():
     s.close()
 
 
-SINE_RUNS = ["sine_euler_run", "sine_ns_run", "sine_cart_o1_run"]
+SINE_RUNS = ["sine_euler_run", "sine_ns_run", "sine_cart_o1_run", "sine_periodic_run",
+             "sine_periodic_ns_cart_run"]
 
 
 @pytest.mark.parametrize("key", SINE_RUNS)

@@ -64,14 +64,27 @@ def test_oracle_bit_identical_to_live_reference(key):
 
 
 @pytest.mark.skipif(not refdump.have_ref(), reason="compiled reference not built")
-def test_mesh_builder_bit_identical_to_reference():
+@pytest.mark.parametrize("kind", ["dmr", "periodic_gmsh", "periodic_cartesian"])
+def test_mesh_builder_bit_identical_to_reference(kind):
     from ccfd_b200 import meshgen
     with tempfile.TemporaryDirectory() as tmp:
-        meshgen.dmr_mesh(30, 8, seed=5).write_gmsh(os.path.join(tmp, "dmr.msh"))
-        ini = meshgen.dmr_ini("dmr")
+        files = {}
+        if kind == "dmr":
+            meshgen.dmr_mesh(30, 8, seed=5).write_gmsh(os.path.join(tmp, "dmr.msh"))
+            ini = meshgen.dmr_ini("dmr")
+            files = {"dmr.msh": os.path.join(tmp, "dmr.msh")}
+        elif kind == "periodic_gmsh":
+            # connectPeriodicBC: matched boundary faces become interior faces
+            meshgen.sinewave_mesh(7, periodic=True).write_gmsh(os.path.join(tmp, "sine.msh"))
+            ini = meshgen.sinewave_ini("sine", periodic=True)
+            files = {"sine.msh": os.path.join(tmp, "sine.msh")}
+        else:
+            ini = meshgen.sinewave_ini(None, n=9, periodic=True)
         case = cc.CaseData.from_text(ini, tmp)
-        d = refdump.run_ref(ini, "mesh", files={"dmr.msh": os.path.join(tmp, "dmr.msh")})
+        d = refdump.run_ref(ini, "mesh", files=files)
     M = case.mesh()
+    if kind != "dmr":
+        assert M["n_bc"] == 0 and M["n_faces"] == len(d["face_sides"]) // 4
     hs = d["hs_geo"].reshape(-1, 12)
     fs = d["face_sides"].reshape(-1, 4)
     fg = d["face_geo"].reshape(-1, 3)
@@ -85,7 +98,8 @@ def test_mesh_builder_bit_identical_to_reference():
     assert np.array_equal(case.prim0().ravel(), d["pvar"])
 
 
-SINE_RUNS = ["sine_euler_run", "sine_ns_run", "sine_cart_o1_run"]
+SINE_RUNS = ["sine_euler_run", "sine_ns_run", "sine_cart_o1_run", "sine_periodic_run",
+             "sine_periodic_ns_cart_run"]
 
 
 @pytest.mark.parametrize("key", SINE_RUNS)
