@@ -140,13 +140,15 @@ class CaseData:
     def file_name(self) -> str:
         return self.c.file_name.decode()
 
-    def write_output(self, prim: np.ndarray, time: float, iteration: int) -> str:
-        """Write the state in the reference's output format (CSV) into the
-        current directory; returns the file name."""
+    def write_output(self, prim: np.ndarray, time: float, iteration: int, exact: bool = False) -> str:
+        """Write the state in the reference's output format (CSV or curve)
+        into the current directory; ``exact``: the exact-solution file
+        (<fileName>_ex_...) of a state from Solver.exact_state.  Returns the
+        file name."""
         p = np.ascontiguousarray(prim, dtype=np.float64).reshape(self.n_cells, 4)
         buf = C.create_string_buffer(600)
-        _check(N.lib.ccfd_write_output(self._ptr, _dptr(p), float(time), int(iteration), buf, 600),
-               "ccfd_write_output")
+        fn = N.lib.ccfd_write_exact_output if exact else N.lib.ccfd_write_output
+        _check(fn(self._ptr, _dptr(p), float(time), int(iteration), buf, 600), "ccfd_write_output")
         return buf.value.decode()
 
 
@@ -272,6 +274,15 @@ class Solver:
         e = np.empty(12)
         _check(N.lib.ccfd_errors(self._ctx, int(which), _dptr(e)), "ccfd_errors")
         return {"L1": e[0:4].copy(), "L2": e[4:8].copy(), "Linf": e[8:12].copy()}
+
+    def exact_state(self, time: float | None = None, exact_func: int | None = None) -> np.ndarray:
+        """Exact function at the cell barycentres (ccfd_exact_state), at the
+        solver's current time by default; [N, 4] primitive."""
+        which = self.case.c.exact_func if exact_func is None else exact_func
+        t = self.time if time is None else time
+        out = np.empty((self.n, 4))
+        _check(N.lib.ccfd_exact_state(self._ctx, int(which), float(t), _dptr(out)), "ccfd_exact_state")
+        return out
 
     def clcd(self):
         cl, cd = C.c_double(), C.c_double()

@@ -118,6 +118,8 @@ def _load():
         "ccfd_wall_cp": (c_int, [C.c_void_p, P(c_double), P(c_double), P(c_double), P(c_int), P(c_int)]),
         "ccfd_write_cp": (c_int, [C.c_void_p, C.c_char_p]),
         "ccfd_errors": (c_int, [C.c_void_p, c_int, P(c_double)]),
+        "ccfd_exact_state": (c_int, [C.c_void_p, c_int, c_double, P(c_double)]),
+        "ccfd_write_exact_output": (c_int, [C.c_void_p, P(c_double), c_double, c_long, C.c_char_p, C.c_size_t]),
         "ccfd_write_output": (c_int, [C.c_void_p, P(c_double), c_double, c_long, C.c_char_p, C.c_size_t]),
         "ccfd_batch_create": (c_int, [c_int, P(C.c_void_p)]),
         "ccfd_batch_destroy": (None, [C.c_void_p]),

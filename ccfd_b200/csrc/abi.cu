@@ -673,6 +673,28 @@ extern "C" int ccfd_errors(ccfd_ctx* ctx, int exact_func, double out[12]) {
     return check_flags(ctx);
 }
 
+extern "C" int ccfd_exact_state(ccfd_ctx* ctx, int exact_func, double time, double* prim_out) {
+    if (!ctx || !prim_out || !ctx->uploaded || exact_func < 1 || exact_func > 6) return CCFD_ERR_ARG;
+    CK(cudaSetDevice(ctx->device));
+    const long N = ctx->N;
+    double4* out = nullptr;
+    CK(cudaMallocAsync((void**)&out, sizeof(double4) * N, ctx->stream));
+    launch_exact_state((int)N, ctx->cell_xq, ctx->phys_g, exact_func, time, out, ctx->flags, ctx->stream);
+    cudaError_t le = cudaGetLastError();
+    std::vector<double4> h(N);
+    cudaError_t ce = le == cudaSuccess ? cudaMemcpyAsync(h.data(), out, sizeof(double4) * N,
+                                                         cudaMemcpyDeviceToHost, ctx->stream)
+                                       : le;
+    cudaFreeAsync(out, ctx->stream);
+    CK(ce);
+    CK(cudaStreamSynchronize(ctx->stream));
+    for (long d = 0; d < N; ++d) {
+        double* s = &prim_out[4 * ctx->cell_of_dev[d]];
+        s[0] = h[d].x; s[1] = h[d].y; s[2] = h[d].z; s[3] = h[d].w;
+    }
+    return check_flags(ctx);
+}
+
 // Autotuner of the stage kernel's launch shape: cells per tile (which sets
 // the CTA's faces and gradient cells per thread) and the cell ordering
 // (Hilbert curve or the reference's numbering).  Every candidate is uploaded

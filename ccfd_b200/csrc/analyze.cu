@@ -89,6 +89,26 @@ __global__ void __launch_bounds__(kErrThreads)
     }
 }
 
+// exactFunc at the cell barycentres (the exact-solution output of
+// csvOutput / curveOutput, src/output.c:59-71)
+__global__ void __launch_bounds__(kErrThreads)
+    k_exact_state(int n, const double4* __restrict__ xq, const Phys* __restrict__ Pg, int which, double time,
+                  double4* __restrict__ out, unsigned* flags) {
+    const int d = blockIdx.x * blockDim.x + threadIdx.x;
+    if (d >= n) return;
+    const double4 c = xq[d];
+    const double x[2] = {c.x, c.y};
+    double pv[4];
+    exact_func(*Pg, which, x, time, pv, flags);
+    out[d] = make_double4(pv[0], pv[1], pv[2], pv[3]);
+}
+
+void launch_exact_state(int n, const double4* xq, const Phys* phys_g, int which, double time, double4* out,
+                        unsigned* flags, cudaStream_t st) {
+    k_exact_state<<<(n + kErrThreads - 1) / kErrThreads, kErrThreads, 0, st>>>(n, xq, phys_g, which, time, out,
+                                                                              flags);
+}
+
 int error_blocks(int n_cells) {
     int b = (n_cells + kErrThreads - 1) / kErrThreads;
     return b < 1 ? 1 : (b > 1184 ? 1184 : b);

@@ -95,6 +95,14 @@ int main(int argc, char **argv)
 			printf("wrote %s\n", path);
 		else if (st != CCFD_ERR_UNSUPPORTED)
 			return fail("output", st);
+		if (st == CCFD_OK && c->params.exact_solution && c->exact_func > 0) {
+			/* the exact-solution file of dataOutput (src/output.c:375-397) */
+			if ((st = ccfd_exact_state(ctx, c->exact_func, rep.t, prim)))
+				return fail("exact state", st);
+			if ((st = ccfd_write_exact_output(c, prim, rep.t, rep.iterations, path, sizeof(path))))
+				return fail("output", st);
+			printf("wrote %s\n", path);
+		}
 		free(prim);
 	}
 	ccfd_destroy(ctx);

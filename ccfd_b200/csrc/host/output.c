@@ -1,13 +1,16 @@
 /*
  * Solution output in the reference's formats (src/output.c).
  *
- * Only the tabular CSV format (outputFormat = 3, csvOutput,
- * src/output.c:53-112) is written: cell barycentre x, density, x-velocity
- * and pressure, rows sorted by x with a stable sort (the reference's bubble
- * sort is stable too), "%15.9f" columns.  File names follow dataOutput
- * (src/output.c:348-353): <fileName>_<iter %09ld>.csv for stationary runs,
- * <fileName>_<time %015.7f>.csv otherwise.  CGNS and curve output are not
- * built (CCFD_ERR_UNSUPPORTED).
+ * The tabular formats are written: CSV (outputFormat = 3, csvOutput,
+ * src/output.c:53-112: cell barycentre x, density, x-velocity and pressure
+ * per row) and curve (outputFormat = 2, curveOutput, src/output.c:253-327:
+ * the x-density, x-velocity and x-pressure series one after another), rows
+ * sorted by x with a stable sort (the reference's bubble sort is stable
+ * too), "%15.9f" columns.  File names follow dataOutput (src/output.c:
+ * 334-398): <fileName>_<iter %09ld> for stationary runs, <fileName>_<time
+ * %015.7f> otherwise, and <fileName>_ex_... for the exact solution.  CGNS
+ * (outputFormat = 1) needs the CGNS library and is not built
+ * (CCFD_ERR_UNSUPPORTED).
  */
 #include <stdio.h>
 #include <stdlib.h>
@@ -34,18 +37,21 @@ static void merge_sort_by_x(long *idx, long *tmp, const double *x, long n)
 	}
 }
 
-int ccfd_write_output(const ccfd_case *c, const double *prim, double time, long iter,
-		      char *path, size_t path_len)
+static int write_tabular(const ccfd_case *c, const double *prim, double time, long iter,
+			 int exact, char *path, size_t path_len)
 {
 	if (!c || !prim)
 		return CCFD_ERR_ARG;
-	if (c->output_format != 3)
+	const int fmt = c->output_format;
+	if (fmt != 2 && fmt != 3)
 		return CCFD_ERR_UNSUPPORTED;
+	const char *ext = fmt == 2 ? "curve" : "csv";
+	const char *tag = exact ? "_ex" : "";
 	char name[600];
 	if (c->params.stationary)
-		snprintf(name, sizeof(name), "%s_%09ld.csv", c->file_name, iter);
+		snprintf(name, sizeof(name), "%s%s_%09ld.%s", c->file_name, tag, iter, ext);
 	else
-		snprintf(name, sizeof(name), "%s_%015.7f.csv", c->file_name, time);
+		snprintf(name, sizeof(name), "%s%s_%015.7f.%s", c->file_name, tag, time, ext);
 	if (path && path_len) {
 		strncpy(path, name, path_len - 1);
 		path[path_len - 1] = '\0';
@@ -72,14 +78,39 @@ int ccfd_write_output(const ccfd_case *c, const double *prim, double time, long 
 		free(x);
 		return CCFD_ERR_ARG;
 	}
-	fprintf(f, "CoordinateX, Density, Velocity, Pressure\n");
-	for (long k = 0; k < n; ++k) {
-		long i = idx[k];
-		fprintf(f, "%15.9f,%15.9f,%15.9f,%15.9f\n", x[i], prim[4 * i], prim[4 * i + 1], prim[4 * i + 3]);
+	if (fmt == 3) {
+		fprintf(f, "CoordinateX, Density, Velocity, Pressure\n");
+		for (long k = 0; k < n; ++k) {
+			long i = idx[k];
+			fprintf(f, "%15.9f,%15.9f,%15.9f,%15.9f\n", x[i], prim[4 * i], prim[4 * i + 1],
+				prim[4 * i + 3]);
+		}
+	} else {
+		static const char *title[3] = {"#Density\n", "\n#Velocity\n", "\n#Pressure\n"};
+		static const int var[3] = {0, 1, 3};
+		for (int s = 0; s < 3; ++s) {
+			fputs(title[s], f);
+			for (long k = 0; k < n; ++k) {
+				long i = idx[k];
+				fprintf(f, "%15.9f,%15.9f\n", x[i], prim[4 * i + var[s]]);
+			}
+		}
 	}
 	fclose(f);
 	free(idx);
 	free(tmp);
 	free(x);
 	return CCFD_OK;
+}
+
+int ccfd_write_output(const ccfd_case *c, const double *prim, double time, long iter,
+		      char *path, size_t path_len)
+{
+	return write_tabular(c, prim, time, iter, 0, path, path_len);
+}
+
+int ccfd_write_exact_output(const ccfd_case *c, const double *prim_exact, double time, long iter,
+			    char *path, size_t path_len)
+{
+	return write_tabular(c, prim_exact, time, iter, 1, path, path_len);
 }

@@ -88,6 +88,8 @@ void launch_dt(const DevMesh& m, const Phys& P, const Ctrl* ctrl, const StepPara
 void launch_step_begin(Ctrl* ctrl, const StepParams& sp, const double2* partial,
                        const int* bad_partial, int nb, cudaStream_t st);
 int error_blocks(int n_cells);
+void launch_exact_state(int n, const double4* xq, const Phys* phys_g, int which, double time, double4* out,
+                        unsigned* flags, cudaStream_t st);
 void launch_errors(const DevMesh& m, const double4* xq, const double4* prim, const double4* grad,
                    const Phys* phys_g, int which, double time, double* partial, unsigned* flags,
                    cudaStream_t st);

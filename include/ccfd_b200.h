@@ -38,7 +38,7 @@ enum ccfd_status {
 	CCFD_ERR_MESH = 10,        /* mesh read / connectivity error, mesh.c   */
 	CCFD_ERR_STATE = 11,       /* non-finite state or residual             */
 	CCFD_ERR_BUDGET = 12,      /* request exceeds the device-memory budget */
-	CCFD_ERR_UNSUPPORTED = 13, /* option not built (e.g. periodic BC)      */
+	CCFD_ERR_UNSUPPORTED = 13, /* option not built (e.g. CGNS output)      */
 	CCFD_ERR_NOT_CONVERGED = 14, /* maxIter reached, timeDiscretization.c:737-750 */
 	CCFD_ERR_GMRES = 15,         /* GMRES breakdown (zero Hessenberg pivot)  */
 	CCFD_ERR_BUSY = 16           /* context is being stepped by a batch      */
@@ -114,7 +114,7 @@ typedef struct ccfd_bc {
 	int exact_func;        /* BCexactFunc for EXACTSOL                      */
 	int is_adiabatic;      /* adiabaticWall (parsed, unused like the reference) */
 	double pvar[4];        /* rho, vx, vy, p (inflow / characteristic / pressure) */
-	double connection[2];  /* periodic offset (periodic BCs are not built)  */
+	double connection[2];  /* periodic BC: offset to the paired boundary    */
 } ccfd_bc;
 
 /* exact-function / initial-condition data used on the device by EXACTSOL
@@ -315,13 +315,23 @@ int ccfd_autotune(ccfd_ctx *ctx, const ccfd_mesh *m, const ccfd_bc *bc, int n_bc
 		  const ccfd_exact *ex, const double *prim, int *tile_cells, int *reorder,
 		  double *ms_per_residual);
 
-/* Final-solution output in the reference's format (dataOutput / csvOutput,
- * src/output.c:53-112, 348-372): only outputFormat = 3 (CSV) is written,
- * named <fileName>_<iter %09ld>.csv (stationary) or <fileName>_<time
- * %015.7f>.csv; prim is [n_cells][4] in reference order; the file name is
- * returned in path (may be NULL).  CCFD_ERR_UNSUPPORTED for CGNS / curve. */
+/* Final-solution output in the reference's format (dataOutput, csvOutput,
+ * curveOutput, src/output.c:53-112, 253-398): outputFormat = 3 (CSV) or 2
+ * (curve), named <fileName>_<iter %09ld>.<ext> (stationary) or
+ * <fileName>_<time %015.7f>.<ext>; prim is [n_cells][4] in reference order;
+ * the file name is returned in path (may be NULL).  CCFD_ERR_UNSUPPORTED for
+ * CGNS. */
 int ccfd_write_output(const ccfd_case *c, const double *prim, double time, long iter,
 		      char *path, size_t path_len);
+/* The exact-solution file that dataOutput adds with exactSolution = T
+ * (<fileName>_ex_...), from the exact state of ccfd_exact_state. */
+int ccfd_write_exact_output(const ccfd_case *c, const double *prim_exact, double time, long iter,
+			    char *path, size_t path_len);
+/* Exact function exact_func (exactFunc, src/exactFunction.c:35-183) at the
+ * cell barycentres at time `time`, evaluated on the device: [n_cells][4]
+ * primitive state in reference order (what csvOutput / curveOutput write
+ * for the exact solution). */
+int ccfd_exact_state(ccfd_ctx *ctx, int exact_func, double time, double *prim_out);
 
 /* ------------------------------------------------------------- batching
  * Many contexts stepped together on one GPU (no counterpart in the

@@ -20,7 +20,9 @@
  *                        when the case has an exact solution
  *
  * The initialisation order mirrors main() (src/main.c:53-118).  Output format
- * is forced to CSV so that the CGNS stand-in is never reached.
+ * CGNS is replaced by CSV so that the CGNS stand-in is never reached; with
+ * CCFD_REF_OUTPUT set in the environment, run / coef end with dataOutput
+ * (solution file, and exact-solution file with exactSolution = T).
  *
  * Dump format: magic "CCFDDMP1", then records of
  *   char name[32]; int32 type (0 = f64, 1 = i64); int32 pad; int64 count; data
@@ -241,7 +243,8 @@ int main(int argc, char *argv[])
 	startTime = 0.0;
 
 	initOutput();
-	iVisuProg = CSV;
+	if (iVisuProg != CURVE)
+		iVisuProg = CSV;
 	initEquation();
 	initBoundary();
 	initMesh();
@@ -346,6 +349,12 @@ int main(int argc, char *argv[])
 			}
 		}
 		double tEnd = omp_get_wtime();
+		if (getenv("CCFD_REF_OUTPUT")) {
+			/* the final solution file (and the exact-solution file)
+			 * of dataOutput (src/output.c:334-398) */
+			dataOutput(t, nhist);
+			finalizeDataOutput();
+		}
 		dump_state();
 		if (hasExactSolution) {
 			/* the error analysis that ends timeDisc (src/analyze.c:

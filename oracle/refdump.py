@@ -49,13 +49,16 @@ def read_dump(path: str) -> dict:
 def run_ref(ini_text: str, mode: str, *args, eqn: str = "euler",
             fast: bool = False, state: np.ndarray | None = None,
             threads: int | None = None, workdir: str | None = None,
-            files: dict | None = None, timeout: float = 3600.0) -> dict:
+            files: dict | None = None, timeout: float = 3600.0,
+            output: bool = False) -> dict:
     """Run the reference driver on an .ini text in a scratch directory.
 
     ``state`` (N x 4 primitive states in reference cell order) replaces the
     initial condition.  ``files`` maps names to paths linked into the scratch
     directory (the reference's parser drops '/' from values, so a mesh file
-    must sit in its working directory).  Returns the parsed dump.
+    must sit in its working directory).  ``output``: the run ends with the
+    reference's dataOutput; its files come back as ``out["output_files"]``
+    ({name: text}).  Returns the parsed dump.
     """
     exe = ref_binary(eqn, fast)
     if not os.access(exe, os.X_OK):
@@ -78,6 +81,8 @@ def run_ref(ini_text: str, mode: str, *args, eqn: str = "euler",
         if threads is not None:
             env["OMP_NUM_THREADS"] = str(threads)
         env.setdefault("OMP_NUM_THREADS", "1")
+        if output:
+            env["CCFD_REF_OUTPUT"] = "1"
         r = subprocess.run(argv, cwd=tmp, env=env, capture_output=True,
                            text=True, timeout=timeout)
         if r.returncode != 0:
@@ -91,6 +96,12 @@ def run_ref(ini_text: str, mode: str, *args, eqn: str = "euler",
             out["errors_printed"] = np.array(rows[-3:], dtype=np.float64)
         # pressure-coefficient files written by calcCoef (src/analyze.c:
         # 302-367), as arrays of (x, y, phi, cp) rows
+        if output:
+            out["output_files"] = {}
+            for name in sorted(os.listdir(tmp)):
+                if name.endswith((".csv", ".curve")) and "_CP_" not in name:
+                    with open(os.path.join(tmp, name)) as f:
+                        out["output_files"][name] = f.read()
         for name in sorted(os.listdir(tmp)):
             if "_CP_" in name and name.endswith(".csv"):
                 side = "cp_pressure" if "pressureSide" in name else "cp_suction"

@@ -237,3 +237,20 @@ def load_case(spec, tmpdir):
     import ccfd_b200 as cc
     ini, files = materialise(spec, tmpdir)
     return cc.CaseData.from_text(ini, tmpdir), ini, files
+
+
+def output_cases() -> dict:
+    """Final-solution files of dataOutput (src/output.c:334-398) in the
+    formats that are built: curve and CSV, transient (time in the name) and
+    stationary (iteration in the name), with the exact-solution file."""
+    sod = meshgen.sod_ini(50, 2, t_end=0.1)
+    return {
+        "out_sod_curve": {"ini": sod.replace("outputFormat = 3", "outputFormat = 2\nexactSolution = T"),
+                          "eqn": "euler"},
+        "out_sod_stationary_csv": {"ini": sod.replace("stationary = F", "stationary = T")
+                                   .replace("maxIter = 1000000", "maxIter = 12")
+                                   .replace("outputFormat = 3", "outputFormat = 3\nexactSolution = T"),
+                                   "eqn": "euler"},
+        "out_sine_periodic_csv": {"ini": meshgen.sinewave_ini(None, n=8, periodic=True, t_end=0.1),
+                                  "eqn": "euler"},
+    }

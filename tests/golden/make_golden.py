@@ -13,6 +13,8 @@ Outputs (small, committed):
                     synthetic cases: residuals at seeded random states for
                     every flux function and limiter, every boundary type,
                     Navier-Stokes, and short explicit runs
+  ref_output.json   the compiled reference's own solution files (curve /
+                    CSV, with the exact-solution file) of small runs
 The synthetic cases themselves are described by CASES below and rebuilt by
 the tests from the same generators and seeds.
 """
@@ -86,6 +88,18 @@ def ref_small(only: str | None = None) -> dict:
     return arrays
 
 
+def ref_output() -> dict:
+    """The reference's own output files (and final state) of the output
+    cases."""
+    out = {}
+    for key, spec in CASES.output_cases().items():
+        d = refdump.run_ref(spec["ini"], "run", 0, eqn=spec["eqn"], output=True)
+        files = {k: v for k, v in d["output_files"].items() if not k.endswith("_analysis.csv")}
+        out[key] = {"files": files, "pvar": d["pvar"].tolist(),
+                    "t": float(d["run_info"][0]), "iterations": int(d["run_info"][1])}
+    return out
+
+
 def main() -> int:
     ap = argparse.ArgumentParser()
     ap.add_argument("--ref", default="/root/reference")
@@ -97,6 +111,11 @@ def main() -> int:
         print("compiled reference missing: run `make -C oracle` first", file=sys.stderr)
         return 1
     npz = os.path.join(HERE, "ref_small.npz")
+    if a.only == "out":
+        with open(os.path.join(HERE, "ref_output.json"), "w") as f:
+            json.dump(ref_output(), f)
+        print("wrote ref_output.json")
+        return 0
     if a.only:
         with np.load(npz) as old:
             arrays = {k: old[k] for k in old.files}
@@ -107,7 +126,9 @@ def main() -> int:
     with open(os.path.join(HERE, "sod_check.json"), "w") as f:
         json.dump(sod_check(a.ref), f)
     np.savez_compressed(npz, **ref_small())
-    print("wrote sod_check.json, ref_small.npz")
+    with open(os.path.join(HERE, "ref_output.json"), "w") as f:
+        json.dump(ref_output(), f)
+    print("wrote sod_check.json, ref_small.npz, ref_output.json")
     return 0
 
 

@@ -1,5 +1,5 @@
-"""Solution output in the reference's CSV format and the command-line
-driver.
+"""Solution output in the reference's CSV and curve formats (with the
+exact-solution files) and the command-line driver.
 
 The writer is checked on the CPU with the oracle's state of the reference's
 own regression cases (check/*.ini): the written file must reproduce the
@@ -7,6 +7,7 @@ golden CSV within the reference's tolerance (Frobenius norm of the
 differences of x, density and velocity <= 1e-5, check/check.py:33-42).  The
 driver (ccfd_run) runs the same cases on the GPU.
 """
+import json
 import os
 import re
 import subprocess
@@ -17,6 +18,7 @@ import pytest
 
 import ccfd_b200 as cc
 from oracle import restated
+from tests.golden import cases as CASES
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 DRIVER = os.path.join(ROOT, "ccfd_b200", "lib", "ccfd_run")
@@ -45,6 +47,7 @@ def test_csv_writer_reproduces_golden_output(sod_check):
 
 
 def test_writer_refuses_formats_it_does_not_build(sod_check):
+    # CGNS (outputFormat = 1) needs the CGNS library
     g = sod_check["sod_FF02"]
     ini = re.sub(r"(?im)^(\s*outputformat\s*=\s*)3", r"\g<1>1", g["ini"])
     case = cc.CaseData.from_text(ini)
@@ -71,3 +74,54 @@ def test_driver_runs_regression_case(sod_check, name):
         assert r.returncode == 0, r.stdout + r.stderr
         assert f"wrote {g['target']}" in r.stdout
         assert _frobenius_vs_golden(os.path.join(tmp, g["target"]), g) < 1e-5
+
+
+@pytest.fixture(scope="module")
+def ref_output():
+    with open(os.path.join(ROOT, "tests", "golden", "ref_output.json")) as f:
+        return json.load(f)
+
+
+def _numbers(text):
+    return np.array([float(v) for v in re.findall(r"-?\d+\.\d+", text)])
+
+
+@pytest.mark.parametrize("key", sorted(CASES.output_cases()))
+def test_writer_reproduces_reference_files_from_its_state(ref_output, key):
+    # the reference's final state through the writer: the solution file must
+    # be the reference's, byte for byte (same name, header, sort, format)
+    g = ref_output[key]
+    case = cc.CaseData.from_text(CASES.output_cases()[key]["ini"])
+    prim = np.array(g["pvar"]).reshape(-1, 4)
+    cwd = os.getcwd()
+    with tempfile.TemporaryDirectory() as tmp:
+        os.chdir(tmp)
+        try:
+            path = case.write_output(prim, g["t"], g["iterations"])
+            with open(path) as f:
+                text = f.read()
+        finally:
+            os.chdir(cwd)
+    assert path in g["files"]
+    assert text == g["files"][path]
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("key", sorted(CASES.output_cases()))
+def test_driver_writes_reference_solution_and_exact_files(ref_output, key):
+    # ccfd_run on the same .ini: the same files (flow solution and exact
+    # solution) as the reference's dataOutput, equal to their printed digits
+    g = ref_output[key]
+    with tempfile.TemporaryDirectory() as tmp:
+        with open(os.path.join(tmp, "case.ini"), "w") as f:
+            f.write(CASES.output_cases()[key]["ini"])
+        r = subprocess.run([DRIVER, "case.ini"], cwd=tmp, capture_output=True, text=True, timeout=300)
+        assert r.returncode == 0, r.stdout + r.stderr
+        written = sorted(n for n in os.listdir(tmp) if n.endswith((".csv", ".curve")))
+        assert written == sorted(g["files"])
+        for name in written:
+            with open(os.path.join(tmp, name)) as f:
+                text = f.read()
+            want = g["files"][name]
+            assert text.splitlines()[0] == want.splitlines()[0]
+            np.testing.assert_allclose(_numbers(text), _numbers(want), rtol=0, atol=2.1e-9)
