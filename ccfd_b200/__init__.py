@@ -140,6 +140,19 @@ class CaseData:
     def file_name(self) -> str:
         return self.c.file_name.decode()
 
+    def record_points(self) -> tuple[np.ndarray, np.ndarray]:
+        """(pointCoords [n, 2], containing cell [n]) of the case."""
+        c = self.c
+        xy = np.array([[c.record_xy[k][0], c.record_xy[k][1]] for k in range(c.n_record)]).reshape(-1, 2)
+        return xy, np.array([c.record_cell[k] for k in range(c.n_record)], dtype=np.int64)
+
+    def write_history(self, rows: np.ndarray, append: bool = False) -> None:
+        """analyze's files (residual file, record points) from history rows,
+        into the current directory."""
+        r = np.ascontiguousarray(rows, dtype=np.float64)
+        _check(N.lib.ccfd_write_history(self._ptr, _dptr(r), r.shape[0], r.shape[1] if r.ndim == 2 else 0,
+                                        int(append)), "ccfd_write_history")
+
     def write_output(self, prim: np.ndarray, time: float, iteration: int, exact: bool = False) -> str:
         """Write the state in the reference's output format (CSV or curve)
         into the current directory; ``exact``: the exact-solution file
@@ -274,6 +287,28 @@ class Solver:
         e = np.empty(12)
         _check(N.lib.ccfd_errors(self._ctx, int(which), _dptr(e)), "ccfd_errors")
         return {"L1": e[0:4].copy(), "L2": e[4:8].copy(), "Linf": e[8:12].copy()}
+
+    def set_history(self, capacity: int = 4096, record_cells=None) -> None:
+        """Record one row per step from now on (ccfd_set_history): residuals,
+        CL / CD and the state of the record cells (default: the case's
+        record points).  capacity <= 0 switches it off."""
+        if record_cells is None:
+            c = self.case.c
+            record_cells = [c.record_cell[k] for k in range(c.n_record)]
+        cells = np.ascontiguousarray(record_cells, dtype=np.int64)
+        _check(N.lib.ccfd_set_history(self._ctx, int(capacity), _lptr(cells), len(cells)),
+               "ccfd_set_history")
+
+    def history(self) -> np.ndarray:
+        """Rows recorded since the last call, [n, 11 + 4 * n_record]:
+        iteration, t, dt, residuals [6], CL, CD, (rho, vx, vy, p) per record
+        cell."""
+        n, w = C.c_long(), C.c_int()
+        _check(N.lib.ccfd_get_history(self._ctx, None, 0, C.byref(n), C.byref(w)), "ccfd_get_history")
+        out = np.empty((n.value, w.value))
+        _check(N.lib.ccfd_get_history(self._ctx, _dptr(out), n.value, C.byref(n), C.byref(w)),
+               "ccfd_get_history")
+        return out[:n.value]
 
     def exact_state(self, time: float | None = None, exact_func: int | None = None) -> np.ndarray:
         """Exact function at the cell barycentres (ccfd_exact_state), at the

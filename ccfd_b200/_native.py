@@ -16,6 +16,7 @@ P = C.POINTER
 
 CCFD_OK, CCFD_ERR_ARG = 0, 1
 NOALLOC_MAX_CELLS = 1 << 20  # CCFD_NOALLOC_MAX_CELLS
+MAX_RECORD = 64  # CCFD_MAX_RECORD
 
 
 class Params(C.Structure):
@@ -56,7 +57,8 @@ class Mesh(C.Structure):
         ("face_cells", P(c_long)), ("face_hs", P(c_long)), ("face_n", P(c_double)),
         ("face_len", P(c_double)), ("face_bb", P(c_double)), ("ghost_gp", P(c_double)),
         ("bc_face", P(c_long)), ("bc_index", P(c_int)), ("bc_ghost_bary", P(c_double)),
-        ("bc_x", P(c_double)), ("cell_gp5", P(c_double)),
+        ("bc_x", P(c_double)), ("cell_gp5", P(c_double)), ("cell_nodes", P(c_long)),
+        ("node_xy", P(c_double)),
         ("total_area_q", c_double), ("dx_ref", c_double), ("x_min", c_double),
         ("x_max", c_double), ("y_min", c_double), ("y_max", c_double),
     ]
@@ -66,7 +68,8 @@ class Case(C.Structure):
     _fields_ = [("params", Params), ("n_bc_table", c_int), ("bc_table", BC * 20),
                 ("exact", Exact), ("mesh", Mesh), ("prim0", P(c_double)),
                 ("file_name", C.c_char * 256), ("output_format", c_int),
-                ("ic_type", c_int), ("exact_func", c_int)]
+                ("ic_type", c_int), ("exact_func", c_int), ("n_record", c_int),
+                ("record_xy", (c_double * 2) * MAX_RECORD), ("record_cell", c_long * MAX_RECORD)]
 
 
 class Report(C.Structure):
@@ -119,6 +122,10 @@ def _load():
         "ccfd_write_cp": (c_int, [C.c_void_p, C.c_char_p]),
         "ccfd_errors": (c_int, [C.c_void_p, c_int, P(c_double)]),
         "ccfd_exact_state": (c_int, [C.c_void_p, c_int, c_double, P(c_double)]),
+        "ccfd_set_history": (c_int, [C.c_void_p, c_int, P(c_long), c_int]),
+        "ccfd_get_history": (c_int, [C.c_void_p, P(c_double), c_long, P(c_long), P(c_int)]),
+        "ccfd_write_history": (c_int, [C.c_void_p, P(c_double), c_long, c_int, c_int]),
+        "ccfd_locate_points": (c_int, [P(Mesh), P(c_double), c_int, P(c_long)]),
         "ccfd_write_exact_output": (c_int, [C.c_void_p, P(c_double), c_double, c_long, C.c_char_p, C.c_size_t]),
         "ccfd_write_output": (c_int, [C.c_void_p, P(c_double), c_double, c_long, C.c_char_p, C.c_size_t]),
         "ccfd_batch_create": (c_int, [c_int, P(C.c_void_p)]),

@@ -695,6 +695,88 @@ extern "C" int ccfd_exact_state(ccfd_ctx* ctx, int exact_func, double time, doub
     return check_flags(ctx);
 }
 
+// Per-step history (analyze, src/analyze.c:393-433): the step end writes a
+// row per step into a device ring; runs drain it after each host
+// synchronisation (every graph of at most 16 steps, every implicit step,
+// every batch call), so the ring needs no more than those rows.
+extern "C" int ccfd_set_history(ccfd_ctx* ctx, int capacity, const long* record_cells, int n_record) {
+    if (!ctx || !ctx->uploaded || n_record < 0 || n_record > CCFD_MAX_RECORD || (n_record > 0 && !record_cells))
+        return CCFD_ERR_ARG;
+    if (ctx->batch) return CCFD_ERR_BUSY;
+    for (int k = 0; k < n_record; ++k)
+        if (record_cells[k] < 0 || record_cells[k] >= ctx->N) return CCFD_ERR_ARG;
+    CK(cudaSetDevice(ctx->device));
+    StepParams& sp = ctx->sp;
+    drop_graphs(ctx);  // the step graphs hold the step parameters by value
+    ctx->h_hist.clear();
+    if (capacity <= 0) {
+        sp.hist = nullptr;
+        sp.n_rec = 0;
+        sp.rec_cell = nullptr;
+        return CCFD_OK;
+    }
+    if (capacity < 64) capacity = 64;
+    const int width = kHistHead + 4 * n_record;
+    std::vector<int> cells(n_record > 0 ? n_record : 1, 0);
+    for (int k = 0; k < n_record; ++k) cells[k] = ctx->dev_of_cell[record_cells[k]];
+    double* ring = nullptr;
+    const int* rec = nullptr;
+    int st;
+    if ((st = dalloc(ctx, &ring, (size_t)capacity * width)) || (st = dupload_c(ctx, &rec, cells))) return st;
+    CK(cudaMemcpyAsync(ctx->h_ctrl, ctx->ctrl, sizeof(Ctrl), cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    ctx->hist_read = ctx->h_ctrl->iter;
+    sp.hist = ring;
+    sp.hist_cap = capacity;
+    sp.hist_width = width;
+    sp.n_rec = n_record;
+    sp.rec_cell = rec;
+    return CCFD_OK;
+}
+
+int ccfd_history_drain(ccfd_ctx* ctx) {
+    const StepParams& sp = ctx->sp;
+    const long long now = ctx->h_ctrl->iter;
+    if (!sp.hist || now <= ctx->hist_read) {
+        ctx->hist_read = now > ctx->hist_read ? now : ctx->hist_read;
+        return CCFD_OK;
+    }
+    long long first = ctx->hist_read + 1;
+    if (now - first + 1 > sp.hist_cap) first = now - sp.hist_cap + 1;  // older rows were overwritten
+    const size_t w = (size_t)sp.hist_width, old = ctx->h_hist.size();
+    const long long n = now - first + 1;
+    ctx->h_hist.resize(old + (size_t)n * w);
+    // one copy per contiguous run of ring slots (at most two)
+    long long it = first;
+    double* dst = ctx->h_hist.data() + old;
+    while (it <= now) {
+        long long slot = (it - 1) % sp.hist_cap;
+        long long run = std::min<long long>(now - it + 1, sp.hist_cap - slot);
+        CK(cudaMemcpyAsync(dst, sp.hist + slot * w, sizeof(double) * w * run, cudaMemcpyDeviceToHost, ctx->stream));
+        dst += run * w;
+        it += run;
+    }
+    CK(cudaStreamSynchronize(ctx->stream));
+    ctx->hist_read = now;
+    return CCFD_OK;
+}
+
+extern "C" int ccfd_get_history(ccfd_ctx* ctx, double* rows, long max_rows, long* n_rows, int* width) {
+    if (!ctx || !n_rows) return CCFD_ERR_ARG;
+    const long w = ctx->sp.hist ? ctx->sp.hist_width : kHistHead;
+    if (width) *width = (int)w;
+    const long have = (long)(ctx->h_hist.size() / (size_t)w);
+    if (!rows) {
+        *n_rows = have;
+        return CCFD_OK;
+    }
+    const long n = std::min(have, max_rows < 0 ? 0L : max_rows);
+    std::copy(ctx->h_hist.begin(), ctx->h_hist.begin() + n * w, rows);
+    ctx->h_hist.erase(ctx->h_hist.begin(), ctx->h_hist.begin() + n * w);
+    *n_rows = n;
+    return CCFD_OK;
+}
+
 // Autotuner of the stage kernel's launch shape: cells per tile (which sets
 // the CTA's faces and gradient cells per thread) and the cell ordering
 // (Hilbert curve or the reference's numbering).  Every candidate is uploaded
@@ -937,6 +1019,7 @@ extern "C" int ccfd_run_explicit(ccfd_ctx* ctx, long nsteps, ccfd_report* report
         // the buffer the last executed stage wrote
         long long ran = c.iter - iter0;
         if ((ran * nrk) & 1) ctx->cur ^= 1;
+        if (ctx->sp.hist && (st = ccfd_history_drain(ctx))) return st;
         if (prof && (st = collect_profile(ctx, ctx->prof_ev[par][which], (size_t)ran * nrk))) return st;
         if (ran == 0) break;  // error in the first stage of the graph
     }
@@ -1005,6 +1088,20 @@ extern "C" int ccfd_write_cp(ccfd_ctx* ctx, const char* base) {
             fprintf(f, "%15.7f,%15.7f,%15.7f,%15.7f\n", x[k], y[k], atan2(y[k], x[k]), cp[k]);
         fclose(f);
     }
+    // the gnuplot script of the CP files, written once (src/analyze.c:370-386)
+    std::string dem = std::string(base) + "_CP.dem";
+    FILE* d = fopen(dem.c_str(), "r");
+    if (!d) {
+        if (!(d = fopen(dem.c_str(), "w"))) return CCFD_ERR_ARG;
+        fprintf(d, "unset key\n");
+        fprintf(d, "set xlabel 'x'\n");
+        fprintf(d, "set ylabel 'cp'\n");
+        fprintf(d, "set yrange [*:*] reverse\n");
+        fprintf(d, "plot '%s_CP_pressureSide.csv' using 1:4 w l lc rgb 'black', \\\n", base);
+        fprintf(d, "     '%s_CP_suctionSide.csv' using 1:4 w l lc rgb 'black'\n", base);
+        fprintf(d, "pause -1");
+    }
+    fclose(d);
     return CCFD_OK;
 }
 

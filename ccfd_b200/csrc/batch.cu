@@ -363,6 +363,9 @@ int ccfd_implicit_batch_steps(ccfd_batch* b, const std::vector<ccfd_ctx*>& membe
 // on their own criteria (tEnd, convergence, maxIter, step budget, errors).
 extern "C" int ccfd_batch_step(ccfd_batch* b, int steps, int* n_running) {
     if (!b || steps <= 0) return CCFD_ERR_ARG;
+    // a member's history ring must hold the rows of one call
+    for (ccfd_ctx* c : b->inst)
+        if (c->sp.hist && steps > c->sp.hist_cap) return CCFD_ERR_ARG;
     CKB(cudaSetDevice(b->device));
     int st;
     bool direct = false;
@@ -398,6 +401,8 @@ extern "C" int ccfd_batch_step(ccfd_batch* b, int steps, int* n_running) {
     }
     CKB(cudaEventRecord(b->ev1, b->stream));
     if ((st = pull_ctrl(b))) return st;
+    for (ccfd_ctx* c : b->inst)
+        if (c->sp.hist && (st = ccfd_history_drain(c))) return st;
     float ms = 0.0f;
     CKB(cudaEventElapsedTime(&ms, b->ev0, b->ev1));
     b->device_ms += ms;

@@ -62,6 +62,10 @@ struct ccfd_ctx {
     double prof_ms = 0.0;
     long prof_count = 0;
     cudaEvent_t ev_run0 = nullptr, ev_run1 = nullptr;
+    // per-step history: device ring (sp.hist), rows drained to the host
+    // after each synchronisation of a run
+    long long hist_read = 0;         // last iteration drained
+    std::vector<double> h_hist;      // drained rows not yet fetched
     void* implicit_state = nullptr;  // owned by the implicit solver
     void* batch = nullptr;           // the batch this context is stepped by, if any
 };
@@ -73,6 +77,9 @@ void ccfd_fill_stage(ccfd_ctx* ctx, ccfd::StageLaunch& L);
 // control block (abi.cu)
 int ccfd_status_from_flags(unsigned f);
 void ccfd_fill_report(ccfd_ctx* ctx, ccfd_report* r);
+// copy the history rows recorded since the last drain (up to the
+// iteration in ctx->h_ctrl, which the caller has refreshed) to the host
+int ccfd_history_drain(ccfd_ctx* ctx);
 // device-side residual of the current state into ctx->u_t (abi.cu)
 int ccfd_residual_device(ccfd_ctx* ctx, double time);
 // residual of an arbitrary primitive state into ut (abi.cu)

@@ -60,15 +60,37 @@ int main(int argc, char **argv)
 		return fail("upload", st);
 	if ((st = ccfd_set_state(ctx, c->prim0, CCFD_PRIMITIVE)))
 		return fail("initial state", st);
+	/* analyze's per-step files (residual file, record points) */
+	const int history = output && (c->n_record > 0 || c->params.stationary || c->params.calc_wing);
+	if (history && (st = ccfd_set_history(ctx, 4096, c->record_cell, c->n_record)))
+		return fail("history", st);
 	ccfd_report rep;
 	st = c->params.implicit ? ccfd_run_implicit(ctx, steps, &rep) : ccfd_run_explicit(ctx, steps, &rep);
+	if (history) {
+		/* written also when the loop stopped on an error, as the
+		 * reference's files hold every step it finished */
+		long n = 0;
+		int w = 0;
+		int hs = ccfd_get_history(ctx, NULL, 0, &n, &w);
+		double *rows = hs == CCFD_OK ? malloc(sizeof(double) * (size_t)(n > 0 ? n : 1) * w) : NULL;
+		if (!rows)
+			return fail("history", hs ? hs : CCFD_ERR_NOMEM);
+		if ((hs = ccfd_get_history(ctx, rows, n, &n, &w)) ||
+		    (hs = ccfd_write_history(c, rows, n, w, 0)))
+			return fail("history", hs);
+		free(rows);
+	}
 	if (st)
 		return fail("time loop", st);
 	printf("iterations %ld  t %.9g  dt %.6g  residual %.6e %.6e %.6e %.6e  device %.3f ms\n",
 	       rep.iterations, rep.t, rep.dt, rep.residual[0], rep.residual[1], rep.residual[2],
 	       rep.residual[3], rep.device_ms);
-	if (c->params.calc_wing)
+	if (c->params.calc_wing) {
 		printf("cl %.12g  cd %.12g\n", rep.cl, rep.cd);
+		/* the CP files calcCoef leaves after the last step */
+		if (output && (st = ccfd_write_cp(ctx, c->file_name)))
+			return fail("CP files", st);
+	}
 	if (c->params.implicit)
 		printf("newton %ld  gmres %ld\n", rep.newton_iterations, rep.gmres_iterations);
 	if (c->params.exact_solution && c->exact_func > 0) {

@@ -523,6 +523,16 @@ int ccfd_case_load_text(const char *text, const char *base_dir, ccfd_case **out)
 		TRY(ccfd_ini_int(ini, "wall_id", NULL, &lv));
 		P->wall_id = (int)lv;
 	}
+	/* record points (initRecordPoints, src/analyze.c:34-90) */
+	TRY(ccfd_ini_int(ini, "nRecordPoints", "0", &lv));
+	if (lv < 0 || lv > CCFD_MAX_RECORD) {
+		st = CCFD_ERR_INI;
+		goto fail;
+	}
+	c->n_record = (int)lv;
+	for (int k = 0; k < c->n_record; ++k)
+		TRY(ccfd_ini_dbl_array(ini, "pointCoords", 2, NULL, c->record_xy[k]));
+	TRY(ccfd_locate_points(&c->mesh, &c->record_xy[0][0], c->n_record, c->record_cell));
 	/* extensions of this implementation (defaults keep the reference's
 	 * behaviour): precision mode and a relative steady stop criterion */
 	TRY(ccfd_ini_int(ini, "precision", "0", &lv));

@@ -94,6 +94,8 @@ void ccfd_mesh_free(ccfd_mesh *m)
 	free(m->bc_face); free(m->bc_index); free(m->bc_ghost_bary);
 	free(m->bc_x);
 	free(m->cell_gp5);
+	free(m->cell_nodes);
+	free(m->node_xy);
 	memset(m, 0, sizeof(*m));
 }
 
@@ -442,6 +444,8 @@ int ccfd_mesh_build(const double *nodes, long n_nodes,
 	m->cell_domain = malloc(sizeof(int) * N);
 	m->cell_bary = malloc(sizeof(double) * 2 * N);
 	m->cell_gp5 = malloc(sizeof(double) * 2 * N);
+	m->cell_nodes = malloc(sizeof(long) * 4 * N);
+	m->node_xy = malloc(sizeof(double) * 2 * n_nodes);
 	m->cell_geo = malloc(sizeof(double) * 4 * N);
 	m->hs_offset = malloc(sizeof(long) * (N + 1));
 	m->hs_face = malloc(sizeof(long) * H);
@@ -462,6 +466,7 @@ int ccfd_mesh_build(const double *nodes, long n_nodes,
 	long *hs_face_of = malloc(sizeof(long) * n_created);
 	long *hs_pos = malloc(sizeof(long) * n_created);
 	if (!m->cell_type || !m->cell_domain || !m->cell_bary || !m->cell_geo || !m->cell_gp5 ||
+	    !m->cell_nodes || !m->node_xy ||
 	    !m->hs_offset || !m->hs_face || !m->hs_sign || !m->hs_nb ||
 	    !m->hs_gp || !m->hs_w || !m->face_cells || !m->face_hs ||
 	    !m->face_n || !m->face_len || !m->face_bb || !m->ghost_gp ||
@@ -494,6 +499,8 @@ int ccfd_mesh_build(const double *nodes, long n_nodes,
 			m->cell_gp5[2 * e + 1] = bary[2 * e + 1];
 		}
 		memcpy(&m->cell_geo[4 * e], &geo[4 * e], sizeof(double) * 4);
+		for (int j = 0; j < 4; ++j)
+			m->cell_nodes[4 * e + j] = j < etype[e] ? enode[4 * e + j] : -1;
 		m->hs_offset[e] = k;
 		for (int j = etype[e] - 1; j >= 0; --j, ++k) {
 			long s = elem_first[e] + j;
@@ -541,6 +548,7 @@ int ccfd_mesh_build(const double *nodes, long n_nodes,
 		m->face_bb[3 * f + 1] = A->bb[1];
 		m->face_bb[3 * f + 2] = A->bbd;
 	}
+	memcpy(m->node_xy, nodes, sizeof(double) * 2 * n_nodes);
 	m->total_area_q = total_area_q;
 	m->dx_ref = sqrt(1.0 / (total_area_q * N));
 	free(hs_face_of);
@@ -563,6 +571,42 @@ void ccfd_venk_eps2(const ccfd_mesh *m, double venk_k, double *eps2)
 		eps2[e] = (venk_k * sqrt(area)) * (venk_k * sqrt(area)) *
 			  (venk_k * sqrt(area));
 	}
+}
+
+int ccfd_locate_points(const ccfd_mesh *m, const double *xy, int n, long *cells_out)
+{
+	if (!m || (n > 0 && (!xy || !cells_out)) || !m->cell_nodes || !m->node_xy)
+		return CCFD_ERR_ARG;
+	/* initRecordPoints, src/analyze.c:43-82.  The edge normal is divided by
+	 * sqrt(2 u_x^2) as there (u_y does not enter); for an edge with u_x = 0
+	 * the projection is not a number and the edge excludes nothing. */
+	for (int p = 0; p < n; ++p) {
+		const double *pt = &xy[2 * p];
+		long found = -1;
+		for (long e = 0; e < m->n_cells && found < 0; ++e) {
+			int t = m->cell_type[e];
+			int inside = 1;
+			for (int i = 0; i < t; ++i) {
+				int j = i + 1 < t ? i + 1 : 0;
+				const double *x1 = &m->node_xy[2 * m->cell_nodes[4 * e + i]];
+				const double *x2 = &m->node_xy[2 * m->cell_nodes[4 * e + j]];
+				double u[2] = {x2[1] - x1[1], x1[0] - x2[0]};
+				double tmp = sqrt(u[0] * u[0] + u[0] * u[0]);
+				u[0] /= tmp;
+				u[1] /= tmp;
+				double x[2] = {pt[0] - x1[0], pt[1] - x1[1]};
+				double projection = u[0] * x[0] + u[1] * x[1];
+				if (projection > 0.0)
+					inside = 0;
+			}
+			if (inside)
+				found = e;
+		}
+		if (found < 0)
+			return CCFD_ERR_MESH; /* "Record Point # is not in Domain" */
+		cells_out[p] = found;
+	}
+	return CCFD_OK;
 }
 
 /* ------------------------------------------------------------ Cartesian */

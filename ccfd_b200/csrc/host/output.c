@@ -114,3 +114,90 @@ int ccfd_write_exact_output(const ccfd_case *c, const double *prim_exact, double
 {
 	return write_tabular(c, prim_exact, time, iter, 1, path, path_len);
 }
+
+/* analyze's files from history rows (ccfd_set_history): the residual file
+ * <fileName>_analysis.csv with its gnuplot scripts for stationary runs or
+ * calcWing (initAnalyze, src/analyze.c:205-281; analyze, :411-433) and one
+ * file per record point (initRecordPoints / evalRecordPoints, :84-89,
+ * 393-403).  The reference prints the time as t + dt of the step (its
+ * elements' dt after the step). */
+int ccfd_write_history(const ccfd_case *c, const double *rows, long n_rows, int width, int append)
+{
+	if (!c || (n_rows > 0 && !rows) || width < 11 + 4 * c->n_record)
+		return CCFD_ERR_ARG;
+	static const char *var_name[4] = {"RHO", "MX", "MY", "E"};
+	const ccfd_params *p = &c->params;
+	const int av = p->abort_variable >= 0 && p->abort_variable < 4 ? p->abort_variable : 0;
+	char name[600];
+	if (p->calc_wing || p->stationary) {
+		snprintf(name, sizeof(name), "%s_analysis.csv", c->file_name);
+		if (!append) {
+			char res_name[600];
+			snprintf(res_name, sizeof(res_name), "%s", name);
+			FILE *d;
+			snprintf(name, sizeof(name), "%s_residuals.dem", c->file_name);
+			if (!(d = fopen(name, "w")))
+				return CCFD_ERR_ARG;
+			fprintf(d, "set title 'Residual Plot'\n");
+			fprintf(d, "set logscale y\n");
+			if (p->calc_wing) {
+				fprintf(d, "plot '%s' using 1:3 title '%s' with lines\n", res_name, var_name[av]);
+			} else {
+				fprintf(d, "plot '%s' using 1:3 title 'RHO' with lines, \\\n", res_name);
+				fprintf(d, "     '%s' using 1:4 title 'MX' with lines, \\\n", res_name);
+				fprintf(d, "     '%s' using 1:5 title 'MY' with lines, \\\n", res_name);
+				fprintf(d, "     '%s' using 1:6 title 'E' with lines\n", res_name);
+			}
+			fprintf(d, "pause -1");
+			fclose(d);
+			if (p->calc_wing) {
+				snprintf(name, sizeof(name), "%s_CLCD.dem", c->file_name);
+				if (!(d = fopen(name, "w")))
+					return CCFD_ERR_ARG;
+				fprintf(d, "set title 'CL/CD Plot'\n");
+				fprintf(d, "plot '%s' using 1:4 title 'CL' with lines, \\\n", res_name);
+				fprintf(d, "     '%s' using 1:5 title 'CD' with lines\n", res_name);
+				fprintf(d, "pause -1");
+				fclose(d);
+			}
+			snprintf(name, sizeof(name), "%s", res_name);
+		}
+		FILE *f = fopen(name, append ? "a" : "w");
+		if (!f)
+			return CCFD_ERR_ARG;
+		if (!append) {
+			if (p->calc_wing)
+				fprintf(f, "Iter, Time, Residual(%s), CL, CD\n", var_name[av]);
+			else
+				fprintf(f, "Iter, Time, Residual(RHO), Residual(VX), Residual(VY), Residual(E)\n");
+		}
+		for (long r = 0; r < n_rows; ++r) {
+			const double *w = &rows[(size_t)r * width];
+			long iter = (long)w[0];
+			double time = w[1] + w[2];
+			if (p->calc_wing)
+				fprintf(f, "%7ld, %13.8f, %15.8e, %15.10f, %15.10f\n", iter, time, w[3 + av], w[9],
+					w[10]);
+			else
+				fprintf(f, "%7ld, %13.8f, %15.8e, %15.8e, %15.8e, %15.8e\n", iter, time, w[3], w[4],
+					w[5], w[6]);
+		}
+		fclose(f);
+	}
+	for (int k = 0; k < c->n_record; ++k) {
+		snprintf(name, sizeof(name), "%s_recordPoint_%d.csv", c->file_name, k);
+		FILE *f = fopen(name, append ? "a" : "w");
+		if (!f)
+			return CCFD_ERR_ARG;
+		if (!append)
+			fprintf(f, "Time, Density, VelocityX, VelocityY, Pressure\n");
+		for (long r = 0; r < n_rows; ++r) {
+			const double *w = &rows[(size_t)r * width];
+			const double *q = &w[11 + 4 * k];
+			fprintf(f, "%20.12f,%20.12f,%20.12f,%20.12f,%20.12f\n", w[1] + w[2], q[0], q[1], q[2],
+				q[3]);
+		}
+		fclose(f);
+	}
+	return CCFD_OK;
+}

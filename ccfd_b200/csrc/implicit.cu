@@ -1325,7 +1325,8 @@ static int set_step(ImpSet* M) {
         launch_dt(ctx->mesh, ctx->phys, nullptr, ctx->sp, ctx->prim_buf[ctx->cur], ctx->dt_partial, ctx->dt_bad,
                   st);
         imp_step_end_launch(ctx->ctrl, ctx->sp, ctx->res_partial, ctx->tiles.n_tiles, ctx->dt_partial,
-                            ctx->dt_bad, ctx->nb_cells, ctx->wall_ghost, ctx->wall_nl, ctx->ghost_pface, st);
+                            ctx->dt_bad, ctx->nb_cells, ctx->wall_ghost, ctx->wall_nl, ctx->ghost_pface,
+                            ctx->prim_buf[ctx->cur], st);
     }
     CKM(cudaGetLastError());
     return CCFD_OK;
@@ -1376,6 +1377,7 @@ static int run_implicit(ccfd_ctx* ctx, long nsteps, ccfd_report* report) {
         CK(cudaMemcpyAsync(ctx->h_ctrl, ctx->ctrl, sizeof(Ctrl), cudaMemcpyDeviceToHost, st));
         CK(cudaMemcpyAsync(&ctl_status, S->ctl + CTL_STATUS, sizeof(int), cudaMemcpyDeviceToHost, st));
         CK(cudaStreamSynchronize(st));
+        if (ctx->sp.hist && (s = ccfd_history_drain(ctx))) return s;
         if (ctl_status) {
             status = ctl_status;
             break;

@@ -95,6 +95,7 @@ void launch_errors(const DevMesh& m, const double4* xq, const double4* prim, con
                    cudaStream_t st);
 void imp_step_end_launch(Ctrl* ctrl, const StepParams& sp, const double* res_partial, int nres,
                          const double2* dt_partial, const int* dt_bad, int ndt, const int* wall_ghost,
-                         const double* wall_nl, const double* ghost_pface, cudaStream_t st);
+                         const double* wall_nl, const double* ghost_pface, const double4* prim_new,
+                         cudaStream_t st);
 
 }  // namespace ccfd

@@ -60,6 +60,16 @@ struct StepParams {
     int n_wall;           // wall faces in CL/CD summation order
     double q_inf_lq, cos_a, sin_a;
     double total_area_q;
+    // per-step history (the residual-file rows of analyze and the record
+    // points, src/analyze.c:393-433): ring of hist_cap rows of hist_width
+    // doubles, nullptr when off
+    double* hist;
+    int hist_cap, hist_width, n_rec;
+    const int* rec_cell;  // [n_rec] device cell of each record point
 };
+
+// history row: iteration, t after the step, dt, residuals [6], CL, CD, then
+// (rho, vx, vy, p) of each record point
+constexpr int kHistHead = 11;
 
 }  // namespace ccfd

@@ -74,17 +74,18 @@ __global__ void k_step_begin(Ctrl* ctrl, StepParams sp, const double2* __restric
 __global__ void k_step_end_sep(Ctrl* ctrl, StepParams sp, const double* res_partial, int nres,
                                const double2* dt_partial, const int* dt_bad, int ndt,
                                const int* wall_ghost, const double* wall_nl,
-                               const double* ghost_pface) {
+                               const double* ghost_pface, const double4* prim_new) {
     if (!ctrl->active) return;
     step_end_block(ctrl, sp, res_partial, nres, dt_partial, dt_bad, ndt, wall_ghost, wall_nl,
-                   ghost_pface);
+                   ghost_pface, prim_new);
 }
 
 void imp_step_end_launch(Ctrl* ctrl, const StepParams& sp, const double* res_partial, int nres,
                          const double2* dt_partial, const int* dt_bad, int ndt, const int* wall_ghost,
-                         const double* wall_nl, const double* ghost_pface, cudaStream_t st) {
+                         const double* wall_nl, const double* ghost_pface, const double4* prim_new,
+                         cudaStream_t st) {
     k_step_end_sep<<<1, 256, 0, st>>>(ctrl, sp, res_partial, nres, dt_partial, dt_bad, ndt, wall_ghost,
-                                      wall_nl, ghost_pface);
+                                      wall_nl, ghost_pface, prim_new);
 }
 
 

@@ -308,7 +308,7 @@ __device__ __forceinline__ void finish_dt(Ctrl* ctrl, const StepParams& sp, doub
 __device__ __forceinline__ void step_end_block(Ctrl* ctrl, const StepParams& sp, const double* res_partial,
                                int nres, const double2* dt_partial, const int* dt_bad, int ndt,
                                const int* wall_ghost, const double* wall_nl,
-                               const double* ghost_pface) {
+                               const double* ghost_pface, const double4* prim_new) {
     __shared__ double s_res[4];
     __shared__ double2 s_dt;
     __shared__ int s_bad;
@@ -355,6 +355,25 @@ __device__ __forceinline__ void step_end_block(Ctrl* ctrl, const StepParams& sp,
     }
 #pragma unroll
     for (int v = 0; v < 6; ++v) ctrl->res[v] = res[v];
+    if (sp.hist) {
+        // the row of this step; the state of other CTAs is read around L1
+        double* row = sp.hist + (size_t)((iter - 1) % sp.hist_cap) * sp.hist_width;
+        row[0] = (double)iter;
+        row[1] = ctrl->t;
+        row[2] = dt;
+#pragma unroll
+        for (int v = 0; v < 6; ++v) row[3 + v] = res[v];
+        row[9] = ctrl->cl;
+        row[10] = ctrl->cd;
+        for (int k = 0; k < sp.n_rec; ++k) {
+            const double2* q = reinterpret_cast<const double2*>(&prim_new[sp.rec_cell[k]]);
+            double2 a = __ldcg(q), b = __ldcg(q + 1);
+            row[kHistHead + 4 * k] = a.x;
+            row[kHistHead + 4 * k + 1] = a.y;
+            row[kHistHead + 4 * k + 2] = b.x;
+            row[kHistHead + 4 * k + 3] = b.y;
+        }
+    }
     if (!ctrl->have_first) {
 #pragma unroll
         for (int v = 0; v < 4; ++v) ctrl->res_first[v] = res[v];
@@ -599,7 +618,7 @@ __device__ __forceinline__ void stage_body(const StageLaunch& L, const int t) {
             __threadfence();
             Ctrl* ctrl = const_cast<Ctrl*>(L.ctrl);
             step_end_block(ctrl, L.sp, L.res_partial, T.n_tiles, L.dt_partial, L.dt_bad, T.n_tiles,
-                           L.wall_ghost, L.wall_nl, L.ghost_pface);
+                           L.wall_ghost, L.wall_nl, L.ghost_pface, L.prim_out);
             if (tid == 0) {
                 ctrl->par ^= (L.sp.nrk & 1);  // buffer holding the state after this step
                 *L.ticket = 0u;

@@ -164,8 +164,14 @@ typedef struct ccfd_mesh {
 	double *cell_gp5;      /* [N][2] fifth quadrature point of a quad (midpoint
 				  of its nodes 0 and 2, src/mesh.c:157-160);
 				  the barycentre for triangles                */
+	long *cell_nodes;      /* [N][4] element node ids (quads: 4, triangles:
+				  3 and -1)                                   */
+	double *node_xy;       /* [n_nodes][2] node coordinates                 */
 	double total_area_q, dx_ref, x_min, x_max, y_min, y_max;
 } ccfd_mesh;
+
+/* Most record points of a case (the reference has no limit). */
+#define CCFD_MAX_RECORD 64
 
 /* A complete case: parameters, boundary table, mesh and initial state, as
  * the reference's init sequence (src/main.c:101-118) produces them. */
@@ -179,6 +185,9 @@ typedef struct ccfd_case {
 	char file_name[256];   /* fileName                                      */
 	int output_format;     /* outputFormat                                  */
 	int ic_type, exact_func;
+	int n_record;          /* nRecordPoints (src/analyze.c:283-286)         */
+	double record_xy[CCFD_MAX_RECORD][2]; /* pointCoords                    */
+	long record_cell[CCFD_MAX_RECORD];    /* containing cell (elem order)   */
 } ccfd_case;
 
 /* -------------------------------------------------------- host-side API */
@@ -204,6 +213,11 @@ void ccfd_mesh_free(ccfd_mesh *m);
 void ccfd_case_free(ccfd_case *c);
 /* Venkatakrishnan epsilon^2 per cell, (K sqrt(A))^3, src/finiteVolume.c:47-52 */
 void ccfd_venk_eps2(const ccfd_mesh *m, double venk_k, double *eps2_out);
+/* The cell holding each point, as initRecordPoints finds it
+ * (src/analyze.c:43-82): the first cell in element order for which no edge
+ * has the point strictly on its outer side, with the reference's edge-normal
+ * arithmetic.  CCFD_ERR_MESH if a point lies in no cell. */
+int ccfd_locate_points(const ccfd_mesh *m, const double *xy, int n, long *cells_out);
 /* Write a gmsh 2.2 ASCII mesh (the format src/mesh.c:498-742 reads). */
 int ccfd_write_gmsh2(const char *path, const double *nodes, long n_nodes,
 		     const long *tria, long n_tria, const long *quad, long n_quad,
@@ -296,6 +310,27 @@ int ccfd_wall_cp(ccfd_ctx *ctx, double *x, double *y, double *cp, int *n, int *n
 /* The reference's CP files <base>_CP_pressureSide.csv / _CP_suctionSide.csv
  * (rows x, y, phi, cp). */
 int ccfd_write_cp(ccfd_ctx *ctx, const char *base);
+
+/* Per-step history, the data of analyze (src/analyze.c:393-433): with
+ * capacity > 0 every following step (explicit, implicit, alone or in a
+ * batch) records one row of width 11 + 4 * n_record doubles: iteration, t
+ * after the step, dt, the six residuals (four variables, CL, CD), CL, CD,
+ * then rho, vx, vy, p of each record cell (reference cell index, e.g. from
+ * ccfd_locate_points).  The device keeps a ring of `capacity` rows (at least
+ * 64); runs move the rows to the host after each synchronisation.
+ * capacity <= 0 switches it off.  ccfd_upload_case / ccfd_autotune reset
+ * it.  A batch call may not step further than the ring holds. */
+int ccfd_set_history(ccfd_ctx *ctx, int capacity, const long *record_cells, int n_record);
+/* Moves up to max_rows recorded rows (oldest first) into rows and drops
+ * them; *n_rows gets the count and *width (may be NULL) the row width.
+ * rows == NULL: only the number waiting. */
+int ccfd_get_history(ccfd_ctx *ctx, double *rows, long max_rows, long *n_rows, int *width);
+/* The files analyze writes from those rows: <fileName>_analysis.csv (for
+ * stationary runs or calcWing, with its gnuplot scripts
+ * <fileName>_residuals.dem / _CLCD.dem, src/analyze.c:205-281, 411-433) and
+ * <fileName>_recordPoint_<k>.csv (src/analyze.c:84-89, 393-403), with
+ * their headers when `append` is 0. */
+int ccfd_write_history(const ccfd_case *c, const double *rows, long n_rows, int width, int append);
 
 /* Drop-in for calcErrors (src/analyze.c:445-514) at the current time: L1,
  * L2 and Linf norms of the primitive variables against exact function

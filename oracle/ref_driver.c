@@ -21,8 +21,10 @@
  *
  * The initialisation order mirrors main() (src/main.c:53-118).  Output format
  * CGNS is replaced by CSV so that the CGNS stand-in is never reached; with
- * CCFD_REF_OUTPUT set in the environment, run / coef end with dataOutput
- * (solution file, and exact-solution file with exactSolution = T).
+ * CCFD_REF_OUTPUT set in the environment, run / coef call the reference's
+ * analyze every step (residual file, record points, CL / CD) and end with
+ * dataOutput (solution file, and exact-solution file with exactSolution =
+ * T).
  *
  * Dump format: magic "CCFDDMP1", then records of
  *   char name[32]; int32 type (0 = f64, 1 = i64); int32 pad; int64 count; data
@@ -286,6 +288,7 @@ int main(int argc, char *argv[])
 		dump_scalar("dt", dt);
 	} else if (!strcmp(mode, "run") || !strcmp(mode, "coef")) {
 		bool doCoef = !strcmp(mode, "coef");
+		bool write_out = getenv("CCFD_REF_OUTPUT") != NULL;
 		long nsteps = argc > 4 ? strtol(argv[4], NULL, 10) : 0;
 		if (argc > 5)
 			load_state(argv[5]);
@@ -312,7 +315,11 @@ int main(int argc, char *argv[])
 				implicitTimeStep(t, dt, resIter);
 			}
 			t += dt;
-			if (doCoef && doCalcWing) {
+			if (write_out) {
+				/* the reference's own analyze: record points,
+				 * calcCoef, residual file */
+				analyze(t, iter, resIter);
+			} else if (doCoef && doCalcWing) {
 				/* analyze() (src/analyze.c:411-433) without the
 				 * residual-file write */
 				resIter[4] = wing.cl;
@@ -349,7 +356,7 @@ int main(int argc, char *argv[])
 			}
 		}
 		double tEnd = omp_get_wtime();
-		if (getenv("CCFD_REF_OUTPUT")) {
+		if (write_out) {
 			/* the final solution file (and the exact-solution file)
 			 * of dataOutput (src/output.c:334-398) */
 			dataOutput(t, nhist);

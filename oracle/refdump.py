@@ -99,7 +99,7 @@ def run_ref(ini_text: str, mode: str, *args, eqn: str = "euler",
         if output:
             out["output_files"] = {}
             for name in sorted(os.listdir(tmp)):
-                if name.endswith((".csv", ".curve")) and "_CP_" not in name:
+                if name.endswith((".csv", ".curve", ".dem")) and "_CP_" not in name:
                     with open(os.path.join(tmp, name)) as f:
                         out["output_files"][name] = f.read()
         for name in sorted(os.listdir(tmp)):

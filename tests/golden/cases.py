@@ -187,7 +187,7 @@ def implicit_cases() -> dict:
 
 
 def make_mesh(spec):
-    kind = spec["mesh"]
+    kind = spec.get("mesh")
     if kind is None:
         return None
     if kind[0] == "dmr":
@@ -253,4 +253,17 @@ def output_cases() -> dict:
                                    "eqn": "euler"},
         "out_sine_periodic_csv": {"ini": meshgen.sinewave_ini(None, n=8, periodic=True, t_end=0.1),
                                   "eqn": "euler"},
+        # residual file with CL / CD (and the CL / CD gnuplot script)
+        "out_naca_wing_imp": {"mesh": ("naca", 32, 12, 101),
+                              "ini": meshgen.airfoil_ini("naca", mach=0.5, alpha=2.0, flux=2, implicit=True,
+                                                         precond=True, n_kdim=10, cfl=20.0, max_iter=3),
+                              "eqn": "euler"},
     }
+
+
+# Record points (nRecordPoints / pointCoords) are not among the output cases:
+# the reference crashes on them (initRecordPoints stores into
+# recordPoint.elem / recordPoint.ioFile, src/analyze.c:72 and 87, which are
+# never allocated), so no reference file exists to compare with.
+RECORD_POINTS = "nRecordPoints = 3\npointCoords = (/0.47, 0.02/)\npointCoords = (/0.51, 0.04/)\n" \
+                "pointCoords = (/0.905, 0.013/)\n"

@@ -92,11 +92,13 @@ def ref_output() -> dict:
     """The reference's own output files (and final state) of the output
     cases."""
     out = {}
-    for key, spec in CASES.output_cases().items():
-        d = refdump.run_ref(spec["ini"], "run", 0, eqn=spec["eqn"], output=True)
-        files = {k: v for k, v in d["output_files"].items() if not k.endswith("_analysis.csv")}
-        out[key] = {"files": files, "pvar": d["pvar"].tolist(),
-                    "t": float(d["run_info"][0]), "iterations": int(d["run_info"][1])}
+    with tempfile.TemporaryDirectory() as tmp:
+        for key, spec in CASES.output_cases().items():
+            ini, files = CASES.materialise(spec, tmp)
+            d = refdump.run_ref(ini, "run", 0, eqn=spec["eqn"], output=True, files=files)
+            out[key] = {"files": d["output_files"], "pvar": d["pvar"].tolist(),
+                        "history": d["history"].tolist(),
+                        "t": float(d["run_info"][0]), "iterations": int(d["run_info"][1])}
     return out
 
 

@@ -138,3 +138,39 @@ def test_source_term_keys_and_quadrature_points():
     tri = ctype == 3
     assert np.array_equal(gp5[tri], bary[tri])
     assert np.abs(gp5[~tri] - bary[~tri]).max() > 1e-4  # jittered quads
+
+
+def test_record_point_location_follows_reference_rule():
+    # initRecordPoints (src/analyze.c:43-82): first cell in element order
+    # with no edge having the point strictly outside; the edge normal is
+    # scaled by sqrt(2 u_x^2), so edges with u_x = 0 (horizontal) exclude
+    # nothing.  Restated here with numpy on a Sod Cartesian mesh.
+    ini = meshgen.sod_ini(50, 2, t_end=0.1) + "nRecordPoints = 3\npointCoords = (/0.47, 0.02/)\n" \
+        "pointCoords = (/0.51, 0.04/)\npointCoords = (/0.905, 0.013/)\n"
+    case = cc.CaseData.from_text(ini)
+    xy, cells = case.record_points()
+    m = case.c.mesh
+    n = case.n_cells
+    nodes = np.ctypeslib.as_array(m.node_xy, shape=(m.n_nodes * 2,)).reshape(-1, 2)
+    en = np.ctypeslib.as_array(m.cell_nodes, shape=(n * 4,)).reshape(n, 4)
+    ctype = np.ctypeslib.as_array(m.cell_type, shape=(n,))
+    want = []
+    with np.errstate(divide="ignore", invalid="ignore"):
+        for p in xy:
+            for e in range(n):
+                t = ctype[e]
+                inside = True
+                for i in range(t):
+                    x1, x2 = nodes[en[e, i]], nodes[en[e, (i + 1) % t]]
+                    u = np.array([x2[1] - x1[1], x1[0] - x2[0]])
+                    u = u / np.sqrt(u[0] * u[0] + u[0] * u[0])
+                    if u[0] * (p[0] - x1[0]) + u[1] * (p[1] - x1[1]) > 0.0:
+                        inside = False
+                if inside:
+                    want.append(e)
+                    break
+    assert list(cells) == want
+    assert np.allclose(xy, [[0.47, 0.02], [0.51, 0.04], [0.905, 0.013]])
+    with pytest.raises(cc.CcfdError) as e:
+        cc.CaseData.from_text(meshgen.sod_ini(50, 2) + "nRecordPoints = 1\npointCoords = (/1.5, 0.02/)\n")
+    assert e.value.status == 10  # "Record Point # is not in Domain"

@@ -83,7 +83,20 @@ def ref_output():
 
 
 def _numbers(text):
-    return np.array([float(v) for v in re.findall(r"-?\d+\.\d+", text)])
+    return np.array([float(v) for v in re.findall(r"-?\d+\.\d+(?:e[+-]\d+)?", text)])
+
+
+def _files_equal_to_printed_digits(got, want, name):
+    if name.endswith(".dem"):
+        assert got == want, name
+        return
+    assert got.splitlines()[0] == want.splitlines()[0], name
+    assert len(got.splitlines()) == len(want.splitlines()), name
+    a, b = _numbers(got), _numbers(want)
+    assert a.shape == b.shape, name
+    # the last printed digit, or 1e-7 relative where the run agrees to
+    # rounding only (implicit iterates)
+    np.testing.assert_allclose(a, b, rtol=1e-7, atol=2.1e-9, err_msg=name)
 
 
 @pytest.mark.parametrize("key", sorted(CASES.output_cases()))
@@ -91,11 +104,13 @@ def test_writer_reproduces_reference_files_from_its_state(ref_output, key):
     # the reference's final state through the writer: the solution file must
     # be the reference's, byte for byte (same name, header, sort, format)
     g = ref_output[key]
-    case = cc.CaseData.from_text(CASES.output_cases()[key]["ini"])
     prim = np.array(g["pvar"]).reshape(-1, 4)
     cwd = os.getcwd()
     with tempfile.TemporaryDirectory() as tmp:
-        os.chdir(tmp)
+        case, _, _ = CASES.load_case(CASES.output_cases()[key], tmp)
+        out_dir = os.path.join(tmp, "out")
+        os.mkdir(out_dir)
+        os.chdir(out_dir)
         try:
             path = case.write_output(prim, g["t"], g["iterations"])
             with open(path) as f:
@@ -106,6 +121,28 @@ def test_writer_reproduces_reference_files_from_its_state(ref_output, key):
     assert text == g["files"][path]
 
 
+def test_history_writer_reproduces_reference_residual_file(ref_output):
+    # the reference's per-step residuals as history rows: the residual file
+    # and its gnuplot script must be the reference's, byte for byte
+    g = ref_output["out_sod_stationary_csv"]
+    case = cc.CaseData.from_text(CASES.output_cases()["out_sod_stationary_csv"]["ini"])
+    h = np.array(g["history"]).reshape(-1, 8)  # t after the step, dt, residuals [6]
+    rows = np.zeros((len(h), 11))
+    rows[:, 0] = np.arange(1, len(h) + 1)
+    rows[:, 1:9] = h
+    cwd = os.getcwd()
+    with tempfile.TemporaryDirectory() as tmp:
+        os.chdir(tmp)
+        try:
+            case.write_history(rows)
+            got = {n: open(n).read() for n in sorted(os.listdir(tmp))}
+        finally:
+            os.chdir(cwd)
+    assert sorted(got) == ["sod_analysis.csv", "sod_residuals.dem"]
+    for name, text in got.items():
+        assert text == g["files"][name], name
+
+
 @pytest.mark.gpu
 @pytest.mark.parametrize("key", sorted(CASES.output_cases()))
 def test_driver_writes_reference_solution_and_exact_files(ref_output, key):
@@ -113,15 +150,14 @@ def test_driver_writes_reference_solution_and_exact_files(ref_output, key):
     # solution) as the reference's dataOutput, equal to their printed digits
     g = ref_output[key]
     with tempfile.TemporaryDirectory() as tmp:
+        ini, _ = CASES.materialise(CASES.output_cases()[key], tmp)
         with open(os.path.join(tmp, "case.ini"), "w") as f:
-            f.write(CASES.output_cases()[key]["ini"])
+            f.write(ini)
         r = subprocess.run([DRIVER, "case.ini"], cwd=tmp, capture_output=True, text=True, timeout=300)
         assert r.returncode == 0, r.stdout + r.stderr
-        written = sorted(n for n in os.listdir(tmp) if n.endswith((".csv", ".curve")))
+        written = sorted(n for n in os.listdir(tmp)
+                         if n.endswith((".csv", ".curve", ".dem")) and "_CP_" not in n)
         assert written == sorted(g["files"])
         for name in written:
             with open(os.path.join(tmp, name)) as f:
-                text = f.read()
-            want = g["files"][name]
-            assert text.splitlines()[0] == want.splitlines()[0]
-            np.testing.assert_allclose(_numbers(text), _numbers(want), rtol=0, atol=2.1e-9)
+                _files_equal_to_printed_digits(f.read(), g["files"][name], name)
