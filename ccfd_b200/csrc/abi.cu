@@ -6,6 +6,7 @@
 #include <string.h>
 
 #include <algorithm>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -36,13 +37,48 @@ int ccfd_status_from_flags(unsigned f) {
     return CCFD_OK;
 }
 
+// One memory pool per device for all of the library's device buffers.  The
+// default pool hands freed memory back to the driver at synchronisations,
+// which made releasing a context take up to a second in a serving loop;
+// this pool keeps up to CCFD_POOL_KEEP_BYTES (default: all) of freed
+// memory for the next contexts.
+static std::mutex g_pool_mu;
+static cudaMemPool_t g_pool[64];
+
+cudaError_t ccfd_malloc_async(void** p, size_t bytes, cudaStream_t st) {
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    if (dev < 0 || dev >= 64) return cudaMallocAsync(p, bytes, st);
+    cudaMemPool_t pool;
+    {
+        std::lock_guard<std::mutex> lk(g_pool_mu);
+        if (!g_pool[dev]) {
+            cudaMemPoolProps props = {};
+            props.allocType = cudaMemAllocationTypePinned;
+            props.handleTypes = cudaMemHandleTypeNone;
+            props.location.type = cudaMemLocationTypeDevice;
+            props.location.id = dev;
+            if ((e = cudaMemPoolCreate(&g_pool[dev], &props)) != cudaSuccess) {
+                g_pool[dev] = nullptr;
+                return e;
+            }
+            unsigned long long keep = ~0ull;
+            if (const char* v = getenv("CCFD_POOL_KEEP_BYTES")) keep = strtoull(v, nullptr, 10);
+            cudaMemPoolSetAttribute(g_pool[dev], cudaMemPoolAttrReleaseThreshold, &keep);
+        }
+        pool = g_pool[dev];
+    }
+    return cudaMallocFromPoolAsync(p, bytes, pool, st);
+}
+
 template <typename T>
 static int dalloc(ccfd_ctx* ctx, T** p, size_t n) {
     void* q = nullptr;
     if (n == 0) n = 1;
     // stream-ordered: allocating and freeing a context never waits for the
     // work of other contexts (a serving loop admits while others step)
-    cudaError_t e = cudaMallocAsync(&q, n * sizeof(T), ctx->stream);
+    cudaError_t e = ccfd_malloc_async(&q, n * sizeof(T), ctx->stream);
     if (e != cudaSuccess) {
         ctx->last_cuda_error = (int)e;
         return CCFD_ERR_NOMEM;
@@ -213,12 +249,21 @@ extern "C" int ccfd_upload_case(ccfd_ctx* ctx, const ccfd_mesh* m, const ccfd_bc
     ctx->dev_of_cell = cinv;
 
     // interior faces in the order of their owner's device index
+    // (stable counting sort by the owner's device index)
     std::vector<int> fint;
-    for (long f = 0; f < F; ++f)
-        if (m->face_cells[2 * f + 1] >= 0) fint.push_back((int)f);
-    std::stable_sort(fint.begin(), fint.end(), [&](int a, int b) {
-        return cinv[m->face_cells[2 * a]] < cinv[m->face_cells[2 * b]];
-    });
+    {
+        std::vector<int> cnt(N + 1, 0);
+        long nfi = 0;
+        for (long f = 0; f < F; ++f)
+            if (m->face_cells[2 * f + 1] >= 0) {
+                ++cnt[cinv[m->face_cells[2 * f]] + 1];
+                ++nfi;
+            }
+        for (long d = 0; d < N; ++d) cnt[d + 1] += cnt[d];
+        fint.resize(nfi);
+        for (long f = 0; f < F; ++f)
+            if (m->face_cells[2 * f + 1] >= 0) fint[cnt[cinv[m->face_cells[2 * f]]]++] = (int)f;
+    }
     std::vector<int> fdev(F, -1);
     for (size_t i = 0; i < fint.size(); ++i) fdev[fint[i]] = (int)i;
     const long FI = (long)fint.size();
@@ -647,7 +692,7 @@ extern "C" int ccfd_errors(ccfd_ctx* ctx, int exact_func, double out[12]) {
     }
     const int nb = error_blocks((int)ctx->N);
     double* part = nullptr;
-    CK(cudaMallocAsync((void**)&part, sizeof(double) * 12 * nb, ctx->stream));
+    CK(ccfd_malloc_async((void**)&part, sizeof(double) * 12 * nb, ctx->stream));
     launch_errors(ctx->mesh, ctx->cell_xq, cur_prim(ctx), second ? ctx->grad : nullptr, ctx->phys_g, exact_func, t,
                   part, ctx->flags, ctx->stream);
     cudaError_t le = cudaGetLastError();
@@ -678,7 +723,7 @@ extern "C" int ccfd_exact_state(ccfd_ctx* ctx, int exact_func, double time, doub
     CK(cudaSetDevice(ctx->device));
     const long N = ctx->N;
     double4* out = nullptr;
-    CK(cudaMallocAsync((void**)&out, sizeof(double4) * N, ctx->stream));
+    CK(ccfd_malloc_async((void**)&out, sizeof(double4) * N, ctx->stream));
     launch_exact_state((int)N, ctx->cell_xq, ctx->phys_g, exact_func, time, out, ctx->flags, ctx->stream);
     cudaError_t le = cudaGetLastError();
     std::vector<double4> h(N);

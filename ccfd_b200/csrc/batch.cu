@@ -158,8 +158,8 @@ static int rebuild(ccfd_batch* b) {
         }
         g.n_tiles = (int)tmap.size();
         g.smem_bytes = stage_smem_bytes(big, g.fp32);
-        CKB(cudaMallocAsync(&g.d_recs, sizeof(StageLaunch) * recs.size(), b->stream));
-        CKB(cudaMallocAsync(&g.d_tmap, sizeof(int2) * tmap.size(), b->stream));
+        CKB(ccfd_malloc_async((void**)&g.d_recs, sizeof(StageLaunch) * recs.size(), b->stream));
+        CKB(ccfd_malloc_async((void**)&g.d_tmap, sizeof(int2) * tmap.size(), b->stream));
         CKB(cudaMemcpyAsync(g.d_recs, recs.data(), sizeof(StageLaunch) * recs.size(), cudaMemcpyHostToDevice,
                             b->stream));
         CKB(cudaMemcpyAsync(g.d_tmap, tmap.data(), sizeof(int2) * tmap.size(), cudaMemcpyHostToDevice,

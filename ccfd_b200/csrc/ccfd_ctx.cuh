@@ -77,6 +77,9 @@ void ccfd_fill_stage(ccfd_ctx* ctx, ccfd::StageLaunch& L);
 // control block (abi.cu)
 int ccfd_status_from_flags(unsigned f);
 void ccfd_fill_report(ccfd_ctx* ctx, ccfd_report* r);
+// stream-ordered device allocation from the library's memory pool of the
+// current device (abi.cu); free with cudaFreeAsync
+cudaError_t ccfd_malloc_async(void** p, size_t bytes, cudaStream_t st);
 // copy the history rows recorded since the last drain (up to the
 // iteration in ctx->h_ctrl, which the caller has refreshed) to the host
 int ccfd_history_drain(ccfd_ctx* ctx);

@@ -843,7 +843,7 @@ template <typename T>
 static int ialloc(ccfd_ctx* ctx, T** p, size_t n) {
     void* q = nullptr;
     if (n == 0) n = 1;
-    if (cudaMallocAsync(&q, n * sizeof(T), ctx->stream) != cudaSuccess) return CCFD_ERR_NOMEM;
+    if (ccfd_malloc_async(&q, n * sizeof(T), ctx->stream) != cudaSuccess) return CCFD_ERR_NOMEM;
     ctx->allocs.push_back(q);
     ctx->device_bytes += n * sizeof(T);
     *p = (T*)q;
@@ -1167,9 +1167,9 @@ static int set_build(const std::vector<ccfd_ctx*>& members, cudaStream_t stream,
         ccfd_fill_stage(ctx, probe);
         by_variant[std::make_tuple(probe.flux_id, probe.order, probe.ns, probe.fp32)].push_back(k);
     }
-    CKM(cudaMallocAsync(&M->dev, sizeof(ImpDev) * M->n, stream));
+    CKM(ccfd_malloc_async((void**)&M->dev, sizeof(ImpDev) * M->n, stream));
     CKM(cudaMemcpyAsync(M->dev, hd.data(), sizeof(ImpDev) * M->n, cudaMemcpyHostToDevice, stream));
-    CKM(cudaMallocAsync(&M->d_count, sizeof(int), stream));
+    CKM(ccfd_malloc_async((void**)&M->d_count, sizeof(int), stream));
     M->h_count = &M->h_count_v;
     for (auto& kv : by_variant) {
         ImpGroup g;
@@ -1213,10 +1213,10 @@ static int set_build(const std::vector<ccfd_ctx*>& members, cudaStream_t stream,
         g.n_tiles = (int)tmap.size();
         g.smem = stage_smem_bytes(big, g.fp32);
         size_t rb = sizeof(StageLaunch) * idx.size();
-        CKM(cudaMallocAsync(&g.rec_mv, rb, stream));
-        CKM(cudaMallocAsync(&g.rec_nt, rb, stream));
-        CKM(cudaMallocAsync(&g.rec_jac, rb, stream));
-        CKM(cudaMallocAsync(&g.tmap, sizeof(int2) * tmap.size(), stream));
+        CKM(ccfd_malloc_async((void**)&g.rec_mv, rb, stream));
+        CKM(ccfd_malloc_async((void**)&g.rec_nt, rb, stream));
+        CKM(ccfd_malloc_async((void**)&g.rec_jac, rb, stream));
+        CKM(ccfd_malloc_async((void**)&g.tmap, sizeof(int2) * tmap.size(), stream));
         CKM(cudaMemcpyAsync(g.rec_mv, mv.data(), rb, cudaMemcpyHostToDevice, stream));
         CKM(cudaMemcpyAsync(g.rec_nt, nt.data(), rb, cudaMemcpyHostToDevice, stream));
         CKM(cudaMemcpyAsync(g.rec_jac, jac.data(), rb, cudaMemcpyHostToDevice, stream));

@@ -4,7 +4,9 @@
 
 #include <algorithm>
 #include <cmath>
+#include <functional>
 #include <stdint.h>
+#include <thread>
 
 // Hilbert index of (x, y) on a 2^16 x 2^16 grid (the classical iterative
 // quadrant-rotation construction).
@@ -39,45 +41,61 @@ void ccfd_hilbert_order(const ccfd_mesh* m, std::vector<int>& cell_order) {
     double span = std::max(x1 - x0, y1 - y0);
     if (span <= 0) span = 1.0;
     std::vector<uint64_t> key(N);
-    for (long c = 0; c < N; ++c) {
-        double fx = (m->cell_bary[2 * c] - x0) / span, fy = (m->cell_bary[2 * c + 1] - y0) / span;
-        uint32_t ix = (uint32_t)std::min(65535.0, std::max(0.0, fx * 65535.0));
-        uint32_t iy = (uint32_t)std::min(65535.0, std::max(0.0, fy * 65535.0));
-        key[c] = hilbert_index(ix, iy);
+    auto keys = [&](long a, long b) {
+        for (long c = a; c < b; ++c) {
+            double fx = (m->cell_bary[2 * c] - x0) / span, fy = (m->cell_bary[2 * c + 1] - y0) / span;
+            uint32_t ix = (uint32_t)std::min(65535.0, std::max(0.0, fx * 65535.0));
+            uint32_t iy = (uint32_t)std::min(65535.0, std::max(0.0, fy * 65535.0));
+            key[c] = hilbert_index(ix, iy);
+        }
+    };
+    {
+        unsigned hw = std::thread::hardware_concurrency();
+        long nth = std::max(1L, std::min<long>(hw ? hw : 1, std::min(16L, N / 65536)));
+        std::vector<std::thread> pool;
+        for (long k = 0; k + 1 < nth; ++k) pool.emplace_back(keys, N * k / nth, N * (k + 1) / nth);
+        keys(N * (nth - 1) / nth, N);
+        for (std::thread& th : pool) th.join();
     }
-    cell_order.resize(N);
-    for (long c = 0; c < N; ++c) cell_order[c] = (int)c;
-    std::stable_sort(cell_order.begin(), cell_order.end(),
-                     [&](int a, int b) { return key[a] < key[b]; });
+    // stable sort of the cells by key (the key is below 2^32): LSD radix
+    // sort, four passes of 8 bits
+    std::vector<int> a(N), b(N);
+    for (long c = 0; c < N; ++c) a[c] = (int)c;
+    for (int pass = 0; pass < 4; ++pass) {
+        const int shift = 8 * pass;
+        size_t cnt[257] = {0};
+        for (long i = 0; i < N; ++i) ++cnt[((key[a[i]] >> shift) & 255u) + 1];
+        for (int k = 0; k < 256; ++k) cnt[k + 1] += cnt[k];
+        for (long i = 0; i < N; ++i) b[cnt[(key[a[i]] >> shift) & 255u]++] = a[i];
+        a.swap(b);
+    }
+    cell_order.swap(a);
 }
 
-void ccfd_build_tiles(const ccfd_mesh* m, const std::vector<int>& cperm, const std::vector<int>& cinv,
-                      const std::vector<int>& fdev, int T, TileSet& ts) {
+namespace {
+
+// tiles [ta, tb) built by one thread: their concatenated arrays and per-tile
+// sizes; u_code entries go straight into the shared array (disjoint ranges)
+struct TilePart {
+    std::vector<int> counts, e_ref, f_id, f_lr, f_hs, n_e, n_hs, n_f;
+    std::vector<int16_t> hs_nbl, hs_loc;
+    int max_e = 0, max_g = 0, max_hs = 0, max_f = 0;
+};
+
+void build_range(const ccfd_mesh* m, const std::vector<int>& cperm, const std::vector<int>& cinv,
+                 const std::vector<int>& fdev, int T, int ta, int tb, const std::vector<long>& dh,
+                 std::vector<int>& u_code, TilePart& P) {
     const long N = m->n_cells, F = m->n_faces, B = m->n_bc;
-    ts = TileSet();
-    ts.tile_cells = T;
-    ts.n_tiles = (int)((N + T - 1) / T);
     std::vector<int> loc(N, -1), gloc(B, -1), fmark(F, -1);
-    std::vector<int> E, R1, R2, G, faces;
-    ts.e_off.push_back(0);
-    ts.hs_off.push_back(0);
-    ts.f_off.push_back(0);
-    // device half-side offsets (device cell order keeps each cell's
-    // reference side order)
-    std::vector<long> dh(N + 1);
-    dh[0] = 0;
-    for (long d = 0; d < N; ++d) {
-        long c = cperm[d];
-        dh[d + 1] = dh[d] + (m->hs_offset[c + 1] - m->hs_offset[c]);
-    }
-    ts.u_code.assign(dh[N], 0);
-    for (int t = 0; t < ts.n_tiles; ++t) {
+    std::vector<int> E, R1, R2, G, faces, bfaces;
+    for (int t = ta; t < tb; ++t) {
         long d0 = (long)t * T, d1 = std::min(N, d0 + T);
         E.clear();
         R1.clear();
         R2.clear();
         G.clear();
         faces.clear();
+        bfaces.clear();
         for (long d = d0; d < d1; ++d) {
             loc[d] = (int)E.size();
             E.push_back((int)d);
@@ -119,20 +137,21 @@ void ccfd_build_tiles(const ccfd_mesh* m, const std::vector<int>& cperm, const s
             }
         }
         // gradient half-sides: local neighbour index per half-side
+        const size_t hs_nbl0 = P.hs_nbl.size();
+        const int blk = (int)P.hs_loc.size();
         int hs_local = 0;
         for (int i = 0; i < nG; ++i) {
-            ts.hs_loc.push_back((int16_t)hs_local);
+            P.hs_loc.push_back((int16_t)hs_local);
             long c = cperm[E[i]];
             for (long h = m->hs_offset[c]; h < m->hs_offset[c + 1]; ++h, ++hs_local) {
                 long nb = m->hs_nb[h];
                 int l = nb >= 0 ? loc[cinv[nb]] : gloc[-1 - nb];
-                ts.hs_nbl.push_back((int16_t)l);
+                P.hs_nbl.push_back((int16_t)l);
             }
         }
-        ts.hs_loc.push_back((int16_t)hs_local);
+        P.hs_loc.push_back((int16_t)hs_local);
         // faces touching tile cells in first-encounter order: interior
         // faces first, then the tile's boundary faces
-        std::vector<int> bfaces;
         for (long d = d0; d < d1; ++d) {
             long c = cperm[d];
             for (long h = m->hs_offset[c]; h < m->hs_offset[c + 1]; ++h) {
@@ -149,23 +168,22 @@ void ccfd_build_tiles(const ccfd_mesh* m, const std::vector<int>& cperm, const s
         }
         const int nFi = (int)faces.size();
         faces.insert(faces.end(), bfaces.begin(), bfaces.end());
-        const int blk = (int)ts.hs_loc.size() - (nG + 1);
         for (size_t j = 0; j < faces.size(); ++j) {
             long f = faces[j];
             long o = m->face_cells[2 * f], nbr = m->face_cells[2 * f + 1];
             int il = loc[cinv[o]];
-            int hl = ts.hs_loc[blk + il] + (int)(m->face_hs[2 * f] - m->hs_offset[o]);
+            int hl = P.hs_loc[blk + il] + (int)(m->face_hs[2 * f] - m->hs_offset[o]);
             if ((int)j < nFi) {
                 int ir = loc[cinv[nbr]];
-                int hr = ts.hs_loc[blk + ir] + (int)(m->face_hs[2 * f + 1] - m->hs_offset[nbr]);
-                ts.f_id.push_back(fdev[f]);
-                ts.f_lr.push_back(il | (ir << 16));
-                ts.f_hs.push_back(hl | (hr << 16));
+                int hr = P.hs_loc[blk + ir] + (int)(m->face_hs[2 * f + 1] - m->hs_offset[nbr]);
+                P.f_id.push_back(fdev[f]);
+                P.f_lr.push_back(il | (ir << 16));
+                P.f_hs.push_back(hl | (hr << 16));
             } else {
                 int g = (int)(-1 - nbr);
-                ts.f_id.push_back(-1 - g);
-                ts.f_lr.push_back(il | (gloc[g] << 16));
-                ts.f_hs.push_back(hl);
+                P.f_id.push_back(-1 - g);
+                P.f_lr.push_back(il | (gloc[g] << 16));
+                P.f_hs.push_back(hl);
             }
             fmark[f] = -3 - (int)j;  // local index for the codes below
         }
@@ -174,25 +192,87 @@ void ccfd_build_tiles(const ccfd_mesh* m, const std::vector<int>& cperm, const s
             long k = dh[d];
             for (long h = m->hs_offset[c]; h < m->hs_offset[c + 1]; ++h, ++k) {
                 int j = -3 - fmark[m->hs_face[h]];
-                ts.u_code[k] = 2 * j + (m->hs_sign[h] > 0 ? 0 : 1);
+                u_code[k] = 2 * j + (m->hs_sign[h] > 0 ? 0 : 1);
             }
         }
         for (size_t j = 0; j < faces.size(); ++j) fmark[faces[j]] = t;
-        ts.counts.push_back(nT);
-        ts.counts.push_back(nG);
-        ts.counts.push_back(nEc);
-        ts.counts.push_back((int)(E.size() + G.size()));
-        for (int d : E) ts.e_ref.push_back(d);
-        for (int g : G) ts.e_ref.push_back(-1 - g);
-        ts.e_off.push_back((int)ts.e_ref.size());
-        ts.hs_off.push_back((int)ts.hs_nbl.size());
-        ts.f_off.push_back((int)ts.f_id.size());
-        ts.max_e = std::max(ts.max_e, (int)(E.size() + G.size()));
-        ts.max_g = std::max(ts.max_g, nG);
-        ts.max_hs = std::max(ts.max_hs, hs_local);
-        ts.max_f = std::max(ts.max_f, (int)faces.size());
+        P.counts.push_back(nT);
+        P.counts.push_back(nG);
+        P.counts.push_back(nEc);
+        P.counts.push_back((int)(E.size() + G.size()));
+        for (int d : E) P.e_ref.push_back(d);
+        for (int g : G) P.e_ref.push_back(-1 - g);
+        P.n_e.push_back((int)(E.size() + G.size()));
+        P.n_hs.push_back((int)(P.hs_nbl.size() - hs_nbl0));
+        P.n_f.push_back((int)faces.size());
+        P.max_e = std::max(P.max_e, (int)(E.size() + G.size()));
+        P.max_g = std::max(P.max_g, nG);
+        P.max_hs = std::max(P.max_hs, hs_local);
+        P.max_f = std::max(P.max_f, (int)faces.size());
         // reset the local maps
         for (int d : E) loc[d] = -1;
         for (int g : G) gloc[g] = -1;
+    }
+}
+
+template <typename V>
+void append(V& dst, const V& src) {
+    dst.insert(dst.end(), src.begin(), src.end());
+}
+
+}  // namespace
+
+// Tiles are independent: ranges of tiles are built on several host threads
+// (each with its own scratch) and concatenated in tile order, so the result
+// does not depend on the thread count.
+void ccfd_build_tiles(const ccfd_mesh* m, const std::vector<int>& cperm, const std::vector<int>& cinv,
+                      const std::vector<int>& fdev, int T, TileSet& ts) {
+    const long N = m->n_cells;
+    ts = TileSet();
+    ts.tile_cells = T;
+    ts.n_tiles = (int)((N + T - 1) / T);
+    // device half-side offsets (device cell order keeps each cell's
+    // reference side order)
+    std::vector<long> dh(N + 1);
+    dh[0] = 0;
+    for (long d = 0; d < N; ++d) {
+        long c = cperm[d];
+        dh[d + 1] = dh[d] + (m->hs_offset[c + 1] - m->hs_offset[c]);
+    }
+    ts.u_code.assign(dh[N], 0);
+    unsigned hw = std::thread::hardware_concurrency();
+    int nth = (int)std::max(1u, std::min(hw ? hw : 1u, 16u));
+    nth = std::max(1, std::min(nth, ts.n_tiles / 64));
+    std::vector<TilePart> parts(nth);
+    std::vector<std::thread> pool;
+    for (int k = 0; k < nth; ++k) {
+        int ta = (int)((long)ts.n_tiles * k / nth), tb = (int)((long)ts.n_tiles * (k + 1) / nth);
+        if (k + 1 == nth)
+            build_range(m, cperm, cinv, fdev, T, ta, tb, dh, ts.u_code, parts[k]);
+        else
+            pool.emplace_back(build_range, m, std::cref(cperm), std::cref(cinv), std::cref(fdev), T, ta, tb,
+                              std::cref(dh), std::ref(ts.u_code), std::ref(parts[k]));
+    }
+    for (std::thread& th : pool) th.join();
+    ts.e_off.push_back(0);
+    ts.hs_off.push_back(0);
+    ts.f_off.push_back(0);
+    for (const TilePart& P : parts) {
+        append(ts.counts, P.counts);
+        append(ts.e_ref, P.e_ref);
+        append(ts.hs_nbl, P.hs_nbl);
+        append(ts.hs_loc, P.hs_loc);
+        append(ts.f_id, P.f_id);
+        append(ts.f_lr, P.f_lr);
+        append(ts.f_hs, P.f_hs);
+        for (size_t i = 0; i < P.n_e.size(); ++i) {
+            ts.e_off.push_back(ts.e_off.back() + P.n_e[i]);
+            ts.hs_off.push_back(ts.hs_off.back() + P.n_hs[i]);
+            ts.f_off.push_back(ts.f_off.back() + P.n_f[i]);
+        }
+        ts.max_e = std::max(ts.max_e, P.max_e);
+        ts.max_g = std::max(ts.max_g, P.max_g);
+        ts.max_hs = std::max(ts.max_hs, P.max_hs);
+        ts.max_f = std::max(ts.max_f, P.max_f);
     }
 }
