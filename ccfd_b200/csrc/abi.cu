@@ -7,6 +7,7 @@
 
 #include <algorithm>
 #include <mutex>
+#include <thread>
 #include <string>
 #include <vector>
 
@@ -221,6 +222,32 @@ static void build_wall_list(const ccfd_mesh* m, const ccfd_bc* bc, int wall_code
     *n_pressure = (int)pressure.size();
 }
 
+// Host loop over [0, n) split across up to 16 threads (the gathers from the
+// reference's cell order into the device order are memory-latency bound).
+template <typename Fn>
+static void par_for(long n, Fn fn) {
+    unsigned hw = std::thread::hardware_concurrency();
+    long nth = std::max(1L, std::min<long>(hw ? hw : 1, std::min(16L, n / 32768)));
+    std::vector<std::thread> pool;
+    for (long k = 0; k + 1 < nth; ++k) pool.emplace_back(fn, n * k / nth, n * (k + 1) / nth);
+    fn(n * (nth - 1) / nth, n);
+    for (std::thread& th : pool) th.join();
+}
+
+// Host staging of an upload, kept per thread from one upload to the next:
+// filling a few hundred MB of freshly allocated host memory per upload cost
+// more in page faults than the work itself.
+struct UploadScratch {
+    std::vector<int> cperm, cinv, fint, fdev, cnt, hs_off, hs_nb, hs_dev_of_ref;
+    std::vector<int> g_cell, g_hs, g_bc, gl_off;
+    std::vector<double4> hs_gw, cell_geo, cell_xq, face_nl, face_bb, g_gn, g_ml, g_bb;
+    std::vector<double> venk, e2;
+    std::vector<int4> counts;
+    std::vector<short> hs_nbl, hs_loc;
+    TileSet ts;
+};
+static thread_local UploadScratch tl_upload;
+
 extern "C" int ccfd_upload_case(ccfd_ctx* ctx, const ccfd_mesh* m, const ccfd_bc* bc, int n_bc,
                                 const ccfd_exact* ex, int reorder) {
     if (!ctx || !m || (!bc && n_bc > 0) || !ex || n_bc > kMaxBC) return CCFD_ERR_ARG;
@@ -234,25 +261,28 @@ extern "C" int ccfd_upload_case(ccfd_ctx* ctx, const ccfd_mesh* m, const ccfd_bc
     const long N = m->n_cells, F = m->n_faces, B = m->n_bc;
     ctx->N = N;
     ctx->B = B;
+    UploadScratch& S = tl_upload;
 
     // cell order: Hilbert curve of the barycentres (or the reference order);
     // results do not depend on it, only the storage order changes
-    std::vector<int> cperm;
+    std::vector<int>& cperm = S.cperm;
     if (reorder) ccfd_hilbert_order(m, cperm);
     else {
         cperm.resize(N);
         for (long i = 0; i < N; ++i) cperm[i] = (int)i;
     }
-    std::vector<int> cinv(N);
+    std::vector<int>& cinv = S.cinv;
+    cinv.resize(N);
     for (long i = 0; i < N; ++i) cinv[cperm[i]] = (int)i;
     ctx->cell_of_dev = cperm;
     ctx->dev_of_cell = cinv;
 
     // interior faces in the order of their owner's device index
     // (stable counting sort by the owner's device index)
-    std::vector<int> fint;
+    std::vector<int>& fint = S.fint;
     {
-        std::vector<int> cnt(N + 1, 0);
+        std::vector<int>& cnt = S.cnt;
+        cnt.assign(N + 1, 0);
         long nfi = 0;
         for (long f = 0; f < F; ++f)
             if (m->face_cells[2 * f + 1] >= 0) {
@@ -264,48 +294,80 @@ extern "C" int ccfd_upload_case(ccfd_ctx* ctx, const ccfd_mesh* m, const ccfd_bc
         for (long f = 0; f < F; ++f)
             if (m->face_cells[2 * f + 1] >= 0) fint[cnt[cinv[m->face_cells[2 * f]]]++] = (int)f;
     }
-    std::vector<int> fdev(F, -1);
+    std::vector<int>& fdev = S.fdev;
+    fdev.assign(F, -1);
     for (size_t i = 0; i < fint.size(); ++i) fdev[fint[i]] = (int)i;
     const long FI = (long)fint.size();
     ctx->F = FI;
 
     // per-cell CSR in device order
-    std::vector<int> hs_off(N + 1), hs_nb;
-    std::vector<double4> hs_gw, cell_geo(N), cell_xq(N);
-    std::vector<int> hs_dev_of_ref(m->n_half_sides);
-    hs_nb.reserve(m->n_half_sides);
-    hs_gw.reserve(m->n_half_sides);
+    std::vector<int>& hs_off = S.hs_off;
+    std::vector<int>& hs_nb = S.hs_nb;
+    std::vector<double4>& hs_gw = S.hs_gw;
+    std::vector<double4>& cell_geo = S.cell_geo;
+    std::vector<double4>& cell_xq = S.cell_xq;
+    std::vector<int>& hs_dev_of_ref = S.hs_dev_of_ref;
+    hs_off.resize(N + 1);
+    cell_geo.resize(N);
+    cell_xq.resize(N);
+    hs_dev_of_ref.resize(m->n_half_sides);
+    hs_off[0] = 0;
     for (long d = 0; d < N; ++d) {
         long c = cperm[d];
-        hs_off[d] = (int)hs_nb.size();
-        for (long h = m->hs_offset[c]; h < m->hs_offset[c + 1]; ++h) {
-            long nb = m->hs_nb[h];
-            hs_dev_of_ref[h] = (int)hs_nb.size();
-            hs_nb.push_back(nb >= 0 ? cinv[nb] : (int)nb);
-            hs_gw.push_back(make_double4(m->hs_gp[2 * h], m->hs_gp[2 * h + 1], m->hs_w[2 * h], m->hs_w[2 * h + 1]));
+        hs_off[d + 1] = hs_off[d] + (int)(m->hs_offset[c + 1] - m->hs_offset[c]);
+    }
+    hs_nb.resize(hs_off[N]);
+    hs_gw.resize(hs_off[N]);
+    std::vector<double>& venk = S.venk;
+    venk.resize(N);
+    const bool vk = p.spatial_order == 2 && p.limiter == 2;
+    par_for(N, [&](long d0, long d1) {
+        for (long d = d0; d < d1; ++d) {
+            long c = cperm[d];
+            long k = hs_off[d];
+            for (long h = m->hs_offset[c]; h < m->hs_offset[c + 1]; ++h, ++k) {
+                long nb = m->hs_nb[h];
+                hs_dev_of_ref[h] = (int)k;
+                hs_nb[k] = nb >= 0 ? cinv[nb] : (int)nb;
+                hs_gw[k] = make_double4(m->hs_gp[2 * h], m->hs_gp[2 * h + 1], m->hs_w[2 * h], m->hs_w[2 * h + 1]);
+            }
+            cell_geo[d] = make_double4(m->cell_geo[4 * c], m->cell_geo[4 * c + 1], m->cell_geo[4 * c + 2],
+                                       m->cell_geo[4 * c + 3]);
+            const double* b = &m->cell_bary[2 * c];
+            const double* q5 = m->cell_gp5 ? &m->cell_gp5[2 * c] : b;
+            cell_xq[d] = make_double4(b[0], b[1], q5[0], q5[1]);
+            // src/finiteVolume.c:47-52, as ccfd_venk_eps2
+            const double a = m->cell_geo[4 * c];
+            venk[d] = vk ? (p.venk_k * sqrt(a)) * (p.venk_k * sqrt(a)) * (p.venk_k * sqrt(a)) : 0.0;
         }
-        cell_geo[d] = make_double4(m->cell_geo[4 * c], m->cell_geo[4 * c + 1], m->cell_geo[4 * c + 2],
-                                   m->cell_geo[4 * c + 3]);
-        const double* b = &m->cell_bary[2 * c];
-        const double* q5 = m->cell_gp5 ? &m->cell_gp5[2 * c] : b;
-        cell_xq[d] = make_double4(b[0], b[1], q5[0], q5[1]);
-    }
-    hs_off[N] = (int)hs_nb.size();
-    std::vector<double> venk(N, 0.0);
-    if (p.spatial_order == 2 && p.limiter == 2) {
-        std::vector<double> e2(N);
-        ccfd_venk_eps2(m, p.venk_k, e2.data());
-        for (long d = 0; d < N; ++d) venk[d] = e2[cperm[d]];
-    }
-    std::vector<double4> face_nl(FI + 1), face_bb(FI + 1);
-    for (long i = 0; i < FI; ++i) {
-        long f = fint[i];
-        face_nl[i] = make_double4(m->face_n[2 * f], m->face_n[2 * f + 1], m->face_len[f], 0.0);
-        face_bb[i] = make_double4(m->face_bb[3 * f], m->face_bb[3 * f + 1], m->face_bb[3 * f + 2], 0.0);
-    }
+    });
+    // face geometry; the barycentre vectors only for the viscous fluxes
+    const bool ns = p.eqn == CCFD_NAVIER_STOKES;
+    std::vector<double4>& face_nl = S.face_nl;
+    std::vector<double4>& face_bb = S.face_bb;
+    face_nl.resize(FI + 1);
+    face_bb.resize(ns ? FI + 1 : 1);
+    face_nl[FI] = face_bb[face_bb.size() - 1] = make_double4(0, 0, 0, 0);
+    par_for(FI, [&](long i0, long i1) {
+        for (long i = i0; i < i1; ++i) {
+            long f = fint[i];
+            face_nl[i] = make_double4(m->face_n[2 * f], m->face_n[2 * f + 1], m->face_len[f], 0.0);
+            if (ns) face_bb[i] = make_double4(m->face_bb[3 * f], m->face_bb[3 * f + 1], m->face_bb[3 * f + 2], 0.0);
+        }
+    });
     // ghosts (BCside order)
-    std::vector<int> g_cell(B + 1), g_hs(B + 1), g_bc(B + 1);
-    std::vector<double4> g_gn(B + 1), g_ml(B + 1), g_bb(B + 1);
+    std::vector<int>& g_cell = S.g_cell;
+    std::vector<int>& g_hs = S.g_hs;
+    std::vector<int>& g_bc = S.g_bc;
+    std::vector<double4>& g_gn = S.g_gn;
+    std::vector<double4>& g_ml = S.g_ml;
+    std::vector<double4>& g_bb = S.g_bb;
+    g_cell.assign(B + 1, 0);
+    g_hs.assign(B + 1, 0);
+    g_bc.assign(B + 1, 0);
+    g_gn.assign(B + 1, make_double4(0, 0, 0, 0));
+    g_ml.assign(B + 1, make_double4(0, 0, 0, 0));
+    g_bb.assign(B + 1, make_double4(0, 0, 0, 0));
     for (long g = 0; g < B; ++g) {
         long f = m->bc_face[g];
         g_cell[g] = cinv[m->face_cells[2 * f]];
@@ -317,11 +379,13 @@ extern "C" int ccfd_upload_case(ccfd_ctx* ctx, const ccfd_mesh* m, const ccfd_bc
         g_bb[g] = make_double4(m->face_bb[3 * f], m->face_bb[3 * f + 1], m->face_bb[3 * f + 2], 0.0);
     }
     // tiles of the fused stage kernel
-    TileSet ts;
+    TileSet& ts = S.ts;
     ccfd_build_tiles(m, cperm, cinv, fdev, ctx->tile_cells, ts);
     if (ts.max_e >= 32768 || ts.max_hs >= 32768) return CCFD_ERR_ARG;
-    std::vector<int4> counts(ts.n_tiles);
-    std::vector<int> gl_off(ts.n_tiles + 1, 0);
+    std::vector<int4>& counts = S.counts;
+    std::vector<int>& gl_off = S.gl_off;
+    counts.resize(ts.n_tiles);
+    gl_off.assign(ts.n_tiles + 1, 0);
     for (int t = 0; t < ts.n_tiles; ++t) {
         counts[t] = make_int4(ts.counts[4 * t], ts.counts[4 * t + 1], ts.counts[4 * t + 2], ts.counts[4 * t + 3]);
         gl_off[t + 1] = gl_off[t] + ts.counts[4 * t + 1] + 1;
@@ -333,7 +397,10 @@ extern "C" int ccfd_upload_case(ccfd_ctx* ctx, const ccfd_mesh* m, const ccfd_bc
     memset(&td, 0, sizeof(td));
     GhostDev& gd = ctx->ghosts;
     memset(&gd, 0, sizeof(gd));
-    std::vector<short> hs_nbl(ts.hs_nbl.begin(), ts.hs_nbl.end()), hs_loc(ts.hs_loc.begin(), ts.hs_loc.end());
+    std::vector<short>& hs_nbl = S.hs_nbl;
+    std::vector<short>& hs_loc = S.hs_loc;
+    hs_nbl.assign(ts.hs_nbl.begin(), ts.hs_nbl.end());
+    hs_loc.assign(ts.hs_loc.begin(), ts.hs_loc.end());
     if ((st = dupload_c(ctx, &dm.hs_off, hs_off)) || (st = dupload_c(ctx, &dm.hs_nb, hs_nb)) ||
         (st = dupload_c(ctx, &dm.hs_gw, hs_gw)) || (st = dupload_c(ctx, &dm.cell_geo, cell_geo)) ||
         (st = dupload_c(ctx, &dm.venk_eps2, venk)) || (st = dupload_c(ctx, &dm.face_nl, face_nl)) ||
@@ -543,21 +610,29 @@ extern "C" int ccfd_set_state(ccfd_ctx* ctx, const double* state, int kind) {
     if (ctx->batch) return CCFD_ERR_BUSY;
     CK(cudaSetDevice(ctx->device));
     const long N = ctx->N;
-    std::vector<double4> prim(N), cons(N);
+    // (thread_local staging reached through references: the worker threads
+    // of par_for must use this thread's buffers, not their own)
+    static thread_local std::vector<double4> tl_prim, tl_cons;
+    std::vector<double4>& prim = tl_prim;
+    std::vector<double4>& cons = tl_cons;
+    prim.resize(N);
+    cons.resize(N);
     double gam1 = ctx->phys.gam1, gam1q = ctx->phys.gam1q;
-    for (long d = 0; d < N; ++d) {
-        const double* s = &state[4 * ctx->cell_of_dev[d]];
-        double pv[4], cv[4];
-        if (kind == CCFD_CONSERVATIVE) {
-            memcpy(cv, s, sizeof(cv));
-            ccfd_host_cons_prim(gam1, cv, pv);
-        } else {
-            memcpy(pv, s, sizeof(pv));
-            ccfd_host_prim_cons(gam1q, pv, cv);
+    par_for(N, [&](long d0, long d1) {
+        for (long d = d0; d < d1; ++d) {
+            const double* s = &state[4 * ctx->cell_of_dev[d]];
+            double pv[4], cv[4];
+            if (kind == CCFD_CONSERVATIVE) {
+                memcpy(cv, s, sizeof(cv));
+                ccfd_host_cons_prim(gam1, cv, pv);
+            } else {
+                memcpy(pv, s, sizeof(pv));
+                ccfd_host_prim_cons(gam1q, pv, cv);
+            }
+            prim[d] = make_double4(pv[0], pv[1], pv[2], pv[3]);
+            cons[d] = make_double4(cv[0], cv[1], cv[2], cv[3]);
         }
-        prim[d] = make_double4(pv[0], pv[1], pv[2], pv[3]);
-        cons[d] = make_double4(cv[0], cv[1], cv[2], cv[3]);
-    }
+    });
     CK(cudaMemcpyAsync(cur_prim(ctx), prim.data(), sizeof(double4) * N, cudaMemcpyHostToDevice, ctx->stream));
     CK(cudaMemcpyAsync(ctx->cons0, cons.data(), sizeof(double4) * N, cudaMemcpyHostToDevice, ctx->stream));
     CK(cudaStreamSynchronize(ctx->stream));
@@ -568,14 +643,18 @@ extern "C" int ccfd_get_state(ccfd_ctx* ctx, double* state, int kind) {
     if (!ctx || !state || !ctx->uploaded) return CCFD_ERR_ARG;
     CK(cudaSetDevice(ctx->device));
     const long N = ctx->N;
-    std::vector<double4> h(N);
+    static thread_local std::vector<double4> tl_h;
+    std::vector<double4>& h = tl_h;  // (see ccfd_set_state)
+    h.resize(N);
     CK(cudaMemcpyAsync(h.data(), kind == CCFD_CONSERVATIVE ? ctx->cons0 : cur_prim(ctx), sizeof(double4) * N,
                        cudaMemcpyDeviceToHost, ctx->stream));
     CK(cudaStreamSynchronize(ctx->stream));
-    for (long d = 0; d < N; ++d) {
-        double* s = &state[4 * ctx->cell_of_dev[d]];
-        s[0] = h[d].x; s[1] = h[d].y; s[2] = h[d].z; s[3] = h[d].w;
-    }
+    par_for(N, [&](long d0, long d1) {
+        for (long d = d0; d < d1; ++d) {
+            double* s = &state[4 * ctx->cell_of_dev[d]];
+            s[0] = h[d].x; s[1] = h[d].y; s[2] = h[d].z; s[3] = h[d].w;
+        }
+    });
     return CCFD_OK;
 }
 

@@ -5,6 +5,8 @@
 #include <algorithm>
 #include <cmath>
 #include <functional>
+#include <memory>
+#include <mutex>
 #include <stdint.h>
 #include <thread>
 
@@ -82,12 +84,50 @@ struct TilePart {
     int max_e = 0, max_g = 0, max_hs = 0, max_f = 0;
 };
 
+// per-thread work arrays, reused across calls (a pool shared by all calls):
+// fresh cell- and face-sized arrays per thread and call cost more in page
+// faults than the tile construction
+struct TileScratch {
+    std::vector<int> loc, gloc, fmark, E, R1, R2, G, faces, bfaces;
+    TilePart part;
+};
+std::mutex g_scratch_mu;
+std::vector<std::unique_ptr<TileScratch>> g_scratch;
+
+std::unique_ptr<TileScratch> take_scratch() {
+    std::lock_guard<std::mutex> lk(g_scratch_mu);
+    if (g_scratch.empty()) return std::unique_ptr<TileScratch>(new TileScratch());
+    std::unique_ptr<TileScratch> s = std::move(g_scratch.back());
+    g_scratch.pop_back();
+    return s;
+}
+
+void give_scratch(std::unique_ptr<TileScratch> s) {
+    std::lock_guard<std::mutex> lk(g_scratch_mu);
+    g_scratch.push_back(std::move(s));
+}
+
 void build_range(const ccfd_mesh* m, const std::vector<int>& cperm, const std::vector<int>& cinv,
                  const std::vector<int>& fdev, int T, int ta, int tb, const std::vector<long>& dh,
-                 std::vector<int>& u_code, TilePart& P) {
+                 std::vector<int>& u_code, TileScratch& W) {
     const long N = m->n_cells, F = m->n_faces, B = m->n_bc;
-    std::vector<int> loc(N, -1), gloc(B, -1), fmark(F, -1);
-    std::vector<int> E, R1, R2, G, faces, bfaces;
+    std::vector<int>&loc = W.loc, &gloc = W.gloc, &fmark = W.fmark;
+    std::vector<int>&E = W.E, &R1 = W.R1, &R2 = W.R2, &G = W.G, &faces = W.faces, &bfaces = W.bfaces;
+    loc.assign(N, -1);
+    gloc.assign(B, -1);
+    fmark.assign(F, -1);
+    TilePart& P = W.part;
+    P.counts.clear();
+    P.e_ref.clear();
+    P.f_id.clear();
+    P.f_lr.clear();
+    P.f_hs.clear();
+    P.n_e.clear();
+    P.n_hs.clear();
+    P.n_f.clear();
+    P.hs_nbl.clear();
+    P.hs_loc.clear();
+    P.max_e = P.max_g = P.max_hs = P.max_f = 0;
     for (int t = ta; t < tb; ++t) {
         long d0 = (long)t * T, d1 = std::min(N, d0 + T);
         E.clear();
@@ -228,7 +268,18 @@ void append(V& dst, const V& src) {
 void ccfd_build_tiles(const ccfd_mesh* m, const std::vector<int>& cperm, const std::vector<int>& cinv,
                       const std::vector<int>& fdev, int T, TileSet& ts) {
     const long N = m->n_cells;
-    ts = TileSet();
+    // (the vectors keep their capacity from an earlier call)
+    ts.e_off.clear();
+    ts.counts.clear();
+    ts.e_ref.clear();
+    ts.hs_off.clear();
+    ts.hs_nbl.clear();
+    ts.hs_loc.clear();
+    ts.f_off.clear();
+    ts.f_id.clear();
+    ts.f_lr.clear();
+    ts.f_hs.clear();
+    ts.max_e = ts.max_g = ts.max_hs = ts.max_f = 0;
     ts.tile_cells = T;
     ts.n_tiles = (int)((N + T - 1) / T);
     // device half-side offsets (device cell order keeps each cell's
@@ -243,21 +294,23 @@ void ccfd_build_tiles(const ccfd_mesh* m, const std::vector<int>& cperm, const s
     unsigned hw = std::thread::hardware_concurrency();
     int nth = (int)std::max(1u, std::min(hw ? hw : 1u, 16u));
     nth = std::max(1, std::min(nth, ts.n_tiles / 64));
-    std::vector<TilePart> parts(nth);
+    std::vector<std::unique_ptr<TileScratch>> work(nth);
+    for (int k = 0; k < nth; ++k) work[k] = take_scratch();
     std::vector<std::thread> pool;
     for (int k = 0; k < nth; ++k) {
         int ta = (int)((long)ts.n_tiles * k / nth), tb = (int)((long)ts.n_tiles * (k + 1) / nth);
         if (k + 1 == nth)
-            build_range(m, cperm, cinv, fdev, T, ta, tb, dh, ts.u_code, parts[k]);
+            build_range(m, cperm, cinv, fdev, T, ta, tb, dh, ts.u_code, *work[k]);
         else
             pool.emplace_back(build_range, m, std::cref(cperm), std::cref(cinv), std::cref(fdev), T, ta, tb,
-                              std::cref(dh), std::ref(ts.u_code), std::ref(parts[k]));
+                              std::cref(dh), std::ref(ts.u_code), std::ref(*work[k]));
     }
     for (std::thread& th : pool) th.join();
     ts.e_off.push_back(0);
     ts.hs_off.push_back(0);
     ts.f_off.push_back(0);
-    for (const TilePart& P : parts) {
+    for (int k = 0; k < nth; ++k) {
+        const TilePart& P = work[k]->part;
         append(ts.counts, P.counts);
         append(ts.e_ref, P.e_ref);
         append(ts.hs_nbl, P.hs_nbl);
@@ -275,4 +328,5 @@ void ccfd_build_tiles(const ccfd_mesh* m, const std::vector<int>& cperm, const s
         ts.max_hs = std::max(ts.max_hs, P.max_hs);
         ts.max_f = std::max(ts.max_f, P.max_f);
     }
+    for (int k = 0; k < nth; ++k) give_scratch(std::move(work[k]));
 }
