@@ -102,6 +102,25 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
+def max_over_ranks(x: float, dist) -> float:
+    """The largest value of x over the ranks (the job's time is its slowest
+    rank's); a plain return without a process group."""
+    if dist is None:
+        return float(x)
+    import torch
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([float(x)], device=dev, dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def replica_throughput(world: int, cells: int, stages: int, steps: int, seconds: float) -> float:
+    """Whole-job cell-updates/s of `world` independent replicas that each
+    ran `steps` steps of `stages` stages over `cells` cells, timed by the
+    slowest rank."""
+    return world * cells * stages * steps / seconds
+
+
 def algorithmic_bytes_per_stage(m: dict, venk: bool) -> int:
     """Compulsory HBM traffic of one residual evaluation + RK stage of the
     fused scheme (gradients and face fluxes never leave the chip), each array
@@ -429,12 +448,9 @@ def main() -> int:
         clk = clocks.stop()
         res_ms, res_cnt = s.profile(reset=True)
         prim_fp64 = s.get_state()
-        t_ms = torch.tensor([rep["device_ms"]], device="cuda", dtype=torch.float64)
-        if dist is not None:
-            dist.all_reduce(t_ms, op=dist.ReduceOp.MAX)
-        t_ms = float(t_ms.item())
+        t_ms = max_over_ranks(rep["device_ms"], dist)
         steps_done = rep["iterations"] - args.warmup
-        value = world * n * nrk * steps_done / (t_ms / 1e3)
+        value = replica_throughput(world, n, nrk, steps_done, t_ms / 1e3)
         s.set_profiling(False)
 
         # end to end through the public API with host buffers: every step
@@ -449,10 +465,7 @@ def main() -> int:
             s.run(1)
             host[:] = s.get_state()
         t_e2e = time.perf_counter() - t0
-        te = torch.tensor([t_e2e], device="cuda", dtype=torch.float64)
-        if dist is not None:
-            dist.all_reduce(te, op=dist.ReduceOp.MAX)
-        e2e_value = world * n * nrk * args.e2e_steps / float(te.item())
+        e2e_value = replica_throughput(world, n, nrk, args.e2e_steps, max_over_ranks(t_e2e, dist))
         s.close()
 
         bytes_stage = algorithmic_bytes_per_stage(m, venk=True)
