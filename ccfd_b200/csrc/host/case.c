@@ -318,11 +318,14 @@ int ccfd_case_load_text(const char *text, const char *base_dir, ccfd_case **out)
 		char full[520];
 		snprintf(full, sizeof(full), "%s%s", file, fmt);
 		dir_join(base_dir, full, path, sizeof(path));
-		if (strcmp(fmt, ".msh") && strcmp(fmt, ".msh2") && strcmp(fmt, ".msh4")) {
-			st = CCFD_ERR_UNSUPPORTED; /* EMC2 / CGNS readers are not built */
+		if (!strcmp(fmt, ".mesh")) {
+			TRY(ccfd_read_emc2(path, &nodes, &nn, &tria, &nt, &quad, &nq, &bcedge, &nb));
+		} else if (strcmp(fmt, ".msh") && strcmp(fmt, ".msh2") && strcmp(fmt, ".msh4")) {
+			st = CCFD_ERR_UNSUPPORTED; /* the CGNS reader needs the CGNS library */
 			goto fail;
+		} else {
+			TRY(ccfd_read_gmsh(path, &nodes, &nn, &tria, &nt, &quad, &nq, &bcedge, &nb));
 		}
-		TRY(ccfd_read_gmsh(path, &nodes, &nn, &tria, &nt, &quad, &nq, &bcedge, &nb));
 	} else if (lv == 1) {
 		ccfd_cart cart;
 		memset(&cart, 0, sizeof(cart));

@@ -23,8 +23,8 @@
  *     matched boundary faces into interior faces before the least-squares
  *     weights are formed.
  *
- * Also here: the Cartesian generator (src/mesh.c:385-486) and a gmsh 2.2
- * reader / writer (the format src/mesh.c:498-742 reads).
+ * Also here: the Cartesian generator (src/mesh.c:385-486), the gmsh 2.2,
+ * gmsh 4 and EMC2 readers (src/mesh.c:498-1139) and a gmsh 2.2 writer.
  */
 #include <math.h>
 #include <stdio.h>
@@ -711,6 +711,185 @@ int ccfd_write_gmsh2(const char *path, const double *nodes, long n_nodes,
  * line elements whose first tag (physical group) is > 100 are BC edges with
  * that code, triangles / quads carry their physical group as the domain;
  * other elements are ignored.  gmsh 4 files are not read. */
+/* gmsh 4 as the reference reads it (readGmsh, src/mesh.c:743-983): the
+ * physical tag of every curve entity that has one, in $Entities order;
+ * nodes by entity blocks (tags must run 1..n); element blocks of lines
+ * (boundary edges whose BC code is the physical tag at the block's own
+ * index), triangles and quadrilaterals (domain 1); lines of blocks of other
+ * element types are not consumed, as there. */
+static int read_gmsh4(FILE *f, double **nodes_out, long *n_nodes, long **tria_out, long *n_tria,
+		      long **quad_out, long *n_quad, long **bc_out, long *n_bc)
+{
+	char line[8192];
+	long np = -1, nc = 0;
+	int st = CCFD_OK;
+	int *ptag = NULL;
+	long nptag = 0, nv = 0, ne = 0, nb = 0, nt = 0, nq = 0;
+	double *nodes = NULL;
+	long *tria = NULL, *quad = NULL, *bc = NULL;
+	rewind(f);
+	while (fgets(line, sizeof(line), f))
+		if (!strcmp(line, "$Entities\n")) {
+			if (!fgets(line, sizeof(line), f) || sscanf(line, "%ld %ld", &np, &nc) != 2)
+				return CCFD_ERR_MESH;
+			break;
+		}
+	if (np < 0 || nc <= 0)
+		return CCFD_ERR_MESH; /* "No curves in mesh file" */
+	ptag = malloc(sizeof(int) * nc);
+	if (!ptag)
+		return CCFD_ERR_NOMEM;
+	for (long l = 0; l < np; ++l)
+		if (!fgets(line, sizeof(line), f)) {
+			st = CCFD_ERR_MESH;
+			goto out;
+		}
+	for (long l = 0; l < nc; ++l) {
+		if (!fgets(line, sizeof(line), f)) {
+			st = CCFD_ERR_MESH;
+			goto out;
+		}
+		char *save = NULL, *tok = strtok_r(line, " ", &save);
+		for (int k = 0; k < 7 && tok; ++k)
+			tok = strtok_r(NULL, " ", &save);
+		if (!tok) {
+			st = CCFD_ERR_MESH;
+			goto out;
+		}
+		if (strtol(tok, NULL, 10)) {
+			tok = strtok_r(NULL, " ", &save);
+			if (!tok) {
+				st = CCFD_ERR_MESH;
+				goto out;
+			}
+			ptag[nptag++] = (int)strtol(tok, NULL, 10);
+		}
+	}
+	int nblk = 0;
+	rewind(f);
+	while (fgets(line, sizeof(line), f))
+		if (!strcmp(line, "$Nodes\n")) {
+			if (!fgets(line, sizeof(line), f) || sscanf(line, "%d %ld", &nblk, &nv) != 2)
+				nv = 0;
+			break;
+		}
+	if (nv <= 0) {
+		st = CCFD_ERR_MESH; /* "No Nodes in Mesh file" */
+		goto out;
+	}
+	nodes = malloc(sizeof(double) * 2 * nv);
+	long *ids = malloc(sizeof(long) * nv);
+	if (!nodes || !ids) {
+		free(ids);
+		st = CCFD_ERR_NOMEM;
+		goto out;
+	}
+	long iv = 0, iid = 0;
+	for (int e = 0; e < nblk && st == CCFD_OK; ++e) {
+		long nin = 0;
+		if (!fgets(line, sizeof(line), f) || sscanf(line, "%*d %*d %*d %ld", &nin) != 1 ||
+		    nin < 0 || iid + nin > nv) {
+			st = CCFD_ERR_MESH;
+			break;
+		}
+		for (long i = 0; i < nin && st == CCFD_OK; ++i)
+			if (!fgets(line, sizeof(line), f) || sscanf(line, "%ld", &ids[iid++]) != 1)
+				st = CCFD_ERR_MESH;
+		for (long i = 0; i < nin && st == CCFD_OK; ++i) {
+			double x, y;
+			if (!fgets(line, sizeof(line), f) || sscanf(line, "%lg %lg", &x, &y) != 2 ||
+			    ids[iv] != iv + 1) {
+				st = CCFD_ERR_MESH; /* "NodeID does not match Node Position" */
+				break;
+			}
+			nodes[2 * iv] = x;
+			nodes[2 * iv + 1] = y;
+			iv++;
+		}
+	}
+	free(ids);
+	if (st != CCFD_OK)
+		goto out;
+	rewind(f);
+	while (fgets(line, sizeof(line), f))
+		if (!strcmp(line, "$Elements\n")) {
+			if (!fgets(line, sizeof(line), f) || sscanf(line, "%d %ld", &nblk, &ne) != 2)
+				ne = 0;
+			break;
+		}
+	if (ne <= 0) {
+		st = CCFD_ERR_MESH; /* "No Elements in Mesh file" */
+		goto out;
+	}
+	tria = malloc(sizeof(long) * 4 * ne);
+	quad = malloc(sizeof(long) * 5 * ne);
+	bc = malloc(sizeof(long) * 3 * ne);
+	if (!tria || !quad || !bc) {
+		st = CCFD_ERR_NOMEM;
+		goto out;
+	}
+	for (int e = 0; e < nblk && st == CCFD_OK; ++e) {
+		int type = 0;
+		long nin = 0;
+		if (!fgets(line, sizeof(line), f) || sscanf(line, "%*d %*d %d %ld", &type, &nin) != 2 || nin < 0) {
+			st = CCFD_ERR_MESH;
+			break;
+		}
+		if (type < 1 || type > 3)
+			continue;
+		if ((type == 1 && e >= nptag) || nb + nt + nq + nin > ne) {
+			st = CCFD_ERR_MESH;
+			break;
+		}
+		for (long i = 0; i < nin; ++i) {
+			long a[4];
+			int want = type + 1, got;
+			if (!fgets(line, sizeof(line), f)) {
+				st = CCFD_ERR_MESH;
+				break;
+			}
+			got = sscanf(line, "%*d %ld %ld %ld %ld", &a[0], &a[1], &a[2], &a[3]);
+			if (got < want) {
+				st = CCFD_ERR_MESH;
+				break;
+			}
+			if (type == 1) {
+				bc[3 * nb] = a[0] - 1;
+				bc[3 * nb + 1] = a[1] - 1;
+				bc[3 * nb + 2] = ptag[e];
+				nb++;
+			} else if (type == 2) {
+				for (int k = 0; k < 3; ++k)
+					tria[4 * nt + k] = a[k] - 1;
+				tria[4 * nt + 3] = 1;
+				nt++;
+			} else {
+				for (int k = 0; k < 4; ++k)
+					quad[5 * nq + k] = a[k] - 1;
+				quad[5 * nq + 4] = 1;
+				nq++;
+			}
+		}
+	}
+	if (st == CCFD_OK && nt + nq == 0)
+		st = CCFD_ERR_MESH;
+out:
+	free(ptag);
+	if (st != CCFD_OK) {
+		free(nodes); free(tria); free(quad); free(bc);
+		return st;
+	}
+	*nodes_out = nodes;
+	*n_nodes = nv;
+	*tria_out = tria;
+	*n_tria = nt;
+	*quad_out = quad;
+	*n_quad = nq;
+	*bc_out = bc;
+	*n_bc = nb;
+	return CCFD_OK;
+}
+
 int ccfd_read_gmsh(const char *path, double **nodes_out, long *n_nodes,
 		   long **tria_out, long *n_tria, long **quad_out, long *n_quad,
 		   long **bc_out, long *n_bc)
@@ -733,8 +912,14 @@ int ccfd_read_gmsh(const char *path, double **nodes_out, long *n_nodes,
 				goto out;
 			}
 			fmt = (int)v;
+			if (fmt == 4) {
+				st = read_gmsh4(f, nodes_out, n_nodes, tria_out, n_tria, quad_out, n_quad,
+						bc_out, n_bc);
+				fclose(f);
+				return st;
+			}
 			if (fmt != 2) {
-				st = CCFD_ERR_UNSUPPORTED;
+				st = CCFD_ERR_MESH; /* "Wrong gmsh Mesh Format" */
 				goto out;
 			}
 		} else if (!strcmp(line, "$Nodes\n")) {
@@ -808,6 +993,132 @@ int ccfd_read_gmsh(const char *path, double **nodes_out, long *n_nodes,
 		}
 	}
 	if (!nodes || (nt + nq) == 0)
+		st = CCFD_ERR_MESH;
+out:
+	fclose(f);
+	if (st != CCFD_OK) {
+		free(nodes); free(tria); free(quad); free(bc);
+		return st;
+	}
+	*nodes_out = nodes;
+	*n_nodes = nv;
+	*tria_out = tria;
+	*n_tria = nt;
+	*quad_out = quad;
+	*n_quad = nq;
+	*bc_out = bc;
+	*n_bc = nb;
+	return CCFD_OK;
+}
+
+/* ------------------------------------------------------------ EMC2 */
+/* next line of f that contains `key`, scanning from the start and stopping at
+ * a line with "End" (the section search of readEMC2); the count on the line
+ * after it, or -1 */
+static long emc2_section(FILE *f, const char *key, char *line, size_t n)
+{
+	rewind(f);
+	while (fgets(line, (int)n, f)) {
+		if (strstr(line, key)) {
+			long c = -1;
+			if (!fgets(line, (int)n, f) || sscanf(line, "%ld", &c) != 1)
+				return -1;
+			return c;
+		} else if (strstr(line, "End")) {
+			break;
+		}
+	}
+	return -1;
+}
+
+int ccfd_read_emc2(const char *path, double **nodes_out, long *n_nodes,
+		   long **tria_out, long *n_tria, long **quad_out, long *n_quad,
+		   long **bc_out, long *n_bc)
+{
+	/* readEMC2, src/mesh.c:1004-1139: Vertices (x y), Edges (a b ref;
+	 * ref 0 is not a boundary edge and is dropped), Triangles (a b c ref),
+	 * Quadrangles (a b c d ref); the element reference is its domain */
+	FILE *f = fopen(path, "r");
+	if (!f)
+		return CCFD_ERR_MESH; /* "Could not find Mesh File" */
+	char line[1024];
+	int st = CCFD_OK;
+	double *nodes = NULL;
+	long *tria = NULL, *quad = NULL, *bc = NULL;
+	long nv = emc2_section(f, "Vertices", line, sizeof(line)), ne = 0, nb = 0, nt = 0, nq = 0;
+	if (nv <= 0) {
+		st = CCFD_ERR_MESH;
+		goto out;
+	}
+	nodes = malloc(sizeof(double) * 2 * nv);
+	if (!nodes) {
+		st = CCFD_ERR_NOMEM;
+		goto out;
+	}
+	for (long i = 0; i < nv; ++i)
+		if (!fgets(line, sizeof(line), f) || sscanf(line, "%lg %lg", &nodes[2 * i], &nodes[2 * i + 1]) != 2) {
+			st = CCFD_ERR_MESH;
+			goto out;
+		}
+	ne = emc2_section(f, "Edges", line, sizeof(line));
+	if (ne < 0)
+		ne = 0;
+	bc = malloc(sizeof(long) * 3 * (ne > 0 ? ne : 1));
+	if (!bc) {
+		st = CCFD_ERR_NOMEM;
+		goto out;
+	}
+	for (long i = 0; i < ne; ++i) {
+		long a, b, r;
+		if (!fgets(line, sizeof(line), f) || sscanf(line, "%ld %ld %ld", &a, &b, &r) != 3) {
+			st = CCFD_ERR_MESH;
+			goto out;
+		}
+		if (r != 0) {
+			bc[3 * nb] = a - 1;
+			bc[3 * nb + 1] = b - 1;
+			bc[3 * nb + 2] = r;
+			nb++;
+		}
+	}
+	nt = emc2_section(f, "Triangles", line, sizeof(line));
+	if (nt < 0)
+		nt = 0;
+	tria = malloc(sizeof(long) * 4 * (nt > 0 ? nt : 1));
+	if (!tria) {
+		st = CCFD_ERR_NOMEM;
+		goto out;
+	}
+	for (long i = 0; i < nt; ++i) {
+		long a[4];
+		if (!fgets(line, sizeof(line), f) || sscanf(line, "%ld %ld %ld %ld", &a[0], &a[1], &a[2], &a[3]) != 4) {
+			st = CCFD_ERR_MESH;
+			goto out;
+		}
+		for (int k = 0; k < 3; ++k)
+			tria[4 * i + k] = a[k] - 1;
+		tria[4 * i + 3] = a[3];
+	}
+	nq = emc2_section(f, "Quadrangles", line, sizeof(line));
+	if (nq < 0)
+		nq = 0;
+	quad = malloc(sizeof(long) * 5 * (nq > 0 ? nq : 1));
+	if (!quad) {
+		st = CCFD_ERR_NOMEM;
+		goto out;
+	}
+	for (long i = 0; i < nq; ++i) {
+		long a[5];
+		if (!fgets(line, sizeof(line), f) ||
+		    sscanf(line, "%ld %ld %ld %ld %ld", &a[0], &a[1], &a[2], &a[3], &a[4]) != 5) {
+			st = CCFD_ERR_MESH;
+			goto out;
+		}
+		for (int k = 0; k < 4; ++k)
+			quad[5 * i + k] = a[k] - 1;
+		quad[5 * i + 4] = a[4];
+	}
+	if (nt + nq == 0)
 		st = CCFD_ERR_MESH;
 out:
 	fclose(f);

@@ -47,6 +47,63 @@ class RawMesh:
         return path
 
 
+def write_gmsh4(mesh: "RawMesh", path: str) -> str:
+    """Write a mesh as gmsh 4.1 ASCII in the layout the reference's gmsh 4
+    reader expects (src/mesh.c:743-983): one curve entity per boundary code
+    with that code as its physical tag, the boundary line blocks first and
+    in the same order, then one triangle and one quadrilateral block (the
+    reference gives cells domain 1 in this format)."""
+    codes = sorted(set(int(c) for c in mesh.bc[:, 2]))
+    nv = len(mesh.nodes)
+    blocks = [(1, k + 1, 1, mesh.bc[mesh.bc[:, 2] == c][:, :2]) for k, c in enumerate(codes)]
+    if len(mesh.tria):
+        blocks.append((2, 1, 2, mesh.tria[:, :3]))
+    if len(mesh.quad):
+        blocks.append((2, 1, 3, mesh.quad[:, :4]))
+    n_el = sum(len(b[3]) for b in blocks)
+    out = ["$MeshFormat", "4.1 0 8", "$EndMeshFormat", "$Entities", f"0 {len(codes)} 1 0"]
+    for k, c in enumerate(codes):
+        out.append(f"{k + 1} 0 0 0 0 0 0 1 {c} 0")
+    out.append("1 0 0 0 0 0 0 0 0")
+    out += ["$EndEntities", "$Nodes", f"1 {nv} 1 {nv}", f"2 1 0 {nv}"]
+    out += [str(i + 1) for i in range(nv)]
+    out += [f"{x!r} {y!r} 0" for x, y in mesh.nodes.tolist()]
+    out += ["$EndNodes", "$Elements", f"{len(blocks)} {n_el} 1 {n_el}"]
+    tag = 1
+    for dim, ent, typ, conn in blocks:
+        out.append(f"{dim} {ent} {typ} {len(conn)}")
+        for row in conn.tolist():
+            out.append(" ".join([str(tag)] + [str(v + 1) for v in row]))
+            tag += 1
+    out += ["$EndElements", ""]
+    with open(path, "w") as f:
+        f.write("\n".join(out))
+    return path
+
+
+def write_emc2(mesh: "RawMesh", path: str, interior_edges: int = 0) -> str:
+    """Write a mesh in the EMC2 format the reference reads (readEMC2,
+    src/mesh.c:1004-1139): boundary edges carry their BC code, elements
+    their domain; ``interior_edges`` edges of the first triangles are added
+    with reference 0 (not boundary edges, dropped by the reader)."""
+    out = ["MeshVersionFormatted 1", "", "Dimension 2", "", "Vertices", str(len(mesh.nodes))]
+    out += [f"{x!r} {y!r} 0" for x, y in mesh.nodes.tolist()]
+    extra = [(int(t[0]), int(t[1])) for t in mesh.tria[:interior_edges]]
+    out += ["", "Edges", str(len(mesh.bc) + len(extra))]
+    out += [f"{a + 1} {b + 1} {c}" for a, b, c in mesh.bc.tolist()]
+    out += [f"{a + 1} {b + 1} 0" for a, b in extra]
+    if len(mesh.tria):
+        out += ["", "Triangles", str(len(mesh.tria))]
+        out += [" ".join(str(v + 1) for v in row[:3]) + f" {row[3]}" for row in mesh.tria.tolist()]
+    if len(mesh.quad):
+        out += ["", "Quadrangles", str(len(mesh.quad))]
+        out += [" ".join(str(v + 1) for v in row[:4]) + f" {row[4]}" for row in mesh.quad.tolist()]
+    out += ["", "End", ""]
+    with open(path, "w") as f:
+        f.write("\n".join(out))
+    return path
+
+
 def _grid_nodes(nx, ny, x0, x1, y0, y1):
     xs = np.linspace(x0, x1, nx + 1)
     ys = np.linspace(y0, y1, ny + 1)

@@ -222,8 +222,16 @@ int ccfd_locate_points(const ccfd_mesh *m, const double *xy, int n, long *cells_
 int ccfd_write_gmsh2(const char *path, const double *nodes, long n_nodes,
 		     const long *tria, long n_tria, const long *quad, long n_quad,
 		     const long *bc_edge, long n_bc_edge);
-/* Read a gmsh 2.2 / 4.1 ASCII mesh into raw arrays (caller frees with free()). */
+/* Read a gmsh 2.2 or 4 ASCII mesh into raw arrays as readGmsh does
+ * (src/mesh.c:498-983; gmsh 4: boundary codes are the curves' physical
+ * tags, cells domain 1); the caller frees them with free(). */
 int ccfd_read_gmsh(const char *path, double **nodes, long *n_nodes,
+		   long **tria, long *n_tria, long **quad, long *n_quad,
+		   long **bc_edge, long *n_bc_edge);
+/* Read an EMC2 (.mesh) mesh as readEMC2 does (src/mesh.c:1004-1139):
+ * edges with reference 0 are not boundary edges; element references are
+ * their domains.  Same outputs as ccfd_read_gmsh. */
+int ccfd_read_emc2(const char *path, double **nodes, long *n_nodes,
 		   long **tria, long *n_tria, long **quad, long *n_quad,
 		   long **bc_edge, long *n_bc_edge);
 const char *ccfd_strerror(int status);

@@ -64,7 +64,8 @@ def test_oracle_bit_identical_to_live_reference(key):
 
 
 @pytest.mark.skipif(not refdump.have_ref(), reason="compiled reference not built")
-@pytest.mark.parametrize("kind", ["dmr", "periodic_gmsh", "periodic_cartesian"])
+@pytest.mark.parametrize("kind", ["dmr", "periodic_gmsh", "periodic_cartesian", "periodic_gmsh4", "dmr_gmsh4",
+                                  "sine_emc2", "riemann_emc2"])
 def test_mesh_builder_bit_identical_to_reference(kind):
     from ccfd_b200 import meshgen
     with tempfile.TemporaryDirectory() as tmp:
@@ -78,12 +79,37 @@ def test_mesh_builder_bit_identical_to_reference(kind):
             meshgen.sinewave_mesh(7, periodic=True).write_gmsh(os.path.join(tmp, "sine.msh"))
             ini = meshgen.sinewave_ini("sine", periodic=True)
             files = {"sine.msh": os.path.join(tmp, "sine.msh")}
+        elif kind == "periodic_gmsh4":
+            # gmsh 4 (readGmsh, src/mesh.c:743-983): BC codes from the
+            # curves' physical tags
+            meshgen.write_gmsh4(meshgen.sinewave_mesh(7, periodic=True), os.path.join(tmp, "sine.msh4"))
+            ini = meshgen.sinewave_ini("sine", periodic=True).replace("meshFormat = .msh\n",
+                                                                     "meshFormat = .msh4\n")
+            files = {"sine.msh4": os.path.join(tmp, "sine.msh4")}
+        elif kind == "dmr_gmsh4":
+            meshgen.write_gmsh4(meshgen.dmr_mesh(30, 8, seed=5), os.path.join(tmp, "dmr.msh4"))
+            ini = meshgen.dmr_ini("dmr").replace("meshFormat = .msh\n", "meshFormat = .msh4\n")
+            files = {"dmr.msh4": os.path.join(tmp, "dmr.msh4")}
+        elif kind == "sine_emc2":
+            # EMC2 (readEMC2, src/mesh.c:1004-1139), with interior edges of
+            # reference 0 that the reader drops
+            meshgen.write_emc2(meshgen.sinewave_mesh(7, periodic=True), os.path.join(tmp, "sine.mesh"),
+                               interior_edges=5)
+            ini = meshgen.sinewave_ini("sine", periodic=True).replace("meshFormat = .msh\n",
+                                                                     "meshFormat = .mesh\n")
+            files = {"sine.mesh": os.path.join(tmp, "sine.mesh")}
+        elif kind == "riemann_emc2":
+            # four quadrant domains from the element references
+            meshgen.write_emc2(meshgen.riemann2d_mesh(12), os.path.join(tmp, "rm.mesh"))
+            states = [(1.0, 0.1, 0.0, 1.0), (0.5, 0.0, 0.2, 0.4), (0.8, -0.3, 0.0, 0.6), (1.2, 0.0, -0.1, 1.1)]
+            ini = meshgen.riemann2d_ini("rm", states).replace("meshFormat = .msh\n", "meshFormat = .mesh\n")
+            files = {"rm.mesh": os.path.join(tmp, "rm.mesh")}
         else:
             ini = meshgen.sinewave_ini(None, n=9, periodic=True)
         case = cc.CaseData.from_text(ini, tmp)
         d = refdump.run_ref(ini, "mesh", files=files)
     M = case.mesh()
-    if kind != "dmr":
+    if kind.startswith("periodic"):
         assert M["n_bc"] == 0 and M["n_faces"] == len(d["face_sides"]) // 4
     hs = d["hs_geo"].reshape(-1, 12)
     fs = d["face_sides"].reshape(-1, 4)
