@@ -32,6 +32,10 @@ def _specs():
         "zoo_ausmd_bj_rk4": {"mesh": None,
                              "ini": CASES.zoo_ini(9, 2, 1).replace("nRKstages = 3", "nRKstages = 4"),
                              "eqn": "euler"},
+        # manufactured source term on a periodic mesh and on a mixed mesh
+        # with the exact-solution boundary
+        "sine_periodic_src": dict(CASES.run_cases()["sine_periodic_run"]),
+        "sine_ns_src": dict(CASES.run_cases()["sine_ns_run"]),
     }
 
 
