@@ -102,6 +102,18 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
+def workload_config(n: int, faces: int, world: int) -> dict:
+    """The `config` object of the JSON line (both arms)."""
+    return {
+        "workload": f"double Mach reflection, {n} jittered triangles ({NX}x{NY} quads "
+                    "split, seed 20260001), HLLC, Venkatakrishnan K=5, RK3 (timeOrder 2), "
+                    "CFL 0.8, FP64",
+        "cells": n, "faces": faces, "rk_stages": 3,
+        "parallelism": f"replicas x{world}",
+        "l2": "inputs larger than L2 (working set > 126 MB), no flush",
+    }
+
+
 def max_over_ranks(x: float, dist) -> float:
     """The largest value of x over the ranks (the job's time is its slowest
     rank's); a plain return without a process group."""
@@ -376,8 +388,7 @@ def run_reference_arm(args, rank: int, world: int) -> None:
             "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": 1e3 * t / args.steps, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": f"double Mach reflection, {n} jittered triangles "
-                                   f"({NX}x{NY} quads split), HLLC, Venkatakrishnan K=5, RK3, CFL 0.8"},
+            "config": workload_config(n, case.c.mesh.n_faces, world),
             "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": kind,
                              "sample": f"{args.warmup} warm-up + {args.steps} timed RK3 steps of the "
                                        "full 500k-cell workload (reference's own time loop, "
@@ -508,14 +519,7 @@ def main() -> int:
             "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": t_ms / max(steps_done, 1), "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {
-                "workload": f"double Mach reflection, {n} jittered triangles ({NX}x{NY} quads "
-                            "split, seed 20260001), HLLC, Venkatakrishnan K=5, RK3 (timeOrder 2), "
-                            "CFL 0.8, FP64",
-                "cells": n, "faces": m["n_faces"], "rk_stages": nrk,
-                "parallelism": f"replicas x{world}",
-                "l2": "inputs larger than L2 (working set > 126 MB), no flush",
-            },
+            "config": workload_config(n, m["n_faces"], world),
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm_peak,
                          "unit": "GB/s", "frac": achieved / hbm_peak,
                          "traffic": STAGE_TRAFFIC_BYTES if (NX, NY) == (1000, 250) else None,
