@@ -197,3 +197,65 @@ def test_driver_prints_error_analysis():
     assert set(rows) == {"L1  ", "L2  ", "Linf"}
     np.testing.assert_allclose(rows["L1  "], e["L1"], rtol=6e-6)
     np.testing.assert_allclose(rows["Linf"], e["Linf"], rtol=6e-6)
+
+
+@pytest.mark.parametrize("shape", ["one_triangle", "one_quad", "two_cells"])
+def test_tiny_meshes_match_oracle(shape):
+    # degenerate sizes: a single cell (every face a boundary face, a tile
+    # without rings) and two cells sharing one face
+    nodes = np.array([[0.0, 0.0], [1.0, 0.0], [1.0, 1.0], [0.0, 1.0]])
+    if shape == "one_triangle":
+        mesh = meshgen.RawMesh(nodes[:3], tria=[[0, 1, 2, 1]], bc=[[0, 1, 301], [1, 2, 401], [2, 0, 101]])
+    elif shape == "one_quad":
+        mesh = meshgen.RawMesh(nodes, quad=[[0, 1, 2, 3, 1]],
+                               bc=[[0, 1, 101], [1, 2, 401], [2, 3, 101], [3, 0, 301]])
+    else:
+        mesh = meshgen.RawMesh(nodes, tria=[[0, 1, 2, 1], [0, 2, 3, 1]],
+                               bc=[[0, 1, 101], [1, 2, 401], [2, 3, 101], [3, 0, 301]])
+    ini = """meshType = 0
+meshFormat = .msh
+meshFile = tiny
+nBC = 3
+BCtype = 101
+BCtype = 301
+rho = 1.2
+mach = 0.4
+alpha = 10.0
+pressure = 1.1
+BCtype = 401
+icType = 1
+nDomains = 1
+domainID = 1
+rho = 1.0
+mach = 0.3
+alpha = 20.0
+pressure = 1.0
+fluxFunction = 5
+spatialOrder = 2
+limiter = 2
+venk_k = 5.0
+timeOrder = 2
+nRKstages = 3
+CFL = 0.5
+stationary = F
+tEnd = 10.0
+maxIter = 100000
+fileName = tiny
+IOtimeInterval = 10.0
+IOiterInterval = 100000000
+outputFormat = 3
+"""
+    with tempfile.TemporaryDirectory() as tmp:
+        mesh.write_gmsh(os.path.join(tmp, "tiny.msh"))
+        case = cc.CaseData.from_text(ini, tmp)
+    s = cc.Solver(case)
+    ut = s.fv_time_derivative(0.0)
+    uo = restated.residual(case, case.prim0(), 0.0)
+    assert rel_max_err(ut, uo) <= RES_TOL
+    rep = s.run(5)
+    prim = s.get_state()
+    s.close()
+    po, info = restated.run_explicit(case, nsteps=5)
+    assert rep["iterations"] == info["iterations"] == 5
+    l1, linf = l1_linf(prim, po)
+    assert l1 <= RUN_TOL and linf <= RUN_TOL
