@@ -29,6 +29,9 @@
 
 #include <cuda_runtime.h>
 
+#include <atomic>
+#include <mutex>
+
 #include "kernels.cuh"
 
 namespace ccfd {
@@ -37,6 +40,27 @@ namespace ccfd {
 // run 384 threads, 2 CTAs per SM (gradient cells and faces of a 256-cell
 // tile in about one pass each); the FP32 kernels need half the shared
 // memory and run 256 threads, 3 CTAs per SM.
+// Dynamic shared memory limit of one kernel, raised as launches need more:
+// per device, only ever raised, and safe when host threads (the lockstep
+// implicit sets, several serving contexts) launch the same kernel at once.
+struct SmemLimit {
+    std::mutex mu;
+    std::atomic<int> bytes[64];
+    SmemLimit() {
+        for (auto& b : bytes) b.store(0);
+    }
+    template <typename K>
+    void ensure(K kern, int smem) {
+        int dev = 0;
+        if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return;
+        if (bytes[dev].load(std::memory_order_acquire) >= smem) return;
+        std::lock_guard<std::mutex> lk(mu);
+        if (bytes[dev].load(std::memory_order_relaxed) >= smem) return;
+        if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem) == cudaSuccess)
+            bytes[dev].store(smem, std::memory_order_release);
+    }
+};
+
 template <typename FT> struct StageShape;
 template <> struct StageShape<double> { static constexpr int threads = 384, min_blocks = 2; };
 template <> struct StageShape<float> { static constexpr int threads = 256, min_blocks = 3; };
