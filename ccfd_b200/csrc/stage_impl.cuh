@@ -463,6 +463,9 @@ __device__ __forceinline__ void stage_body(const StageLaunch& L, const int t) {
     const int4 cnt = T.counts[t];
     const int nT = cnt.x, nG = cnt.y, nEc = cnt.z, nE = cnt.w;
     const int e0 = T.e_off[t];
+    // the tile's own cells are consecutive device cells (staged entries
+    // 0..nT-1): their indices need no lookup
+    const int d_first = T.e_ref[e0];
     const double time = stage_time(L.ctrl, L.tfix, L.a_time);
     V4* ps = reinterpret_cast<V4*>(smem);             // [max_e] states
     V4* gs = ps + T.max_e;                            // [2 max_g] gradients
@@ -474,7 +477,7 @@ __device__ __forceinline__ void stage_body(const StageLaunch& L, const int t) {
     // reads back in D (same cell-to-thread mapping)
     if (m.cell_src)
         for (int i = tid; i < nT; i += kThreads) {
-            const int d = T.e_ref[e0 + i];
+            const int d = d_first + i;
             m.src_buf[d] = cell_source(P, m.hs_gw, m.hs_off[d], m.hs_off[d + 1], m.cell_src[d],
                                        m.cell_geo[d].x, time);
         }
@@ -483,7 +486,8 @@ __device__ __forceinline__ void stage_body(const StageLaunch& L, const int t) {
     // boundary state at their mirrored barycentre (second order only: the
     // reference sets ghost cell states in its second-order reconstruction
     // and leaves them zero otherwise)
-    for (int e = tid; e < nEc; e += kThreads) ps[e] = cvt4<FT>(L.prim_in[T.e_ref[e0 + e]]);
+    for (int e = tid; e < nEc; e += kThreads)
+        ps[e] = cvt4<FT>(L.prim_in[e < nT ? d_first + e : T.e_ref[e0 + e]]);
     for (int e = nEc + tid; e < nE; e += kThreads) {
         int g = -1 - T.e_ref[e0 + e];
         double4 gq = make_double4(0.0, 0.0, 0.0, 0.0);
@@ -498,7 +502,7 @@ __device__ __forceinline__ void stage_body(const StageLaunch& L, const int t) {
     const int hb = T.hs_off[t], gb = T.gl_off[t];
     if (ORDER == 2) {
         for (int i = tid; i < nG; i += kThreads) {
-            int d = T.e_ref[e0 + i];
+            int d = i < nT ? d_first + i : T.e_ref[e0 + i];
             int h0 = m.hs_off[d], nh = m.hs_off[d + 1] - h0;
             int lo = T.hs_loc[gb + i];
             FT q[4], ux[4], uy[4];
@@ -576,7 +580,7 @@ __device__ __forceinline__ void stage_body(const StageLaunch& L, const int t) {
     int bad = 0;
     const bool rk = L.mode == 1;
     for (int i = tid; i < nT; i += kThreads) {
-        int d = T.e_ref[e0 + i];
+        int d = d_first + i;
         int h0 = m.hs_off[d], h1 = m.hs_off[d + 1];
         double s[4] = {0.0, 0.0, 0.0, 0.0};
         for (int h = h0; h < h1; ++h) {
