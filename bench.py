@@ -528,7 +528,7 @@ def main() -> int:
                          "bytes_per_launch": bytes_stage, "avg_ms": avg_res_ms,
                          "peak_source": peak_src},
             "e2e": {"value": e2e_value, "unit": UNIT,
-                    "h2d_bytes_per_step": 2 * n * 4 * 8, "d2h_bytes_per_step": n * 4 * 8},
+                    "h2d_bytes_per_step": n * 4 * 8, "d2h_bytes_per_step": n * 4 * 8},
             "gpu_launches": int(steps_done * nrk + 2),
             "clocks": clk,
             "cpu_baseline": cpu,

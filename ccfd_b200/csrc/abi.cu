@@ -498,7 +498,9 @@ extern "C" int ccfd_upload_case(ccfd_ctx* ctx, const ccfd_mesh* m, const ccfd_bc
     // state and scratch
     ctx->nb_cells = (int)((N + 255) / 256);
     ctx->nb_part = std::max(ctx->nb_cells, ts.n_tiles);
-    if ((st = dalloc(ctx, &ctx->prim_buf[0], N)) || (st = dalloc(ctx, &ctx->prim_buf[1], N)) ||
+    if ((st = dupload_c(ctx, &ctx->d_cell_of_dev, ctx->cell_of_dev)) ||
+        (st = dupload_c(ctx, &ctx->d_dev_of_cell, ctx->dev_of_cell)) || (st = dalloc(ctx, &ctx->xfer, N)) ||
+        (st = dalloc(ctx, &ctx->prim_buf[0], N)) || (st = dalloc(ctx, &ctx->prim_buf[1], N)) ||
         (st = dalloc(ctx, &ctx->cons0, N)) || (st = dalloc(ctx, &ctx->u_t, N)) ||
         (st = dalloc(ctx, &ctx->grad, 2 * N)) || (st = dalloc(ctx, &ctx->ticket, 1)) ||
         (st = dalloc(ctx, &ctx->ghost_pface, B + 1)) ||
@@ -605,36 +607,43 @@ static double4* cur_prim(ccfd_ctx* ctx) {
     return ctx->prim_buf[ctx->batch ? ctx->h_ctrl->par : ctx->cur];
 }
 
+// State transfers move the caller's array as it is (reference cell order)
+// and permute / convert on the device: a pinned caller buffer goes by DMA
+// at full speed, and no host loop touches the cells.
+__global__ void k_state_in(int n, const double4* __restrict__ src, const int* __restrict__ cell_of_dev,
+                           int conservative, double gam1, double gam1q, double4* __restrict__ prim,
+                           double4* __restrict__ cons) {
+    const int d = blockIdx.x * blockDim.x + threadIdx.x;
+    if (d >= n) return;
+    const double4 v = src[cell_of_dev[d]];
+    double a[4] = {v.x, v.y, v.z, v.w}, pv[4], cv[4];
+    if (conservative) {
+        for (int k = 0; k < 4; ++k) cv[k] = a[k];
+        cons_prim(gam1, cv, pv);
+    } else {
+        for (int k = 0; k < 4; ++k) pv[k] = a[k];
+        prim_cons(gam1q, pv, cv);
+    }
+    prim[d] = make_double4(pv[0], pv[1], pv[2], pv[3]);
+    cons[d] = make_double4(cv[0], cv[1], cv[2], cv[3]);
+}
+
+__global__ void k_state_out(int n, const double4* __restrict__ src, const int* __restrict__ dev_of_cell,
+                            double4* __restrict__ dst) {
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c < n) dst[c] = src[dev_of_cell[c]];
+}
+
 extern "C" int ccfd_set_state(ccfd_ctx* ctx, const double* state, int kind) {
     if (!ctx || !state || !ctx->uploaded) return CCFD_ERR_ARG;
     if (ctx->batch) return CCFD_ERR_BUSY;
     CK(cudaSetDevice(ctx->device));
     const long N = ctx->N;
-    // (thread_local staging reached through references: the worker threads
-    // of par_for must use this thread's buffers, not their own)
-    static thread_local std::vector<double4> tl_prim, tl_cons;
-    std::vector<double4>& prim = tl_prim;
-    std::vector<double4>& cons = tl_cons;
-    prim.resize(N);
-    cons.resize(N);
-    double gam1 = ctx->phys.gam1, gam1q = ctx->phys.gam1q;
-    par_for(N, [&](long d0, long d1) {
-        for (long d = d0; d < d1; ++d) {
-            const double* s = &state[4 * ctx->cell_of_dev[d]];
-            double pv[4], cv[4];
-            if (kind == CCFD_CONSERVATIVE) {
-                memcpy(cv, s, sizeof(cv));
-                ccfd_host_cons_prim(gam1, cv, pv);
-            } else {
-                memcpy(pv, s, sizeof(pv));
-                ccfd_host_prim_cons(gam1q, pv, cv);
-            }
-            prim[d] = make_double4(pv[0], pv[1], pv[2], pv[3]);
-            cons[d] = make_double4(cv[0], cv[1], cv[2], cv[3]);
-        }
-    });
-    CK(cudaMemcpyAsync(cur_prim(ctx), prim.data(), sizeof(double4) * N, cudaMemcpyHostToDevice, ctx->stream));
-    CK(cudaMemcpyAsync(ctx->cons0, cons.data(), sizeof(double4) * N, cudaMemcpyHostToDevice, ctx->stream));
+    CK(cudaMemcpyAsync(ctx->xfer, state, sizeof(double4) * N, cudaMemcpyHostToDevice, ctx->stream));
+    k_state_in<<<(unsigned)((N + 255) / 256), 256, 0, ctx->stream>>>(
+        (int)N, ctx->xfer, ctx->d_cell_of_dev, kind == CCFD_CONSERVATIVE, ctx->phys.gam1, ctx->phys.gam1q,
+        cur_prim(ctx), ctx->cons0);
+    CK(cudaGetLastError());
     CK(cudaStreamSynchronize(ctx->stream));
     return CCFD_OK;
 }
@@ -643,18 +652,11 @@ extern "C" int ccfd_get_state(ccfd_ctx* ctx, double* state, int kind) {
     if (!ctx || !state || !ctx->uploaded) return CCFD_ERR_ARG;
     CK(cudaSetDevice(ctx->device));
     const long N = ctx->N;
-    static thread_local std::vector<double4> tl_h;
-    std::vector<double4>& h = tl_h;  // (see ccfd_set_state)
-    h.resize(N);
-    CK(cudaMemcpyAsync(h.data(), kind == CCFD_CONSERVATIVE ? ctx->cons0 : cur_prim(ctx), sizeof(double4) * N,
-                       cudaMemcpyDeviceToHost, ctx->stream));
+    k_state_out<<<(unsigned)((N + 255) / 256), 256, 0, ctx->stream>>>(
+        (int)N, kind == CCFD_CONSERVATIVE ? ctx->cons0 : cur_prim(ctx), ctx->d_dev_of_cell, ctx->xfer);
+    CK(cudaGetLastError());
+    CK(cudaMemcpyAsync(state, ctx->xfer, sizeof(double4) * N, cudaMemcpyDeviceToHost, ctx->stream));
     CK(cudaStreamSynchronize(ctx->stream));
-    par_for(N, [&](long d0, long d1) {
-        for (long d = d0; d < d1; ++d) {
-            double* s = &state[4 * ctx->cell_of_dev[d]];
-            s[0] = h[d].x; s[1] = h[d].y; s[2] = h[d].z; s[3] = h[d].w;
-        }
-    });
     return CCFD_OK;
 }
 

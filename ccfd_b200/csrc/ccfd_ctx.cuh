@@ -37,6 +37,9 @@ struct ccfd_ctx {
     double4* u_t = nullptr;
     double4* grad = nullptr;
     const double4* cell_xq = nullptr;  // [N] (bary, fifth quad point): source term and error norms
+    const int* d_cell_of_dev = nullptr;  // [N] on the device: state transfers permute there
+    const int* d_dev_of_cell = nullptr;
+    double4* xfer = nullptr;             // [N] state in the reference's cell order (transfers)
     unsigned* ticket = nullptr;
     ccfd::Phys* phys_g = nullptr;
     double* ghost_pface = nullptr;

@@ -75,7 +75,7 @@ extern "C" int ccfd_estimate_device_bytes(const ccfd_params* p, const ccfd_mesh*
     const double N = (double)m->n_cells, H = (double)m->n_half_sides, F = (double)m->n_faces,
                  B = (double)m->n_bc;
     // mesh, state, tiles and per-tile scratch of the explicit path
-    double b = 372.0 * N + 52.0 * H + 80.0 * F + 120.0 * B + (1 << 20);
+    double b = 412.0 * N + 52.0 * H + 80.0 * F + 120.0 * B + (1 << 20);
     if (p->source_func) b += 32.0 * N;
     if (p->implicit) {
         const double K = (double)(p->n_kdim > 0 ? p->n_kdim : 1);
