@@ -474,7 +474,7 @@ def main() -> int:
         for _ in range(args.e2e_steps):
             s.set_state(host)
             s.run(1)
-            host[:] = s.get_state()
+            s.get_state(out=host)
         t_e2e = time.perf_counter() - t0
         e2e_value = replica_throughput(world, n, nrk, args.e2e_steps, max_over_ranks(t_e2e, dist))
         s.close()

@@ -109,7 +109,10 @@ class CaseData:
 
     def __del__(self):
         if getattr(self, "_ptr", None):
-            N.lib.ccfd_case_free(self._ptr)
+            try:
+                N.lib.ccfd_case_free(self._ptr)
+            except Exception:  # interpreter shutdown: the module is gone
+                pass
             self._ptr = None
 
     @property
@@ -199,8 +202,13 @@ class Solver:
         s = np.ascontiguousarray(state, dtype=np.float64).reshape(self.n, 4)
         _check(N.lib.ccfd_set_state(self._ctx, _dptr(s), kind), "ccfd_set_state")
 
-    def get_state(self, kind: int = PRIMITIVE) -> np.ndarray:
-        out = np.empty((self.n, 4))
+    def get_state(self, kind: int = PRIMITIVE, out: np.ndarray | None = None) -> np.ndarray:
+        """The state [N, 4] in reference cell order; `out` (C-contiguous
+        float64, e.g. pinned host memory) receives it without a new array."""
+        if out is None:
+            out = np.empty((self.n, 4))
+        elif out.dtype != np.float64 or not out.flags.c_contiguous or out.size != 4 * self.n:
+            raise ValueError("out must be a C-contiguous float64 array of n_cells x 4")
         _check(N.lib.ccfd_get_state(self._ctx, _dptr(out), kind), "ccfd_get_state")
         return out
 

@@ -259,3 +259,28 @@ outputFormat = 3
     assert rep["iterations"] == info["iterations"] == 5
     l1, linf = l1_linf(prim, po)
     assert l1 <= RUN_TOL and linf <= RUN_TOL
+
+
+def test_state_transfers_roundtrip_in_reference_order():
+    # the state moves in the caller's (reference) cell order and is permuted
+    # and converted on the device: primitive and conservative round trips,
+    # into a new array and into a caller-provided one
+    with tempfile.TemporaryDirectory() as tmp:
+        meshgen.dmr_mesh(40, 10).write_gmsh(os.path.join(tmp, "dmr.msh"))
+        case = cc.CaseData.from_text(meshgen.dmr_ini("dmr"), tmp)
+    s = cc.Solver(case, reorder=True)
+    rng = np.random.Generator(np.random.PCG64(11))
+    n = case.n_cells
+    prim = np.stack([rng.uniform(0.5, 2, n), rng.uniform(-1, 1, n), rng.uniform(-1, 1, n),
+                     rng.uniform(0.5, 2, n)], 1)
+    s.set_state(prim)
+    assert np.array_equal(s.get_state(), prim)
+    out = np.full((n, 4), np.nan)
+    assert s.get_state(out=out) is out and np.array_equal(out, prim)
+    cons = s.get_state(cc.CONSERVATIVE)
+    assert np.allclose(cons[:, 1], prim[:, 1] * prim[:, 0], rtol=1e-15)
+    s.set_state(cons, cc.CONSERVATIVE)
+    np.testing.assert_allclose(s.get_state(), prim, rtol=1e-14)
+    with pytest.raises(ValueError):
+        s.get_state(out=np.empty((n, 3)))
+    s.close()
