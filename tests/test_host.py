@@ -174,3 +174,21 @@ def test_record_point_location_follows_reference_rule():
     with pytest.raises(cc.CcfdError) as e:
         cc.CaseData.from_text(meshgen.sod_ini(50, 2) + "nRecordPoints = 1\npointCoords = (/1.5, 0.02/)\n")
     assert e.value.status == 10  # "Record Point # is not in Domain"
+
+
+def test_degenerate_mesh_files_are_errors(tmp_path):
+    # a gmsh file without cells, an EMC2 file without vertices and a gmsh 4
+    # file without physical curves: mesh errors, no crash
+    (tmp_path / "empty.msh").write_text("$MeshFormat\n2.2 0 8\n$EndMeshFormat\n$Nodes\n3\n"
+                                        "1 0 0 0\n2 1 0 0\n3 0 1 0\n$EndNodes\n$Elements\n1\n"
+                                        "1 1 2 101 101 1 2\n$EndElements\n")
+    (tmp_path / "empty.mesh").write_text("MeshVersionFormatted 1\nDimension 2\nEnd\n")
+    (tmp_path / "nocurves.msh4").write_text("$MeshFormat\n4.1 0 8\n$EndMeshFormat\n$Entities\n0 0 1 0\n"
+                                            "1 0 0 0 0 0 0 0 0\n$EndEntities\n")
+    base = meshgen.dmr_ini("empty")
+    for fmt, name in ((".msh", "empty"), (".mesh", "empty"), (".msh4", "nocurves")):
+        ini = base.replace("meshFormat = .msh\n", f"meshFormat = {fmt}\n").replace(
+            "meshFile = empty", f"meshFile = {name}")
+        with pytest.raises(cc.CcfdError) as e:
+            cc.CaseData.from_text(ini, str(tmp_path))
+        assert e.value.status == 10, fmt
