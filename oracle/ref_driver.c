@@ -16,6 +16,9 @@
  *                        559-732) without file output, at most nsteps
  *                        iterations (<=0: until tEnd / convergence)
  *   coef                 like run, plus calcCoef (src/analyze.c:292) per step
+ *                        (CCFD_REF_REL_ABORT=<r>: stationary runs also stop
+ *                        once the abort variable's residual is at most r
+ *                        times the first step's)
  *                        run / coef end with calcErrors (src/analyze.c:445)
  *                        when the case has an exact solution
  *
@@ -289,6 +292,8 @@ int main(int argc, char *argv[])
 	} else if (!strcmp(mode, "run") || !strcmp(mode, "coef")) {
 		bool doCoef = !strcmp(mode, "coef");
 		bool write_out = getenv("CCFD_REF_OUTPUT") != NULL;
+		const char *rel = getenv("CCFD_REF_REL_ABORT");
+		double relAbort = rel ? strtod(rel, NULL) : 0.0, relFirst = 0.0;
 		long nsteps = argc > 4 ? strtol(argv[4], NULL, 10) : 0;
 		if (argc > 5)
 			load_state(argv[5]);
@@ -347,6 +352,16 @@ int main(int argc, char *argv[])
 				}
 				if (converged)
 					break;
+			}
+			/* relative stop around the reference's loop (the residual
+			 * of the abort variable relative to the first step's) */
+			if (isStationary && relAbort > 0.0) {
+				if (nhist == 1)
+					relFirst = resIter[abortVariable];
+				if (resIter[abortVariable] <= relAbort * relFirst) {
+					converged = true;
+					break;
+				}
 			}
 			if ((printTime - t <= 1e-15) || (iter == printIter)) {
 				if (printTime - t <= 1e-15)

@@ -50,7 +50,7 @@ def run_ref(ini_text: str, mode: str, *args, eqn: str = "euler",
             fast: bool = False, state: np.ndarray | None = None,
             threads: int | None = None, workdir: str | None = None,
             files: dict | None = None, timeout: float = 3600.0,
-            output: bool = False) -> dict:
+            output: bool = False, rel_abort: float | None = None) -> dict:
     """Run the reference driver on an .ini text in a scratch directory.
 
     ``state`` (N x 4 primitive states in reference cell order) replaces the
@@ -83,6 +83,8 @@ def run_ref(ini_text: str, mode: str, *args, eqn: str = "euler",
         env.setdefault("OMP_NUM_THREADS", "1")
         if output:
             env["CCFD_REF_OUTPUT"] = "1"
+        if rel_abort is not None:
+            env["CCFD_REF_REL_ABORT"] = repr(float(rel_abort))
         r = subprocess.run(argv, cwd=tmp, env=env, capture_output=True,
                            text=True, timeout=timeout)
         if r.returncode != 0:

@@ -175,6 +175,13 @@ def implicit_cases() -> dict:
         # slowly, so 1e-8 is out of reach of the dense reference Jacobian)
         "naca_euler_imp_pc_long": {"mesh": ("naca", 32, 12, 101), "ini": ini(steps=200), "eqn": "euler",
                                    "steps": 200},
+        # steady run to a relative residual of 0.3 (relAbortResidual; the
+        # reference driver stops at the same relative drop)
+        "naca_euler_imp_rel": {"mesh": ("naca", 32, 12, 101),
+                               "ini": meshgen.airfoil_ini("naca", mach=0.5, alpha=2.0, flux=2, implicit=True,
+                                                          precond=True, n_kdim=10, cfl=20.0, max_iter=200,
+                                                          rel_res=0.3),
+                               "eqn": "euler", "steps": 0, "rel_abort": 0.3},
         # time-accurate implicit steps of the sine wave on a periodic mesh
         # (with the source term or the exact-solution boundary the
         # reference's Newton iteration stalls at a relative residual of

@@ -78,7 +78,8 @@ def ref_small(only: str | None = None) -> dict:
                 arrays[f"{key}/err_u_y"] = d["err_u_y"]
         for key, spec in pick(CASES.implicit_cases()).items():
             ini, files = CASES.materialise(spec, tmp)
-            d = refdump.run_ref(ini, "coef", spec["steps"], eqn=spec["eqn"], files=files)
+            d = refdump.run_ref(ini, "coef", spec["steps"], eqn=spec["eqn"], files=files,
+                                rel_abort=spec.get("rel_abort"))
             arrays[f"{key}/pvar"] = d["pvar"]
             arrays[f"{key}/info"] = d["run_info"]
             arrays[f"{key}/history"] = d["history"]

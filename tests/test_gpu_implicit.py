@@ -30,6 +30,7 @@ def test_implicit_steps_match_reference(ref_small, key):
     ref = ref_small[f"{key}/pvar"].reshape(-1, 4)
     info = ref_small[f"{key}/info"]
     assert rep["iterations"] == int(info[1])
+    assert bool(rep["converged"]) == bool(info[4])  # relative stop: both at the same step
     assert rep["newton_iterations"] == int(info[5])
     assert rep["gmres_iterations"] == int(info[6])
     err = np.abs(prim - ref).max(axis=0) / np.abs(ref).max(axis=0)
