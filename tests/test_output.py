@@ -161,3 +161,32 @@ def test_driver_writes_reference_solution_and_exact_files(ref_output, key):
         for name in written:
             with open(os.path.join(tmp, name)) as f:
                 _files_equal_to_printed_digits(f.read(), g["files"][name], name)
+
+
+def test_history_writer_record_points_and_append(tmp_path):
+    # record-point files (initRecordPoints / evalRecordPoints format) and
+    # appending further rows without repeating the headers
+    ini = CASES.output_cases()["out_sod_stationary_csv"]["ini"] + CASES.RECORD_POINTS
+    case = cc.CaseData.from_text(ini)
+    xy, cells = case.record_points()
+    assert len(cells) == 3
+    w = 11 + 4 * 3
+    rows = np.zeros((2, w))
+    rows[:, 0] = [1, 2]
+    rows[:, 1] = [0.01, 0.02]
+    rows[:, 2] = [0.01, 0.01]
+    rows[:, 3:7] = 1e-3
+    rows[:, 11:] = np.arange(12, dtype=float) / 10
+    cwd = os.getcwd()
+    os.chdir(tmp_path)
+    try:
+        case.write_history(rows)
+        case.write_history(rows, append=True)
+        rp = open("sod_recordPoint_2.csv").read().splitlines()
+        an = open("sod_analysis.csv").read().splitlines()
+    finally:
+        os.chdir(cwd)
+    assert rp[0] == "Time, Density, VelocityX, VelocityY, Pressure" and len(rp) == 5
+    assert rp[1] == "%20.12f,%20.12f,%20.12f,%20.12f,%20.12f" % (0.02, 0.8, 0.9, 1.0, 1.1)
+    assert an[0].startswith("Iter, Time, Residual(RHO)") and len(an) == 5
+    assert an[3] == "%7d, %13.8f, %15.8e, %15.8e, %15.8e, %15.8e" % (1, 0.02, 1e-3, 1e-3, 1e-3, 1e-3)
