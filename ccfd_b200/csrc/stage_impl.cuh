@@ -672,19 +672,39 @@ template <int FLUX, int ORDER, int NS, typename FT>
 __global__ void __launch_bounds__(StageShape<FT>::threads, StageShape<FT>::min_blocks)
     k_stage_batch(const StageLaunch* __restrict__ Ls, const int2* __restrict__ tmap, int rk_mode,
                   int stage) {
+    // The member's launch record goes to shared memory.  In RK mode the
+    // records of both buffer parities are copied while one thread reads the
+    // member's control block, so resolving the record costs one round trip
+    // after the tile map instead of a chain of dependent loads.
+    static_assert(sizeof(StageLaunch) % 16 == 0, "launch record copied in 16-byte words");
+    constexpr int W = (int)(sizeof(StageLaunch) / 16);
+    __shared__ int4 s_rec[2 * W];
+    __shared__ int s_go, s_sel;
     const int2 tm = tmap[blockIdx.x];
     if (rk_mode) {
         const StageLaunch* rec = Ls + (size_t)tm.x * 2 * kBatchStages;
-        const Ctrl* c = rec[0].ctrl;
-        if (!c->active) return;
-        const StageLaunch& L = rec[c->par * kBatchStages + stage];
-        if (L.mode < 0) return;
-        stage_body<FLUX, ORDER, NS, FT>(L, tm.y);
+        const int4* a = reinterpret_cast<const int4*>(rec + stage);
+        const int4* b = reinterpret_cast<const int4*>(rec + kBatchStages + stage);
+        for (int k = threadIdx.x; k < 2 * W; k += blockDim.x) s_rec[k] = k < W ? a[k] : b[k - W];
+        if (threadIdx.x == 0) {
+            const Ctrl* c = rec[0].ctrl;
+            s_go = c->active;
+            s_sel = c->par;
+        }
     } else {
-        const StageLaunch& L = Ls[tm.x];
-        if (L.skip && *L.skip) return;
-        stage_body<FLUX, ORDER, NS, FT>(L, tm.y);
+        const int4* a = reinterpret_cast<const int4*>(Ls + tm.x);
+        for (int k = threadIdx.x; k < W; k += blockDim.x) s_rec[k] = a[k];
+        if (threadIdx.x == 0) {
+            const int* skip = Ls[tm.x].skip;
+            s_go = !(skip && *skip);
+            s_sel = 0;
+        }
     }
+    __syncthreads();
+    if (!s_go) return;
+    const StageLaunch& L = *reinterpret_cast<const StageLaunch*>(s_rec + s_sel * W);
+    if (L.mode < 0) return;
+    stage_body<FLUX, ORDER, NS, FT>(L, tm.y);
 }
 
 
