@@ -148,7 +148,12 @@ extern "C" int ccfd_create(const ccfd_params* params, ccfd_ctx** out) {
     ccfd_ctx* ctx = new ccfd_ctx();
     ctx->params = p;
     ctx->device = dev;
-    if (cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking) != cudaSuccess) {
+    // a context's own stream has the highest priority: its uploads, state
+    // transfers and releases then do not queue behind the long stage
+    // launches of a batch that steps other contexts (serving)
+    int prio_least = 0, prio_greatest = 0;
+    cudaDeviceGetStreamPriorityRange(&prio_least, &prio_greatest);
+    if (cudaStreamCreateWithPriority(&ctx->stream, cudaStreamNonBlocking, prio_greatest) != cudaSuccess) {
         delete ctx;
         return CCFD_ERR_CUDA;
     }
