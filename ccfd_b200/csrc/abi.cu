@@ -160,7 +160,10 @@ extern "C" int ccfd_create(const ccfd_params* params, ccfd_ctx** out) {
     // host copy of the control block in ordinary memory: releasing pinned
     // memory would wait for all work on the device (other contexts included)
     ctx->h_ctrl = new Ctrl();
-    if (cudaEventCreate(&ctx->ev_run0) != cudaSuccess || cudaEventCreate(&ctx->ev_run1) != cudaSuccess) {
+    if (cudaEventCreate(&ctx->ev_run0) != cudaSuccess || cudaEventCreate(&ctx->ev_run1) != cudaSuccess ||
+        cudaEventCreateWithFlags(&ctx->ev_xfer, cudaEventDisableTiming) != cudaSuccess) {
+        if (ctx->ev_run0) cudaEventDestroy(ctx->ev_run0);
+        if (ctx->ev_run1) cudaEventDestroy(ctx->ev_run1);
         delete ctx->h_ctrl;
         cudaStreamDestroy(ctx->stream);
         delete ctx;
@@ -196,6 +199,7 @@ extern "C" void ccfd_destroy(ccfd_ctx* ctx) {
     free_device(ctx);
     if (ctx->ev_run0) cudaEventDestroy(ctx->ev_run0);
     if (ctx->ev_run1) cudaEventDestroy(ctx->ev_run1);
+    if (ctx->ev_xfer) cudaEventDestroy(ctx->ev_xfer);
     delete ctx->h_ctrl;
     cudaStreamDestroy(ctx->stream);
     delete ctx;
@@ -645,11 +649,15 @@ extern "C" int ccfd_set_state(ccfd_ctx* ctx, const double* state, int kind) {
     CK(cudaSetDevice(ctx->device));
     const long N = ctx->N;
     CK(cudaMemcpyAsync(ctx->xfer, state, sizeof(double4) * N, cudaMemcpyHostToDevice, ctx->stream));
+    CK(cudaEventRecord(ctx->ev_xfer, ctx->stream));
     k_state_in<<<(unsigned)((N + 255) / 256), 256, 0, ctx->stream>>>(
         (int)N, ctx->xfer, ctx->d_cell_of_dev, kind == CCFD_CONSERVATIVE, ctx->phys.gam1, ctx->phys.gam1q,
         cur_prim(ctx), ctx->cons0);
     CK(cudaGetLastError());
-    CK(cudaStreamSynchronize(ctx->stream));
+    // the caller's array is free once the copy is done; the permutation runs
+    // on in stream order before anything else that reads the state (a batch
+    // synchronises the context's stream when it takes the context in)
+    CK(cudaEventSynchronize(ctx->ev_xfer));
     return CCFD_OK;
 }
 
@@ -1154,13 +1162,13 @@ extern "C" int ccfd_run_explicit(ccfd_ctx* ctx, long nsteps, ccfd_report* report
         if (prof && (st = collect_profile(ctx, ctx->prof_ev[par][which], (size_t)ran * nrk))) return st;
         if (ran == 0) break;  // error in the first stage of the graph
     }
+    // one synchronisation for the end event and the flags
     CK(cudaEventRecord(ctx->ev_run1, ctx->stream));
-    CK(cudaEventSynchronize(ctx->ev_run1));
-    float run_ms = 0.0f;
-    CK(cudaEventElapsedTime(&run_ms, ctx->ev_run0, ctx->ev_run1));
     unsigned f = 0;
     CK(cudaMemcpyAsync(&f, ctx->flags, sizeof(unsigned), cudaMemcpyDeviceToHost, ctx->stream));
     CK(cudaStreamSynchronize(ctx->stream));
+    float run_ms = 0.0f;
+    CK(cudaEventElapsedTime(&run_ms, ctx->ev_run0, ctx->ev_run1));
     if (report) {
         ccfd_fill_report(ctx, report);
         report->device_ms = run_ms;

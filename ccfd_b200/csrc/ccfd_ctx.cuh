@@ -65,6 +65,7 @@ struct ccfd_ctx {
     double prof_ms = 0.0;
     long prof_count = 0;
     cudaEvent_t ev_run0 = nullptr, ev_run1 = nullptr;
+    cudaEvent_t ev_xfer = nullptr;  // end of a state upload's host-to-device copy
     // per-step history: device ring (sp.hist), rows drained to the host
     // after each synchronisation of a run
     long long hist_read = 0;         // last iteration drained
