@@ -1142,6 +1142,11 @@ extern "C" int ccfd_run_explicit(ccfd_ctx* ctx, long nsteps, ccfd_report* report
     launch_dt(ctx->mesh, ctx->phys, ctx->ctrl, ctx->sp, cur_prim(ctx), ctx->dt_partial, ctx->dt_bad, ctx->stream);
     launch_step_begin(ctx->ctrl, ctx->sp, ctx->dt_partial, ctx->dt_bad, ctx->nb_cells, ctx->stream);
     CK(cudaGetLastError());
+    // each graph launch is followed by the end event and the reads of the
+    // control block and the flags, so the synchronisation after the last
+    // graph also ends the run
+    unsigned f = 0;
+    bool ended = false;
     while (!c.done && c.iter < stop_at) {
         long long remaining = stop_at - c.iter;
         int which = remaining >= kMany ? 1 : 0;
@@ -1152,8 +1157,11 @@ extern "C" int ccfd_run_explicit(ccfd_ctx* ctx, long nsteps, ccfd_report* report
             return st;
         long long iter0 = c.iter;
         CK(cudaGraphLaunch(ctx->graph[par][which], ctx->stream));
+        CK(cudaEventRecord(ctx->ev_run1, ctx->stream));
         CK(cudaMemcpyAsync(ctx->h_ctrl, ctx->ctrl, sizeof(Ctrl), cudaMemcpyDeviceToHost, ctx->stream));
+        CK(cudaMemcpyAsync(&f, ctx->flags, sizeof(unsigned), cudaMemcpyDeviceToHost, ctx->stream));
         CK(cudaStreamSynchronize(ctx->stream));
+        ended = true;
         // steps after a stop inside the graph do not run: the state is in
         // the buffer the last executed stage wrote
         long long ran = c.iter - iter0;
@@ -1162,11 +1170,11 @@ extern "C" int ccfd_run_explicit(ccfd_ctx* ctx, long nsteps, ccfd_report* report
         if (prof && (st = collect_profile(ctx, ctx->prof_ev[par][which], (size_t)ran * nrk))) return st;
         if (ran == 0) break;  // error in the first stage of the graph
     }
-    // one synchronisation for the end event and the flags
-    CK(cudaEventRecord(ctx->ev_run1, ctx->stream));
-    unsigned f = 0;
-    CK(cudaMemcpyAsync(&f, ctx->flags, sizeof(unsigned), cudaMemcpyDeviceToHost, ctx->stream));
-    CK(cudaStreamSynchronize(ctx->stream));
+    if (!ended) {  // no graph ran: end after the time-step kernels
+        CK(cudaEventRecord(ctx->ev_run1, ctx->stream));
+        CK(cudaMemcpyAsync(&f, ctx->flags, sizeof(unsigned), cudaMemcpyDeviceToHost, ctx->stream));
+        CK(cudaStreamSynchronize(ctx->stream));
+    }
     float run_ms = 0.0f;
     CK(cudaEventElapsedTime(&run_ms, ctx->ev_run0, ctx->ev_run1));
     if (report) {
