@@ -272,7 +272,9 @@ int ccfd_upload_case(ccfd_ctx *ctx, const ccfd_mesh *mesh, const ccfd_bc *bc,
 /* State in reference cell order, [N][4], primitive or conservative.  Setting
  * primitives also sets cVar = primCons(pVar) like setInitialCondition
  * (src/initialCondition.c:346-350); setting conservatives sets
- * pVar = consPrim(cVar). */
+ * pVar = consPrim(cVar).  Returns once the array has been copied (the caller
+ * may reuse it); the conversion finishes on the context's stream before any
+ * later call on the context reads the state. */
 int ccfd_set_state(ccfd_ctx *ctx, const double *state, int kind);
 int ccfd_get_state(ccfd_ctx *ctx, double *state, int kind);
 /* Set / get the simulation time t (src/timeDiscretization.c:31). */
