@@ -284,3 +284,37 @@ def test_state_transfers_roundtrip_in_reference_order():
     with pytest.raises(ValueError):
         s.get_state(out=np.empty((n, 3)))
     s.close()
+
+
+def test_state_upload_returns_after_its_copy():
+    # ccfd_set_state returns once the caller's array is copied and lets the
+    # conversion run on in the context's stream: overwriting a pinned array
+    # right after the call leaves the uploaded state intact, and a run that
+    # follows the upload at once equals one after a synchronising read
+    import torch
+
+    with tempfile.TemporaryDirectory() as tmp:
+        meshgen.dmr_mesh(400, 100).write_gmsh(os.path.join(tmp, "dmr.msh"))
+        case = cc.CaseData.from_text(meshgen.dmr_ini("dmr"), tmp)
+    a = cc.Solver(case, reorder=True)
+    b = cc.Solver(case, reorder=True)
+    n = case.n_cells
+    a.run(2)
+    prim = a.get_state()
+    host = torch.empty((n, 4), dtype=torch.float64, pin_memory=True).numpy()
+    for _ in range(3):
+        host[:] = prim
+        a.set_state(host)
+        host[:] = np.nan
+        assert np.array_equal(a.get_state(), prim)
+    host[:] = prim
+    a.set_state(host)
+    host[:] = np.nan
+    a.run(3)
+    b.run(2)
+    b.set_state(prim)
+    assert np.array_equal(b.get_state(), prim)
+    b.run(3)
+    assert np.array_equal(a.get_state(), b.get_state())
+    a.close()
+    b.close()
