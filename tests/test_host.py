@@ -94,7 +94,7 @@ def test_undefined_bc_code_is_a_mesh_error():
 def test_mesh_build_rejects_inconsistent_boundary(tmp_path):
     m = meshgen.dmr_mesh(4, 2)
     m.bc = m.bc[:-1]  # drop one boundary edge: odd side count
-    path = m.write_gmsh(str(tmp_path / "dmr.msh"))
+    m.write_gmsh(str(tmp_path / "dmr.msh"))
     with pytest.raises(cc.CcfdError) as e:
         cc.CaseData.from_text(meshgen.dmr_ini("dmr"), str(tmp_path))
     assert e.value.status == 10
