@@ -147,10 +147,48 @@ def algorithmic_bytes_per_stage(m: dict, venk: bool) -> int:
     return n * per_cell + h * (4 + 4 + 16 + 16) + f * (16 + 8 + 8)
 
 
-# DRAM bytes per launch of the stage kernel on this workload, from the ncu
-# capture summarised in profiles/k_stage_dmr500k_hllc_vk_fp64.md
-# (dram__bytes_read.sum + dram__bytes_write.sum)
-STAGE_TRAFFIC_BYTES = 151.42e6 + 12.26e6
+# Algorithmic bytes per residual evaluation and cell of the two-pass
+# scheme (gradient pass, then face pass, each array touched once), FP64:
+# triangles 356 B (Barth-Jespersen) / 364 B (Venkatakrishnan), quads 408 /
+# 416 B.  The roofline's `achieved` uses these per-cell figures.
+ROOFLINE_BYTES_PER_CELL = {("tri", False): 356, ("tri", True): 364,
+                           ("quad", False): 408, ("quad", True): 416}
+
+
+def roofline_bytes_per_residual(n_tri: int, n_quad: int, venk: bool) -> int:
+    return (n_tri * ROOFLINE_BYTES_PER_CELL[("tri", venk)]
+            + n_quad * ROOFLINE_BYTES_PER_CELL[("quad", venk)])
+
+
+# DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) per launch of the
+# stage kernel on this workload from one ncu capture, valid only for the
+# kernel sources whose digest is recorded beside it (STAGE_SOURCES); for
+# other sources the line reports no traffic.
+STAGE_TRAFFIC = {"bytes": 151.42e6 + 12.26e6,
+                 "sha256": "unset"}
+STAGE_SOURCES = ("ccfd_b200/csrc/stage_impl.cuh", "ccfd_b200/csrc/physics.cuh",
+                 "ccfd_b200/csrc/kernels.cuh", "ccfd_b200/csrc/stage_flux.inc",
+                 "ccfd_b200/csrc/stage_f05.cu", "ccfd_b200/csrc/tiles.cpp")
+
+
+def stage_sources_digest() -> str:
+    import hashlib
+    h = hashlib.sha256()
+    for rel in STAGE_SOURCES:
+        with open(os.path.join(ROOT, rel), "rb") as f:
+            h.update(f.read())
+    return h.hexdigest()[:16]
+
+
+def stage_traffic():
+    """(bytes, note): the recorded ncu traffic if it was measured on the
+    current stage-kernel sources, else (None, why)."""
+    dig = stage_sources_digest()
+    if (NX, NY) != (1000, 250):
+        return None, "recorded for the 1000x250 workload only"
+    if STAGE_TRAFFIC["sha256"] != dig:
+        return None, f"no ncu capture of this kernel revision (sources {dig})"
+    return STAGE_TRAFFIC["bytes"], f"ncu dram__bytes_read.sum + dram__bytes_write.sum, sources {dig}"
 
 
 def make_case(tmpdir: str, precision: int = 0):
@@ -352,32 +390,98 @@ def run_serving(n_req: int, load: float, budget: int, seed: int = 20260005) -> d
     }
 
 
+def host_cpu() -> dict:
+    """Host CPU of this process: model name, the logical CPUs it may run on
+    and the physical cores behind them (distinct package / core ids)."""
+    try:
+        allowed = sorted(os.sched_getaffinity(0))
+    except AttributeError:
+        allowed = list(range(os.cpu_count() or 1))
+    cores = set()
+    for c in allowed:
+        base = f"/sys/devices/system/cpu/cpu{c}/topology/"
+        try:
+            with open(base + "physical_package_id") as f:
+                pkg = f.read().strip()
+            with open(base + "core_id") as f:
+                core = f.read().strip()
+            cores.add((pkg, core))
+        except OSError:
+            cores.add(("?", str(c)))
+    model = "unknown"
+    try:
+        with open("/proc/cpuinfo") as f:
+            for ln in f:
+                if ln.startswith("model name"):
+                    model = ln.split(":", 1)[1].strip()
+                    break
+    except OSError:
+        pass
+    return {"model": model, "logical_cpus": len(allowed), "physical_cores": len(cores)}
+
+
 def cpu_reference_sample(ini: str, mesh_path: str, steps: int, threads: int):
     """Time the reference (compiled from its sources, oracle/_ref) on the
-    host cores for `steps` time steps: returns the wall clock (seconds,
-    omp_get_wtime since the start of its time loop) at the end of each step
-    and the whole dump of the run."""
+    host cores for `steps` time steps, `threads` OpenMP threads bound one per
+    physical core (OMP_PROC_BIND=close, OMP_PLACES=cores): returns the wall
+    clock (seconds, omp_get_wtime since the start of its time loop) at the
+    end of each step and the whole dump of the run."""
     from oracle import refdump
+    os.environ["OMP_PROC_BIND"] = "close"
+    os.environ["OMP_PLACES"] = "cores"
     d = refdump.run_ref(ini, "run", steps, fast=True, threads=threads,
                         files={"dmr.msh": mesh_path}, timeout=1800)
     return d["step_wall"], d
+
+
+def step_seconds(wall, first: int, last: int) -> float:
+    """Wall time of steps first+1..last from the per-step clock of the
+    reference's time loop (wall[k] = time at the end of step k+1)."""
+    return wall[last - 1] - (wall[first - 1] if first > 0 else 0.0)
+
+
+def load_meshgen_standalone():
+    """The mesh generator module loaded by file path, without the package:
+    the reference arm writes its input with it and must not load this
+    library's native code."""
+    import importlib.util
+    spec = importlib.util.spec_from_file_location(
+        "ccfd_meshgen_standalone", os.path.join(ROOT, "ccfd_b200", "meshgen.py"))
+    mod = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(mod)
+    return mod
+
+
+def reference_arm_inputs(tmpdir: str):
+    """Mesh file, .ini text, cell and face counts of the benchmark workload
+    for the reference arm, made without importing the ccfd_b200 package."""
+    mg = load_meshgen_standalone()
+    mesh = mg.dmr_mesh(NX, NY)
+    path = os.path.join(tmpdir, "dmr.msh")
+    mesh.write_gmsh_text(path)
+    return mg.dmr_ini("dmr"), path, mesh.n_cells, mesh.n_faces
 
 
 def run_reference_arm(args, rank: int, world: int) -> None:
     if rank != 0:
         return
     from oracle import refdump
-    threads = os.cpu_count() or 1
+    cpu = host_cpu()
+    threads = cpu["physical_cores"]
     with tempfile.TemporaryDirectory() as tmp:
-        case, ini, path = make_case(tmp)
-        n = case.n_cells
+        ini, path, n, faces = reference_arm_inputs(tmp)
+        one = None
         if refdump.have_ref("euler", fast=True):
             kind = "reference"
             wall, _ = cpu_reference_sample(ini, path, args.warmup + args.steps, threads)
-            t = wall[args.warmup + args.steps - 1] - (wall[args.warmup - 1] if args.warmup else 0.0)
+            t = step_seconds(wall, args.warmup, args.warmup + args.steps)
             cores = threads
+            w1, _ = cpu_reference_sample(ini, path, 2, 1)
+            one = n * 3 / step_seconds(w1, 1, 2)
         else:
             from oracle import restated
+            import ccfd_b200 as cc  # the restatement reads the library's mesh arrays
+            case = cc.CaseData.from_text(ini, tmp)
             kind = "port"
             cores = 1
             t0 = time.perf_counter()
@@ -388,11 +492,14 @@ def run_reference_arm(args, rank: int, world: int) -> None:
             "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": 1e3 * t / args.steps, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": workload_config(n, case.c.mesh.n_faces, world),
+            "config": workload_config(n, faces, world),
             "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": kind,
+                             "cpu": cpu, "omp": "OMP_PROC_BIND=close OMP_PLACES=cores",
+                             "one_thread_value": one,
                              "sample": f"{args.warmup} warm-up + {args.steps} timed RK3 steps of the "
                                        "full 500k-cell workload (reference's own time loop, "
-                                       "omp_get_wtime per step)"},
+                                       "omp_get_wtime per step); one_thread_value: step 2 of a "
+                                       "2-step run on one thread"},
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
 
@@ -401,7 +508,7 @@ def main() -> int:
     global NX, NY
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--steps", type=int, default=500)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--e2e-steps", type=int, default=20)
@@ -445,18 +552,22 @@ def main() -> int:
         nrk = 3
         s = cc.Solver(case, reorder=True)
         s.set_profiling(True)
+        # clocks are sampled from the start of the warm-up to the end of the
+        # timed steps (the timed region alone can be shorter than a sample
+        # period)
+        clocks = ClockSampler(local)
+        clocks.start()
         s.run(args.warmup)
         s.profile(reset=True)
         torch.cuda.synchronize()
         if dist is not None:
             dist.barrier()
-        clocks = ClockSampler(local)
-        clocks.start()
         rep = s.run(args.steps)
         torch.cuda.synchronize()
         if dist is not None:
             dist.barrier()
         clk = clocks.stop()
+        clk["window"] = "FP64 leg: warm-up and timed steps"
         res_ms, res_cnt = s.profile(reset=True)
         prim_fp64 = s.get_state()
         t_ms = max_over_ranks(rep["device_ms"], dist)
@@ -479,7 +590,9 @@ def main() -> int:
         e2e_value = replica_throughput(world, n, nrk, args.e2e_steps, max_over_ranks(t_e2e, dist))
         s.close()
 
-        bytes_stage = algorithmic_bytes_per_stage(m, venk=True)
+        n_tri = int((m["cell_type"] == 3).sum())
+        bytes_stage = roofline_bytes_per_residual(n_tri, n - n_tri, venk=True)
+        bytes_fused = algorithmic_bytes_per_stage(m, venk=True)
         mixed = None
         if not args.no_mixed:
             mixed = run_mixed(tmp, args.steps, args.warmup, prim_fp64, nrk, bytes_stage)
@@ -491,26 +604,33 @@ def main() -> int:
                 serving = run_serving(args.requests, load=0.8, budget=150 * 10**9)
         avg_res_ms = res_ms / max(res_cnt, 1)
         achieved = bytes_stage / (avg_res_ms / 1e3) / 1e9
+        traffic, traffic_note = stage_traffic()
 
         cpu = None
         if rank == 0 and world == 1 and not args.no_cpu:
             from oracle import refdump
-            threads = os.cpu_count() or 1
+            hc = host_cpu()
+            threads = hc["physical_cores"]
             if refdump.have_ref("euler", fast=True):
                 wall, _ = cpu_reference_sample(ini, mesh_path, args.cpu_steps, threads)
-                t_cpu = wall[-1] - wall[0] if len(wall) > 1 else wall[-1]
-                st_cpu = len(wall) - 1 if len(wall) > 1 else 1
+                first = 1 if len(wall) > 1 else 0  # the first step is untimed
+                st_cpu = len(wall) - first
+                t_cpu = step_seconds(wall, first, len(wall))
+                w1, _ = cpu_reference_sample(ini, mesh_path, 2, 1)
                 cpu = {"value": n * nrk * st_cpu / t_cpu, "unit": UNIT, "cores": threads,
-                       "kind": "reference",
+                       "kind": "reference", "cpu": hc,
+                       "omp": "OMP_PROC_BIND=close OMP_PLACES=cores",
+                       "one_thread_value": n * nrk / step_seconds(w1, 1, 2),
                        "sample": f"{args.cpu_steps} RK3 steps of the same 500k-cell workload "
                                  "(first step untimed), reference compiled from its sources "
-                                 "(-O3 -march=x86-64-v3, OpenMP)"}
+                                 "(-O3 -march=x86-64-v3, OpenMP, one thread per physical core); "
+                                 "one_thread_value: step 2 of a 2-step run on one thread"}
             else:
                 from oracle import restated
                 t0 = time.perf_counter()
                 restated.residual(case, case.prim0(), 0.0)
                 t_cpu = time.perf_counter() - t0
-                cpu = {"value": n / t_cpu, "unit": UNIT, "cores": 1, "kind": "port",
+                cpu = {"value": n / t_cpu, "unit": UNIT, "cores": 1, "kind": "port", "cpu": hc,
                        "sample": "one residual evaluation of the 500k-cell workload (C restatement)"}
 
     if rank == 0:
@@ -522,10 +642,11 @@ def main() -> int:
             "config": workload_config(n, m["n_faces"], world),
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm_peak,
                          "unit": "GB/s", "frac": achieved / hbm_peak,
-                         "traffic": STAGE_TRAFFIC_BYTES if (NX, NY) == (1000, 250) else None,
-                         "kernel": "k_stage: fused residual evaluation + RK stage (one CTA per "
-                                   "256-cell tile)",
-                         "bytes_per_launch": bytes_stage, "avg_ms": avg_res_ms,
+                         "traffic": traffic, "traffic_source": traffic_note,
+                         "kernel": "k_stage: fused residual evaluation + RK stage",
+                         "bytes_per_launch": bytes_stage,
+                         "bytes_per_cell": "364 (two-pass scheme, triangles, Venkatakrishnan)",
+                         "fused_bytes_per_launch": bytes_fused, "avg_ms": avg_res_ms,
                          "peak_source": peak_src},
             "e2e": {"value": e2e_value, "unit": UNIT,
                     "h2d_bytes_per_step": n * 4 * 8, "d2h_bytes_per_step": n * 4 * 8},

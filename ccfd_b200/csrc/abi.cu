@@ -930,9 +930,16 @@ extern "C" int ccfd_autotune(ccfd_ctx* ctx, const ccfd_mesh* m, const ccfd_bc* b
     CK(cudaSetDevice(ctx->device));
     static const int kTiles[] = {128, 192, 256, 320, 384};
     const int kReps = 5;
-    cudaEvent_t e0, e1;
-    CK(cudaEventCreate(&e0));
-    CK(cudaEventCreate(&e1));
+    // the two timing events are released on every return path
+    struct Events {
+        cudaEvent_t a = nullptr, b = nullptr;
+        ~Events() {
+            if (a) cudaEventDestroy(a);
+            if (b) cudaEventDestroy(b);
+        }
+    } ev;
+    CK(cudaEventCreate(&ev.a));
+    CK(cudaEventCreate(&ev.b));
     double best = 1e300;
     int best_tile = ctx->tile_cells, best_order = 1;
     for (int order = 1; order >= 0; --order)
@@ -940,27 +947,21 @@ extern "C" int ccfd_autotune(ccfd_ctx* ctx, const ccfd_mesh* m, const ccfd_bc* b
             ctx->tile_cells = tc;
             int st = ccfd_upload_case(ctx, m, bc, n_bc, ex, order);
             if (st == CCFD_ERR_ARG) continue;  // tile too large for shared memory
-            if (st || (st = ccfd_set_state(ctx, prim, CCFD_PRIMITIVE))) {
-                cudaEventDestroy(e0);
-                cudaEventDestroy(e1);
-                return st;
-            }
+            if (st || (st = ccfd_set_state(ctx, prim, CCFD_PRIMITIVE))) return st;
             if ((st = ccfd_residual_device(ctx, 0.0))) return st;  // warm-up
-            CK(cudaEventRecord(e0, ctx->stream));
+            CK(cudaEventRecord(ev.a, ctx->stream));
             for (int r = 0; r < kReps; ++r)
                 if ((st = ccfd_residual_device(ctx, 0.0))) return st;
-            CK(cudaEventRecord(e1, ctx->stream));
-            CK(cudaEventSynchronize(e1));
+            CK(cudaEventRecord(ev.b, ctx->stream));
+            CK(cudaEventSynchronize(ev.b));
             float ms = 0.0f;
-            CK(cudaEventElapsedTime(&ms, e0, e1));
+            CK(cudaEventElapsedTime(&ms, ev.a, ev.b));
             if (ms / kReps < best) {
                 best = ms / kReps;
                 best_tile = tc;
                 best_order = order;
             }
         }
-    cudaEventDestroy(e0);
-    cudaEventDestroy(e1);
     ctx->tile_cells = best_tile;
     int st = ccfd_upload_case(ctx, m, bc, n_bc, ex, best_order);
     if (!st) st = ccfd_set_state(ctx, prim, CCFD_PRIMITIVE);

@@ -30,7 +30,9 @@ constexpr int kMaxDevices = 64;
 static __device__ __align__(256) double g_partial[kMaxBlocks * 4];
 
 // device address of g_partial, looked up once per device with that device
-// current (the host-side symbol is only a stand-in, never a device address)
+// current (the host-side symbol is only a stand-in, never a device address).
+// It stays valid while the device's context lives, so a device must not be
+// reset while the library is loaded.
 double* g_partial_addr[kMaxDevices] = {nullptr};
 std::mutex g_setup_mutex;
 

@@ -19,8 +19,6 @@ import os
 
 import numpy as np
 
-from . import _native as N
-
 
 class RawMesh:
     def __init__(self, nodes, tria=None, quad=None, bc=None):
@@ -37,6 +35,9 @@ class RawMesh:
         return len(self.tria) + len(self.quad)
 
     def write_gmsh(self, path: str) -> str:
+        """Write the mesh as gmsh 2.2 ASCII through the library's writer
+        (``ccfd_write_gmsh2``)."""
+        from . import _native as N
         lp = lambda a: a.ctypes.data_as(C.POINTER(C.c_long))
         st = N.lib.ccfd_write_gmsh2(os.fsencode(path),
                                     self.nodes.ctypes.data_as(C.POINTER(C.c_double)),
@@ -45,6 +46,36 @@ class RawMesh:
         if st != 0:
             raise OSError(f"writing {path} failed ({st})")
         return path
+
+    def write_gmsh_text(self, path: str) -> str:
+        """The same gmsh 2.2 file as ``write_gmsh``, byte for byte, written
+        in Python: for callers that must not load the native library (the
+        timed reference arm of the benchmark reads its mesh from here).
+        The module has no import of the package, so it can be loaded by
+        file path on its own."""
+        out = ["$MeshFormat\n2.2 0 8\n$EndMeshFormat\n$Nodes\n%d\n" % len(self.nodes)]
+        out += ["%d %.17g %.17g 0\n" % (i + 1, x, y) for i, (x, y) in enumerate(self.nodes.tolist())]
+        out.append("$EndNodes\n$Elements\n%d\n" % (len(self.bc) + len(self.tria) + len(self.quad)))
+        k = 1
+        for a, b, c in self.bc.tolist():
+            out.append("%d 1 2 %d %d %d %d\n" % (k, c, c, a + 1, b + 1))
+            k += 1
+        for a, b, c, dom in self.tria.tolist():
+            out.append("%d 2 2 %d %d %d %d %d\n" % (k, dom, dom, a + 1, b + 1, c + 1))
+            k += 1
+        for a, b, c, d, dom in self.quad.tolist():
+            out.append("%d 3 2 %d %d %d %d %d %d\n" % (k, dom, dom, a + 1, b + 1, c + 1, d + 1))
+            k += 1
+        out.append("$EndElements\n")
+        with open(path, "w") as f:
+            f.write("".join(out))
+        return path
+
+    @property
+    def n_faces(self) -> int:
+        """Unique faces of the mesh: every interior edge is shared by two
+        cells, every boundary edge belongs to one."""
+        return (3 * len(self.tria) + 4 * len(self.quad) + len(self.bc)) // 2
 
 
 def write_gmsh4(mesh: "RawMesh", path: str) -> str:

@@ -274,7 +274,10 @@ int ccfd_upload_case(ccfd_ctx *ctx, const ccfd_mesh *mesh, const ccfd_bc *bc,
  * (src/initialCondition.c:346-350); setting conservatives sets
  * pVar = consPrim(cVar).  Returns once the array has been copied (the caller
  * may reuse it); the conversion finishes on the context's stream before any
- * later call on the context reads the state. */
+ * later call on the context reads the state.  A failure of that conversion
+ * kernel is therefore not seen by this call: the next call on the context
+ * that synchronises its stream (a run, a residual, ccfd_get_state) returns
+ * it as CCFD_ERR_CUDA. */
 int ccfd_set_state(ccfd_ctx *ctx, const double *state, int kind);
 int ccfd_get_state(ccfd_ctx *ctx, double *state, int kind);
 /* Set / get the simulation time t (src/timeDiscretization.c:31). */
@@ -445,7 +448,9 @@ int ccfd_server_times(ccfd_server *s, double out[3]);
  * partial sums live in a file-scope device array that every device loading
  * the library keeps until exit.  The first call on a device looks up that
  * array's device address (cudaGetSymbolAddress, with the device current), so
- * make the first call on each device before any stream capture.  All calls
+ * make the first call on each device before any stream capture.  That
+ * address is kept for the life of the process: do not reset a device
+ * (cudaDeviceReset) while this library is loaded.  All calls
  * share the array: calls that overlap on the GPU race.  Returns CCFD_ERR_ARG
  * for n_cells <= 0 or n_cells > CCFD_NOALLOC_MAX_CELLS. */
 int ccfd_global_residual_noalloc(const double *u_t, const double *area, long n_cells,

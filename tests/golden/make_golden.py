@@ -1,7 +1,7 @@
 """Generate the committed golden fixtures of the parity tests.
 
-Run in a checkout that has the reference project (default ../reference path
-given by --ref) and the compiled reference oracle (``make -C oracle``):
+Run in a checkout that has the reference project (its directory given by
+--ref or the environment variable CCFD_REFERENCE_DIR) and the compiled reference oracle (``make -C oracle``):
 
     python tests/golden/make_golden.py --ref /path/to/ccfd
 
@@ -105,11 +105,15 @@ def ref_output() -> dict:
 
 def main() -> int:
     ap = argparse.ArgumentParser()
-    ap.add_argument("--ref", default="/root/reference")
+    ap.add_argument("--ref", default=os.environ.get("CCFD_REFERENCE_DIR"),
+                    help="reference project directory (default: $CCFD_REFERENCE_DIR)")
     ap.add_argument("--only", default=None,
                     help="regenerate only the cases whose key starts with this prefix and "
                          "merge them into the existing ref_small.npz")
     a = ap.parse_args()
+    if not a.ref or not os.path.isdir(a.ref):
+        print("reference project not found: pass --ref or set CCFD_REFERENCE_DIR", file=sys.stderr)
+        return 1
     if not refdump.have_ref("euler") or not refdump.have_ref("navierstokes"):
         print("compiled reference missing: run `make -C oracle` first", file=sys.stderr)
         return 1

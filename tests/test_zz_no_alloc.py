@@ -62,6 +62,35 @@ def test_noalloc_global_residual_matches(tmp_path):
 
 
 @pytest.mark.gpu
+@pytest.mark.parametrize("n", [300_001, 1 << 20])
+def test_noalloc_large_fields_match_float64_sum(n):
+    """Synthetic fields well above 65,536 cells (the final pass then walks
+    many partials per thread) and at the scratch's full size, two calls in a
+    row, against a float64 sum of the same terms."""
+    import torch
+
+    from ccfd_b200 import _native as N
+
+    assert n <= N.NOALLOC_MAX_CELLS
+    torch.cuda.set_device(0)
+    stream = torch.cuda.current_stream().cuda_stream
+    res_dev = torch.full((4,), np.nan, dtype=torch.float64, device="cuda")
+    for seed in (1, 2):
+        rng = np.random.default_rng(seed)
+        ut = rng.standard_normal((n, 4)) * np.array([1.0, 10.0, 0.1, 100.0])
+        area = rng.uniform(0.5, 2.0, n) * 1e-4
+        taq = 1.0 / area.sum()
+        want = np.sqrt((area[:, None] * ut * ut).sum(axis=0) * taq)
+        ut_dev = torch.from_numpy(ut).cuda()
+        area_dev = torch.from_numpy(area).cuda()
+        torch.cuda.synchronize()
+        st = _call(N.lib, ut_dev, area_dev, n, taq, res_dev, stream)
+        assert st == 0, N.lib.ccfd_strerror(st)
+        torch.cuda.synchronize()
+        np.testing.assert_allclose(res_dev.cpu().numpy(), want, rtol=RTOL, atol=0.0)
+
+
+@pytest.mark.gpu
 def test_noalloc_rejects_sizes_beyond_scratch():
     import torch
 
