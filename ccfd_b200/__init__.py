@@ -332,6 +332,29 @@ class Solver:
         _check(N.lib.ccfd_clcd(self._ctx, C.byref(cl), C.byref(cd)), "ccfd_clcd")
         return cl.value, cd.value
 
+    def build_matrix(self, time: float, dt: float):
+        """buildMatrix + calcDinv at the current state (first Newton
+        iteration of a step from `time` with step `dt`): D, Dinv [N,4,4] and
+        the off-diagonal block of every half-side [H,4,4], reference order."""
+        n = self.case.n_cells
+        h = self.case.c.mesh.n_half_sides
+        D = np.zeros((n, 4, 4))
+        Di = np.zeros((n, 4, 4))
+        O = np.zeros((h, 4, 4))
+        dp = lambda a: a.ctypes.data_as(C.POINTER(C.c_double))
+        _check(N.lib.ccfd_build_matrix(self._ctx, float(time), float(dt), dp(D), dp(Di), dp(O)),
+               "ccfd_build_matrix")
+        return D, Di, O
+
+    def lusgs(self, b: np.ndarray) -> np.ndarray:
+        """LUSGS of b [N,4] with the blocks of the last build_matrix."""
+        n = self.case.n_cells
+        bb = np.ascontiguousarray(b, dtype=np.float64).reshape(n, 4)
+        x = np.zeros((n, 4))
+        dp = lambda a: a.ctypes.data_as(C.POINTER(C.c_double))
+        _check(N.lib.ccfd_lusgs(self._ctx, dp(bb), dp(x)), "ccfd_lusgs")
+        return x
+
 
 class Batch:
     """Many solvers stepped together on one device (see ccfd_batch_* in the

@@ -32,7 +32,7 @@ class Params(C.Structure):
         ("eps_newton", c_double), ("eps_gmres", c_double), ("gamma_ew", c_double),
         ("calc_wing", c_int), ("wall_id", c_int), ("ref_length", c_double),
         ("precision", c_int), ("rel_abort_residual", c_double),
-        ("source_func", c_int), ("exact_solution", c_int),
+        ("source_func", c_int), ("exact_solution", c_int), ("ser_cfl_max", c_double),
     ]
 
 
@@ -112,6 +112,9 @@ def _load():
         "ccfd_run_implicit": (c_int, [C.c_void_p, c_long, P(Report)]),
         "ccfd_global_residual": (c_int, [C.c_void_p, P(c_double)]),
         "ccfd_clcd": (c_int, [C.c_void_p, P(c_double), P(c_double)]),
+        "ccfd_build_matrix": (c_int, [C.c_void_p, c_double, c_double, P(c_double), P(c_double),
+                                      P(c_double)]),
+        "ccfd_lusgs": (c_int, [C.c_void_p, P(c_double), P(c_double)]),
         "ccfd_set_profiling": (c_int, [C.c_void_p, c_int]),
         "ccfd_get_profile": (c_int, [C.c_void_p, P(c_double), P(c_long), c_int]),
         "ccfd_global_residual_noalloc": (c_int, [C.c_void_p, C.c_void_p, c_long, c_double,

@@ -538,6 +538,8 @@ extern "C" int ccfd_upload_case(ccfd_ctx* ctx, const ccfd_mesh* m, const ccfd_bc
     c.print_iter = (0 / c.io_iter_interval + 1) * c.io_iter_interval;
     c.max_iter = p.max_iter;
     c.stop_at = 0;
+    c.cfl = p.cfl;
+    c.dfl = p.dfl;
     CK(cudaMemcpyAsync(ctx->ctrl, ctx->h_ctrl, sizeof(Ctrl), cudaMemcpyHostToDevice, ctx->stream));
     CK(cudaStreamSynchronize(ctx->stream));
 
@@ -546,6 +548,8 @@ extern "C" int ccfd_upload_case(ccfd_ctx* ctx, const ccfd_mesh* m, const ccfd_bc
     memset(&sp, 0, sizeof(sp));
     sp.cfl = p.cfl;
     sp.dfl = p.dfl;
+    sp.ser = p.implicit && p.ser_cfl_max > 0.0;
+    sp.ser_cfl_max = p.ser_cfl_max;
     sp.gam_pr_max = fmax(4.0 / 3.0, P.gam / P.Pr);
     for (int i = 0; i < 6; ++i) sp.rk[i] = ctx->rk[i];
     sp.nrk = (p.n_rk_stages == 1 && p.time_order == 1) ? 1 : p.n_rk_stages;
@@ -989,7 +993,7 @@ extern "C" int ccfd_time_step(ccfd_ctx* ctx, double* dt_out) {
     if (!ctx || !dt_out || !ctx->uploaded) return CCFD_ERR_ARG;
     if (ctx->batch) return CCFD_ERR_BUSY;
     CK(cudaSetDevice(ctx->device));
-    launch_dt(ctx->mesh, ctx->phys, nullptr, ctx->sp, cur_prim(ctx), ctx->dt_partial, ctx->dt_bad, ctx->stream);
+    launch_dt(ctx->mesh, ctx->phys, ctx->ctrl, ctx->sp, cur_prim(ctx), ctx->dt_partial, ctx->dt_bad, ctx->stream);
     CK(cudaGetLastError());
     std::vector<double2> part(ctx->nb_cells);
     std::vector<int> bad(ctx->nb_cells);

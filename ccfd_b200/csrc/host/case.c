@@ -541,6 +541,7 @@ int ccfd_case_load_text(const char *text, const char *base_dir, ccfd_case **out)
 	TRY(ccfd_ini_int(ini, "precision", "0", &lv));
 	P->precision = (int)lv;
 	TRY(ccfd_ini_dbl(ini, "relAbortResidual", "0", &P->rel_abort_residual));
+	TRY(ccfd_ini_dbl(ini, "serCFLmax", "0", &P->ser_cfl_max));
 
 	free(nodes); free(tria); free(quad); free(bcedge);
 	ccfd_ini_free(ini);

@@ -128,6 +128,8 @@ struct ImpState {
     int4 *fw_nb = nullptr, *fw_h = nullptr, *bw_nb = nullptr, *bw_h = nullptr;
     bool ready = false;
     void* solo = nullptr;        // the member set of this context running alone
+    std::vector<int> hs_off_h;   // device CSR offsets of the half-sides (host copy)
+    bool jac_built = false;      // ccfd_build_matrix has filled the blocks
 };
 
 __device__ __forceinline__ void ld(const double4& v, double q[4]) {
@@ -823,12 +825,6 @@ __global__ void kb_count(const ImpDev* __restrict__ I, int n, int what, int* out
 
 }  // namespace
 
-namespace ccfd {
-void imp_step_end_launch(Ctrl* ctrl, const StepParams& sp, const double* res_partial, int nres,
-                         const double2* dt_partial, const int* dt_bad, int ndt, const int* wall_ghost,
-                         const double* wall_nl, const double* ghost_pface, cudaStream_t st);
-}
-
 // ------------------------------------------------------------------- host
 #define CK(x)                               \
     do {                                    \
@@ -879,6 +875,7 @@ int ccfd_implicit_setup(ccfd_ctx* ctx, const std::vector<int>& hs_off, const std
     S->K = K;
     S->N = N;
     S->nb = (int)((N + kB - 1) / kB);
+    S->hs_off_h = hs_off;
     const long H = hs_off[N];
     int st;
     S->fp32 = ctx->params.precision == CCFD_MIXED;
@@ -1321,13 +1318,10 @@ static int set_step(ImpSet* M) {
     }
     // global residual of the final residual evaluation, stop tests and the
     // next dt (calcTimeStep of the new state) of the members that stepped
-    for (ccfd_ctx* ctx : M->members) {
-        launch_dt(ctx->mesh, ctx->phys, nullptr, ctx->sp, ctx->prim_buf[ctx->cur], ctx->dt_partial, ctx->dt_bad,
-                  st);
-        imp_step_end_launch(ctx->ctrl, ctx->sp, ctx->res_partial, ctx->tiles.n_tiles, ctx->dt_partial,
-                            ctx->dt_bad, ctx->nb_cells, ctx->wall_ghost, ctx->wall_nl, ctx->ghost_pface,
-                            ctx->prim_buf[ctx->cur], st);
-    }
+    for (ccfd_ctx* ctx : M->members)
+        imp_step_end_launch(ctx->ctrl, ctx->mesh, ctx->phys, ctx->sp, ctx->res_partial, ctx->tiles.n_tiles,
+                            ctx->dt_partial, ctx->dt_bad, ctx->nb_cells, ctx->wall_ghost, ctx->wall_nl,
+                            ctx->ghost_pface, ctx->prim_buf[ctx->cur], st);
     CKM(cudaGetLastError());
     return CCFD_OK;
 }
@@ -1414,6 +1408,143 @@ extern "C" int ccfd_run_implicit(ccfd_ctx* ctx, long nsteps, ccfd_report* report
     if (!ctx || !ctx->uploaded) return CCFD_ERR_ARG;
     if (ctx->batch) return CCFD_ERR_BUSY;
     return run_implicit(ctx, nsteps, report);
+}
+
+// the member set of a context alone (built on first use)
+static int solo_set(ccfd_ctx* ctx, ImpSet** out) {
+    ImpState* S = (ImpState*)ctx->implicit_state;
+    if (!S || !S->ready) return CCFD_ERR_ARG;
+    if (!S->solo) {
+        ImpSet* M = nullptr;
+        int s = set_build({ctx}, ctx->stream, &M);
+        S->solo = M;
+        if (s) return s;
+    }
+    *out = (ImpSet*)S->solo;
+    return CCFD_OK;
+}
+
+// buildMatrix + calcDinv (src/linearSolver.c:136-252) at the context's state
+// as at the first Newton iteration of an implicit step from t with time step
+// dt, the blocks copied out in the reference's cell and half-side order.
+extern "C" int ccfd_build_matrix(ccfd_ctx* ctx, double t, double dt, double* d_out, double* dinv_out,
+                                 double* off_out) {
+    if (!ctx || !ctx->uploaded || !ctx->params.implicit || !ctx->params.precond) return CCFD_ERR_ARG;
+    if (ctx->batch) return CCFD_ERR_BUSY;
+    CK(cudaSetDevice(ctx->device));
+    ImpSet* M = nullptr;
+    int s = solo_set(ctx, &M);
+    if (s) return s;
+    ImpState* S = (ImpState*)ctx->implicit_state;
+    cudaStream_t st = ctx->stream;
+    const long N = S->N, H = S->hs_off_h[N];
+    // the step's control block (t, dt) and member words (Newton on, no GMRES
+    // cycle), restored afterwards
+    CK(cudaMemcpyAsync(ctx->h_ctrl, ctx->ctrl, sizeof(Ctrl), cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    const Ctrl saved = *ctx->h_ctrl;
+    Ctrl c = saved;
+    c.t = t;
+    c.dt = dt;
+    c.active = 1;
+    c.done = 0;
+    int ctl[CTL_WORDS] = {0};
+    ctl[CTL_NEWTON] = 1;
+    ctl[CTL_SKIP_GMRES] = 1;
+    CK(cudaMemcpyAsync(ctx->ctrl, &c, sizeof(Ctrl), cudaMemcpyHostToDevice, st));
+    CK(cudaMemcpyAsync(S->ctl, ctl, sizeof(ctl), cudaMemcpyHostToDevice, st));
+    CK(cudaMemsetAsync(S->flag, 0, sizeof(int) * 8, st));
+    // boundary sides have no block: zero, as the reference's untouched
+    // dense entries
+    if (S->fp32) CK(cudaMemsetAsync(S->Of, 0, sizeof(float) * 16 * (size_t)H, st));
+    else CK(cudaMemsetAsync(S->O, 0, sizeof(double) * 16 * (size_t)H, st));
+    const dim3 gv(M->max_nb, M->n), g1(1, M->n);
+    residuals(M, REC_NT);  // R_XK = R(U, t + dt)
+    kb_jac_copy<<<gv, kB, 0, st>>>(M->dev);
+    const dim3 gc((M->max_colsize + kB - 1) / kB, M->n);
+    for (int col = 0; col < M->max_col; ++col) {
+        kb_jac_gate<<<g1, 32, 0, st>>>(M->dev, col);
+        for (int v = 0; v < 4; ++v) {
+            kb_jac_perturb<<<gc, kB, 0, st>>>(M->dev, col, v, 1);
+            residuals(M, REC_JAC);
+            kb_jac_collect<<<gc, kB, 0, st>>>(M->dev, col, v);
+            kb_jac_perturb<<<gc, kB, 0, st>>>(M->dev, col, v, 0);
+        }
+    }
+    kb_jac_finish<<<gv, kB, 0, st>>>(M->dev);
+    CK(cudaGetLastError());
+    std::vector<double> D(16 * N), Di(16 * N), O(16 * H);
+    int flag[8];
+    CK(cudaMemcpyAsync(D.data(), S->D, sizeof(double) * D.size(), cudaMemcpyDeviceToHost, st));
+    if (S->fp32) {
+        std::vector<float> a(16 * N), b(16 * H);
+        CK(cudaMemcpyAsync(a.data(), S->Dinvf, sizeof(float) * a.size(), cudaMemcpyDeviceToHost, st));
+        CK(cudaMemcpyAsync(b.data(), S->Of, sizeof(float) * b.size(), cudaMemcpyDeviceToHost, st));
+        CK(cudaStreamSynchronize(st));
+        for (size_t k = 0; k < a.size(); ++k) Di[k] = a[k];
+        for (size_t k = 0; k < b.size(); ++k) O[k] = b[k];
+    } else {
+        CK(cudaMemcpyAsync(Di.data(), S->Dinv, sizeof(double) * Di.size(), cudaMemcpyDeviceToHost, st));
+        CK(cudaMemcpyAsync(O.data(), S->O, sizeof(double) * O.size(), cudaMemcpyDeviceToHost, st));
+    }
+    CK(cudaMemcpyAsync(flag, S->flag, sizeof(flag), cudaMemcpyDeviceToHost, st));
+    int zero[CTL_WORDS] = {0};
+    CK(cudaMemcpyAsync(ctx->ctrl, &saved, sizeof(Ctrl), cudaMemcpyHostToDevice, st));
+    CK(cudaMemcpyAsync(S->ctl, zero, sizeof(zero), cudaMemcpyHostToDevice, st));
+    CK(cudaStreamSynchronize(st));
+    *ctx->h_ctrl = saved;
+    S->jac_built = true;
+    // device order -> reference order (cells keep their side order)
+    long ho = 0;
+    for (long cr = 0; cr < N; ++cr) {
+        const int d = ctx->dev_of_cell[cr];
+        const int h0 = S->hs_off_h[d], nh = S->hs_off_h[d + 1] - h0;
+        if (d_out) memcpy(d_out + 16 * cr, &D[16 * (size_t)d], sizeof(double) * 16);
+        if (dinv_out) memcpy(dinv_out + 16 * cr, &Di[16 * (size_t)d], sizeof(double) * 16);
+        if (off_out) memcpy(off_out + 16 * ho, &O[16 * (size_t)h0], sizeof(double) * 16 * nh);
+        ho += nh;
+    }
+    return flag[2] ? CCFD_ERR_SINGULAR : CCFD_OK;
+}
+
+// LUSGS (src/linearSolver.c:261-333) of b with the blocks of the last
+// ccfd_build_matrix, in the reference's cell order.
+extern "C" int ccfd_lusgs(ccfd_ctx* ctx, const double* b, double* x) {
+    if (!ctx || !b || !x || !ctx->uploaded) return CCFD_ERR_ARG;
+    if (ctx->batch) return CCFD_ERR_BUSY;
+    ImpState* S = (ImpState*)ctx->implicit_state;
+    if (!S || !S->jac_built) return CCFD_ERR_ARG;
+    CK(cudaSetDevice(ctx->device));
+    ImpSet* M = nullptr;
+    int s = solo_set(ctx, &M);
+    if (s) return s;
+    cudaStream_t st = ctx->stream;
+    const long N = S->N;
+    std::vector<double> h(4 * N);
+    for (long d = 0; d < N; ++d) memcpy(&h[4 * d], b + 4 * (size_t)ctx->cell_of_dev[d], sizeof(double) * 4);
+    std::vector<float> hf;
+    if (S->fp32) {
+        hf.assign(h.begin(), h.end());
+        CK(cudaMemcpyAsync(S->Vf, hf.data(), sizeof(float) * hf.size(), cudaMemcpyHostToDevice, st));
+    } else {
+        CK(cudaMemcpyAsync(S->V, h.data(), sizeof(double) * h.size(), cudaMemcpyHostToDevice, st));
+    }
+    int ctl[CTL_WORDS] = {0};  // GMRES "on": the sweep runs
+    CK(cudaMemcpyAsync(S->ctl, ctl, sizeof(ctl), cudaMemcpyHostToDevice, st));
+    if (S->fp32) {
+        kb_lusgs<kSweepThreads, float><<<M->n, kSweepThreads, 0, st>>>(M->dev, 0);
+        CK(cudaGetLastError());
+        CK(cudaMemcpyAsync(hf.data(), S->Zf, sizeof(float) * hf.size(), cudaMemcpyDeviceToHost, st));
+        CK(cudaStreamSynchronize(st));
+        for (size_t k = 0; k < hf.size(); ++k) h[k] = hf[k];
+    } else {
+        kb_lusgs<kSweepThreads, double><<<M->n, kSweepThreads, 0, st>>>(M->dev, 0);
+        CK(cudaGetLastError());
+        CK(cudaMemcpyAsync(h.data(), S->Z, sizeof(double) * h.size(), cudaMemcpyDeviceToHost, st));
+        CK(cudaStreamSynchronize(st));
+    }
+    for (long d = 0; d < N; ++d) memcpy(x + 4 * (size_t)ctx->cell_of_dev[d], &h[4 * d], sizeof(double) * 4);
+    return CCFD_OK;
 }
 
 // ---------------------------------------------------------------- batching

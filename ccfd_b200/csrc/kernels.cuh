@@ -93,9 +93,9 @@ void launch_exact_state(int n, const double4* xq, const Phys* phys_g, int which,
 void launch_errors(const DevMesh& m, const double4* xq, const double4* prim, const double4* grad,
                    const Phys* phys_g, int which, double time, double* partial, unsigned* flags,
                    cudaStream_t st);
-void imp_step_end_launch(Ctrl* ctrl, const StepParams& sp, const double* res_partial, int nres,
-                         const double2* dt_partial, const int* dt_bad, int ndt, const int* wall_ghost,
-                         const double* wall_nl, const double* ghost_pface, const double4* prim_new,
-                         cudaStream_t st);
+void imp_step_end_launch(Ctrl* ctrl, const DevMesh& m, const Phys& P, const StepParams& sp,
+                         const double* res_partial, int nres, double2* dt_partial, int* dt_bad, int ndt,
+                         const int* wall_ghost, const double* wall_nl, const double* ghost_pface,
+                         const double4* prim_new, cudaStream_t st);
 
 }  // namespace ccfd

@@ -43,6 +43,7 @@ struct Ctrl {
     double cl, cd;
     double visc_dominates;
     int par;         // primitive buffer holding the current state (batched RK runs)
+    double cfl, dfl; // CFL / DFL numbers of the next time step (switched evolution relaxation)
 };
 
 // Run parameters of the explicit integrator (kernel argument).
@@ -66,6 +67,11 @@ struct StepParams {
     double* hist;
     int hist_cap, hist_width, n_rec;
     const int* rec_cell;  // [n_rec] device cell of each record point
+    // switched evolution relaxation of the CFL number (implicit runs):
+    // Ctrl::cfl = min(ser_cfl_max, cfl * r_1 / r_n) after step n,
+    // Ctrl::dfl = dfl * Ctrl::cfl / cfl
+    double ser_cfl_max;
+    int ser, ser_pad;
 };
 
 // history row: iteration, t after the step, dt, residuals [6], CL, CD, then

@@ -9,17 +9,20 @@
 
 namespace ccfd {
 
-// per-block minima of the convective and viscous time steps
+// per-block minima of the convective and viscous time steps; the CFL
+// number is the control block's under switched evolution relaxation
 __global__ void __launch_bounds__(256) k_dt(DevMesh m, Phys P, const Ctrl* ctrl, StepParams sp,
                                             const double4* __restrict__ prim,
                                             double2* __restrict__ partial, int* bad_partial) {
     int c = blockIdx.x * blockDim.x + threadIdx.x;
     double dconv = 1e150, dvisc = 1e150;
     int bad = 0;
+    const double cfl = (ctrl && sp.ser) ? ctrl->cfl : sp.cfl;
+    const double dfl = (ctrl && sp.ser) ? ctrl->dfl : sp.dfl;
     if (c < m.N) {
         double q[4];
         ld4(prim[c], q);
-        if (!local_dt(P, sp, q, m.cell_geo[c], &dconv, &dvisc)) {
+        if (!local_dt(P, sp, cfl, dfl, q, m.cell_geo[c], &dconv, &dvisc)) {
             bad = 1;
             dconv = dvisc = 1e150;
         }
@@ -70,22 +73,34 @@ __global__ void k_step_begin(Ctrl* ctrl, StepParams sp, const double2* __restric
 }
 
 // end of an implicit step (the residual partials come from the last
-// residual evaluation, the dt partials from k_dt of the new state)
+// residual evaluation): global residual, stop tests and the CFL number of
+// the next step; its dt follows from k_dt and k_step_dt
 __global__ void k_step_end_sep(Ctrl* ctrl, StepParams sp, const double* res_partial, int nres,
-                               const double2* dt_partial, const int* dt_bad, int ndt,
                                const int* wall_ghost, const double* wall_nl,
                                const double* ghost_pface, const double4* prim_new) {
     if (!ctrl->active) return;
-    step_end_block(ctrl, sp, res_partial, nres, dt_partial, dt_bad, ndt, wall_ghost, wall_nl,
-                   ghost_pface, prim_new);
+    step_end_block(ctrl, sp, res_partial, nres, nullptr, nullptr, 0, wall_ghost, wall_nl, ghost_pface,
+                   prim_new, false);
 }
 
-void imp_step_end_launch(Ctrl* ctrl, const StepParams& sp, const double* res_partial, int nres,
-                         const double2* dt_partial, const int* dt_bad, int ndt, const int* wall_ghost,
-                         const double* wall_nl, const double* ghost_pface, const double4* prim_new,
-                         cudaStream_t st) {
-    k_step_end_sep<<<1, 256, 0, st>>>(ctrl, sp, res_partial, nres, dt_partial, dt_bad, ndt, wall_ghost,
-                                      wall_nl, ghost_pface, prim_new);
+// dt of the next step of a member that steps on (calcTimeStep of the new
+// state, src/timeDiscretization.c:249-329)
+__global__ void k_step_dt(Ctrl* ctrl, StepParams sp, const double2* __restrict__ partial,
+                          const int* __restrict__ bad_partial, int nb) {
+    double a, b;
+    int bad;
+    reduce_min2(partial, bad_partial, nb, &a, &b, &bad);
+    if (threadIdx.x != 0 || !ctrl->active) return;
+    finish_dt(ctrl, sp, a, b, bad);
+}
+
+void imp_step_end_launch(Ctrl* ctrl, const DevMesh& m, const Phys& P, const StepParams& sp,
+                         const double* res_partial, int nres, double2* dt_partial, int* dt_bad, int ndt,
+                         const int* wall_ghost, const double* wall_nl, const double* ghost_pface,
+                         const double4* prim_new, cudaStream_t st) {
+    k_step_end_sep<<<1, 256, 0, st>>>(ctrl, sp, res_partial, nres, wall_ghost, wall_nl, ghost_pface, prim_new);
+    launch_dt(m, P, ctrl, sp, prim_new, dt_partial, dt_bad, st);
+    k_step_dt<<<1, 256, 0, st>>>(ctrl, sp, dt_partial, dt_bad, ndt);
 }
 
 

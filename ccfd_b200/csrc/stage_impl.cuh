@@ -288,21 +288,22 @@ __device__ __forceinline__ void block_min2(double a, double b, int bad, double2*
 }
 
 // local convective / viscous time step of one cell (calcTimeStep,
-// src/timeDiscretization.c:253-308); returns false if not finite
-__device__ __forceinline__ bool local_dt(const Phys& P, const StepParams& sp, const double q[4],
-                                         double4 geo, double* dc, double* dv) {
+// src/timeDiscretization.c:253-308) at CFL number cfl; returns false if not
+// finite
+__device__ __forceinline__ bool local_dt(const Phys& P, const StepParams& sp, double cfl, double dfl,
+                                         const double q[4], double4 geo, double* dc, double* dv) {
     double a = sqrt(P.gam * q[3] / q[0]);
     *dv = 1e150;
     if (sp.ts1d) {
-        *dc = sp.cfl * geo.w / (fabs(q[1]) + a);
+        *dc = cfl * geo.w / (fabs(q[1]) + a);
         return isfinite(*dc);
     }
     double ssr = (fabs(q[1]) + a) * geo.z + (fabs(q[2]) + a) * geo.w;
-    *dc = sp.cfl * geo.x / ssr;
+    *dc = cfl * geo.x / ssr;
     bool ok = isfinite(*dc);
     if (sp.visc) {
         double ssv = sp.gam_pr_max * P.mu * geo.z * geo.z + sp.gam_pr_max * P.mu * geo.w * geo.w;
-        *dv = sp.dfl * q[0] * q[0] * geo.x * geo.x / (4.0 * ssv);
+        *dv = dfl * q[0] * q[0] * geo.x * geo.x / (4.0 * ssv);
         ok = ok && isfinite(*dv);
     }
     return ok;
@@ -328,11 +329,15 @@ __device__ __forceinline__ void finish_dt(Ctrl* ctrl, const StepParams& sp, doub
 
 // End of a step, executed by one whole block: global residual (fixed-order
 // reduction of the per-tile partials), wing coefficients, t += dt, the stop
-// tests of timeDisc (src/timeDiscretization.c:609-731) and the next dt.
+// tests of timeDisc (src/timeDiscretization.c:609-731), the CFL number of
+// the next step under switched evolution relaxation and, with with_dt, the
+// next dt from the partial minima (otherwise a later k_step_dt computes it
+// at the new CFL number).
 __device__ __forceinline__ void step_end_block(Ctrl* ctrl, const StepParams& sp, const double* res_partial,
                                int nres, const double2* dt_partial, const int* dt_bad, int ndt,
                                const int* wall_ghost, const double* wall_nl,
-                               const double* ghost_pface, const double4* prim_new) {
+                               const double* ghost_pface, const double4* prim_new,
+                               bool with_dt = true) {
     __shared__ double s_res[4];
     __shared__ double2 s_dt;
     __shared__ int s_bad;
@@ -403,6 +408,12 @@ __device__ __forceinline__ void step_end_block(Ctrl* ctrl, const StepParams& sp,
         for (int v = 0; v < 4; ++v) ctrl->res_first[v] = res[v];
         ctrl->have_first = 1;
     }
+    // switched evolution relaxation (Mulder and van Leer, 1985): the CFL
+    // number of the next step from the first and the latest residual
+    if (sp.ser && res[sp.abort_variable] > 0.0) {
+        ctrl->cfl = fmin(sp.ser_cfl_max, sp.cfl * ctrl->res_first[sp.abort_variable] / res[sp.abort_variable]);
+        ctrl->dfl = sp.dfl * ctrl->cfl / sp.cfl;
+    }
     bool nonfinite = false;
 #pragma unroll
     for (int v = 0; v < 4; ++v) nonfinite |= !isfinite(res[v]);
@@ -445,7 +456,7 @@ __device__ __forceinline__ void step_end_block(Ctrl* ctrl, const StepParams& sp,
     }
     if (iter >= ctrl->stop_at) return;
     ctrl->active = 1;
-    finish_dt(ctrl, sp, s_dt.x, s_dt.y, s_bad);
+    if (with_dt) finish_dt(ctrl, sp, s_dt.x, s_dt.y, s_bad);
 }
 
 // fused residual evaluation (+ RK stage) of tile t by one CTA; FT is the
@@ -617,7 +628,7 @@ __device__ __forceinline__ void stage_body(const StageLaunch& L, const int t) {
             if (L.last_stage) {
                 L.cons0[d] = mk4(cn);
                 double a, b;
-                if (!local_dt(P, L.sp, pn, geo, &a, &b)) bad = 1;
+                if (!local_dt(P, L.sp, L.sp.cfl, L.sp.dfl, pn, geo, &a, &b)) bad = 1;
                 else {
                     dconv = fmin(dconv, a);
                     dvisc = fmin(dvisc, b);

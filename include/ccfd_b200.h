@@ -104,6 +104,13 @@ typedef struct ccfd_params {
 	double rel_abort_residual; /* >0: stop when res/res_first <= this (extension) */
 	int source_func;       /* calcSource / sourceFunction (0: none), src/source.c */
 	int exact_solution;    /* exactSolution (error norms at the end of a run) */
+	double ser_cfl_max;    /* >0: implicit runs ramp the CFL number by switched
+				  evolution relaxation (Mulder and van Leer, 1985):
+				  before step n >= 2, CFL = min(ser_cfl_max,
+				  CFL_0 * r_1 / r_{n-1}), r the abort variable's
+				  global residual after a step, and DFL =
+				  DFL_0 * CFL / CFL_0 (extension, key serCFLmax;
+				  0: the reference's fixed CFL and DFL) */
 } ccfd_params;
 
 /* one boundary condition, src/boundary.h:19-46, parsed by initBoundary
@@ -300,8 +307,24 @@ int ccfd_run_explicit(ccfd_ctx *ctx, long nsteps, ccfd_report *report);
  * (src/timeDiscretization.c:412-552) with GMRES_M (src/linearSolver.c:
  * 385-510), matrixVector (:343-373) and, if params.precond, the LU-SGS
  * preconditioner (buildMatrix :186-252, calcDinv :136-179, LUSGS :261-333)
- * on block-sparse storage. */
+ * on block-sparse storage.  With params.ser_cfl_max > 0 the CFL number of
+ * each step follows switched evolution relaxation (see ccfd_params). */
 int ccfd_run_implicit(ccfd_ctx *ctx, long nsteps, ccfd_report *report);
+/* buildMatrix + calcDinv (src/linearSolver.c:186-252, :136-179) at the
+ * context's state, as at the first Newton iteration of an implicit step from
+ * time t with step dt: R_XK = R(U, t + dt), the finite-difference columns
+ * R(U + sqrt(DBL_EPSILON) e_k, t) of the primitive variables.  Out (each may
+ * be NULL), reference cell order, row-major 4x4 blocks (rows: residual
+ * variables, columns: perturbed primitive variables): d and dinv [N][16],
+ * the diagonal blocks of I - dt dR/dU and their inverses; off [H][16], per
+ * half-side (reference side order) the block of its cell's row and the
+ * column of the cell across it (zero at boundary sides).  Needs implicit
+ * and precond.  CCFD_ERR_SINGULAR as calcDinv's exit. */
+int ccfd_build_matrix(ccfd_ctx *ctx, double t, double dt, double *d, double *dinv, double *off);
+/* LUSGS (src/linearSolver.c:261-333): x = M^-1 b with the blocks of the last
+ * ccfd_build_matrix, b and x [N][4] in reference cell order (mixed
+ * precision: the sweep runs on the FP32 blocks). */
+int ccfd_lusgs(ccfd_ctx *ctx, const double *b, double *x);
 /* Profiling of the residual evaluations inside the timed step graphs: with
  * profiling on, every residual evaluation of a step (gradient, face flux and
  * update kernels of one Runge-Kutta stage) is bracketed by CUDA events on the

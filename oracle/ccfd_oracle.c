@@ -674,6 +674,172 @@ static void o_ghost_bary(orc *o, long b, double t, const double *prim, double ou
 		   &m->bc_ghost_bary[2 * b]);
 }
 
+/* Limited least-squares gradient of cell c (spatialReconstruction,
+ * src/reconstruction.c:252-275, limiters :25-192): neighbour states from
+ * prim, ghost states at the mirrored barycentres from gb; g = (u_x[4],
+ * u_y[4]). */
+static void o_gradient(const orc *o, const ccfd_mesh *m, const double *prim, const double *gb,
+		       long c, double g[8])
+{
+	const double *q = &prim[4 * c];
+	double *ux = g, *uy = g + 4;
+	for (int v = 0; v < NV; ++v)
+		ux[v] = uy[v] = 0.0;
+	for (long h = m->hs_offset[c]; h < m->hs_offset[c + 1]; ++h) {
+		long nb = m->hs_nb[h];
+		const double *qn = nb >= 0 ? &prim[4 * nb] : &gb[4 * (-1 - nb)];
+		for (int v = 0; v < NV; ++v) {
+			double d = qn[v] - q[v];
+			ux[v] += m->hs_w[2 * h] * d;
+			uy[v] += m->hs_w[2 * h + 1] * d;
+		}
+	}
+	double lo[4], hi[4], phi[4] = {1.0, 1.0, 1.0, 1.0};
+	memcpy(lo, q, sizeof(lo));
+	memcpy(hi, q, sizeof(hi));
+	for (long h = m->hs_offset[c]; h < m->hs_offset[c + 1]; ++h) {
+		long nb = m->hs_nb[h];
+		const double *qn = nb >= 0 ? &prim[4 * nb] : &gb[4 * (-1 - nb)];
+		for (int v = 0; v < NV; ++v) {
+			lo[v] = fmin(lo[v], qn[v]);
+			hi[v] = fmax(hi[v], qn[v]);
+		}
+	}
+	for (long h = m->hs_offset[c]; h < m->hs_offset[c + 1]; ++h) {
+		for (int v = 0; v < NV; ++v) {
+			double mn = lo[v] - q[v], mx = hi[v] - q[v];
+			double d = ux[v] * m->hs_gp[2 * h] + uy[v] * m->hs_gp[2 * h + 1];
+			double ph = 1.0;
+			if (o->limiter == CCFD_LIM_BARTH_JESPERSEN) {
+				/* src/reconstruction.c:25-96 */
+				if (d > 0.0)
+					ph = fmin(1.0, mx / d);
+				else if (d < 0.0)
+					ph = fmin(1.0, mn / d);
+			} else {
+				/* src/reconstruction.c:103-192 */
+				double e2 = o->eps2[c], d2 = d * d;
+				if (d > 0.0)
+					ph = 1.0 / d * (((mx * mx + e2) * d + 2.0 * d2 * mx) /
+							(mx * mx + 2.0 * d2 + d * mx + e2));
+				else if (d < 0.0)
+					ph = 1.0 / d * (((mn * mn + e2) * d + 2.0 * d2 * mn) /
+							(mn * mn + 2.0 * d2 + d * mn + e2));
+			}
+			phi[v] = fmin(phi[v], ph);
+		}
+	}
+	for (int v = 0; v < NV; ++v) {
+		ux[v] *= phi[v];
+		uy[v] *= phi[v];
+	}
+}
+
+/* Flux of face f times its length (setBCatSides + fluxCalculation,
+ * src/boundary.c:300-314, src/fluxCalculation.c:882-998): gradients g
+ * ([N][8], zero in first order), ghost states gb. */
+static void o_face_flux(orc *o, const ccfd_case *cs, const double *prim, const double *g,
+			const double *gb, long f, double t, double F4[4], double *wall_p)
+{
+	const ccfd_mesh *m = &cs->mesh;
+	long c0 = m->face_cells[2 * f], c1 = m->face_cells[2 * f + 1];
+	long h0 = m->face_hs[2 * f], h1 = m->face_hs[2 * f + 1];
+	const double *n = &m->face_n[2 * f];
+	double L[4], R[4], q1[4] = {0, 0, 0, 0};
+	const double *g1x = NULL, *g1y = NULL;
+	static const double zero4[4] = {0, 0, 0, 0};
+	for (int v = 0; v < NV; ++v)
+		L[v] = prim[4 * c0 + v] + m->hs_gp[2 * h0] * g[8 * c0 + v] +
+		       m->hs_gp[2 * h0 + 1] * g[8 * c0 + 4 + v];
+	if (c1 >= 0) {
+		for (int v = 0; v < NV; ++v) {
+			R[v] = prim[4 * c1 + v] + m->hs_gp[2 * h1] * g[8 * c1 + v] +
+			       m->hs_gp[2 * h1 + 1] * g[8 * c1 + 4 + v];
+			q1[v] = prim[4 * c1 + v];
+		}
+		g1x = &g[8 * c1];
+		g1y = &g[8 * c1 + 4];
+	} else {
+		long b = -1 - c1;
+		o_boundary(o, &cs->bc_table[m->bc_index[b]], n, t, L, R, &m->bc_x[2 * b]);
+		if (wall_p)
+			wall_p[b] = L[3];
+		memcpy(q1, &gb[4 * b], sizeof(q1));
+		g1x = g1y = zero4;
+	}
+	fin s = {L[0], R[0], n[0] * L[1] + n[1] * L[2], n[0] * R[1] + n[1] * R[2],
+		 -n[1] * L[1] + n[0] * L[2], -n[1] * R[1] + n[0] * R[2], L[3], R[3]};
+	double fc[4];
+	o_flux(o, &s, fc);
+	F4[0] = fc[0];
+	F4[1] = n[0] * fc[1] - n[1] * fc[2];
+	F4[2] = n[1] * fc[1] + n[0] * fc[2];
+	F4[3] = fc[3];
+	if (o->eqn == CCFD_NAVIER_STOKES) {
+		const double *bb = &m->face_bb[3 * f];
+		double bx = bb[0] / bb[2], by = bb[1] / bb[2];
+		double st[4], gx[4], gy[4], fx[4], fy[4];
+		for (int v = 0; v < NV; ++v) {
+			st[v] = 0.5 * (R[v] + L[v]);
+			double mx = 0.5 * (g[8 * c0 + v] + g1x[v]);
+			double my = 0.5 * (g[8 * c0 + 4 + v] + g1y[v]);
+			double corr = mx * bx + my * by - (q1[v] - prim[4 * c0 + v]) / bb[2];
+			gx[v] = mx - corr * bx;
+			gy[v] = my - corr * by;
+		}
+		/* diffusionFlux, src/fluxCalculation.c:855-873 */
+		double mu = o->mu, k = o->gam / (o->gam1 * o->Pr * st[0] * st[0]);
+		fx[0] = fy[0] = 0.0;
+		fx[1] = (4.0 / 3.0 * gx[1] - 2.0 / 3.0 * gy[2]) * mu;
+		fx[2] = (gy[1] + gx[2]) * mu;
+		fx[3] = (4.0 / 3.0 * st[1] * gx[1] - 2.0 / 3.0 * st[1] * gy[2] + (gx[2] + gy[1]) * st[2]
+			 + k * (st[0] * gx[3] - st[3] * gx[0])) * mu;
+		fy[1] = (gy[1] + gx[2]) * mu;
+		fy[2] = (4.0 / 3.0 * gy[2] - 2.0 / 3.0 * gx[1]) * mu;
+		fy[3] = (4.0 / 3.0 * st[2] * gy[2] - 2.0 / 3.0 * st[2] * gx[1] + (gy[1] + gx[2]) * st[1]
+			 + k * (st[0] * gy[3] - st[3] * gy[0])) * mu;
+		for (int v = 0; v < NV; ++v)
+			F4[v] -= (fx[v] * n[0] + fy[v] * n[1]);
+	}
+	for (int v = 0; v < NV; ++v)
+		F4[v] *= m->face_len[f];
+}
+
+/* u_t of cell c from the face fluxes ff ([F][4]) in side-list order
+ * (src/finiteVolume.c:96-120) */
+static void o_cell_ut(const orc *o, const ccfd_case *cs, const double *ff, long c, double t,
+		      double ut[4])
+{
+	const ccfd_mesh *m = &cs->mesh;
+	double s[4] = {0.0, 0.0, 0.0, 0.0};
+	for (long h = m->hs_offset[c]; h < m->hs_offset[c + 1]; ++h) {
+		const double *F4 = &ff[4 * m->hs_face[h]];
+		for (int v = 0; v < NV; ++v)
+			s[v] += m->hs_sign[h] > 0 ? F4[v] : -F4[v];
+	}
+	double src[4] = {0.0, 0.0, 0.0, 0.0};
+	if (cs->params.source_func)
+		o_cell_source(o, m, c, t, src);
+	for (int v = 0; v < NV; ++v)
+		ut[v] = (src[v] - s[v]) * m->cell_geo[4 * c + 1];
+}
+
+static double *o_venk_eps2(const ccfd_case *cs)
+{
+	const ccfd_mesh *m = &cs->mesh;
+	if (cs->params.spatial_order != 2 || cs->params.limiter != CCFD_LIM_VENKATAKRISHNAN)
+		return NULL;
+	double *eps2 = malloc(sizeof(double) * m->n_cells);
+	if (!eps2)
+		return NULL;
+	for (long e = 0; e < m->n_cells; ++e) {
+		double a = m->cell_geo[4 * e];
+		eps2[e] = (cs->params.venk_k * sqrt(a)) * (cs->params.venk_k * sqrt(a)) *
+			  (cs->params.venk_k * sqrt(a));
+	}
+	return eps2;
+}
+
 /* Residual R(U) of primitive state prim at time t.  grad (N x 8) and fflux
  * (F x 4) are optional outputs (limited gradients, face fluxes). */
 int oracle_residual(const ccfd_case *cs, const double *prim, double t, double *u_t,
@@ -682,15 +848,7 @@ int oracle_residual(const ccfd_case *cs, const double *prim, double t, double *u
 	const ccfd_mesh *m = &cs->mesh;
 	const long N = m->n_cells, F = m->n_faces, B = m->n_bc;
 	orc o;
-	double *eps2 = NULL;
-	if (cs->params.spatial_order == 2 && cs->params.limiter == CCFD_LIM_VENKATAKRISHNAN) {
-		eps2 = malloc(sizeof(double) * N);
-		for (long e = 0; e < N; ++e) {
-			double a = m->cell_geo[4 * e];
-			eps2[e] = (cs->params.venk_k * sqrt(a)) * (cs->params.venk_k * sqrt(a)) *
-				  (cs->params.venk_k * sqrt(a));
-		}
-	}
+	double *eps2 = o_venk_eps2(cs);
 	o_init(&o, cs, eps2);
 	double *g = calloc(8 * N, sizeof(double));
 	double *gb = calloc(4 * (B + 1), sizeof(double));
@@ -703,142 +861,13 @@ int oracle_residual(const ccfd_case *cs, const double *prim, double t, double *u
 	if (o.order == 2) {
 		for (long b = 0; b < B; ++b)
 			o_ghost_bary(&o, b, t, prim, &gb[4 * b]);
-		for (long c = 0; c < N; ++c) {
-			const double *q = &prim[4 * c];
-			double *ux = &g[8 * c], *uy = &g[8 * c + 4];
-			for (long h = m->hs_offset[c]; h < m->hs_offset[c + 1]; ++h) {
-				long nb = m->hs_nb[h];
-				const double *qn = nb >= 0 ? &prim[4 * nb] : &gb[4 * (-1 - nb)];
-				for (int v = 0; v < NV; ++v) {
-					double d = qn[v] - q[v];
-					ux[v] += m->hs_w[2 * h] * d;
-					uy[v] += m->hs_w[2 * h + 1] * d;
-				}
-			}
-		}
-		for (long c = 0; c < N; ++c) {
-			const double *q = &prim[4 * c];
-			double *ux = &g[8 * c], *uy = &g[8 * c + 4];
-			double lo[4], hi[4], phi[4] = {1.0, 1.0, 1.0, 1.0};
-			memcpy(lo, q, sizeof(lo));
-			memcpy(hi, q, sizeof(hi));
-			for (long h = m->hs_offset[c]; h < m->hs_offset[c + 1]; ++h) {
-				long nb = m->hs_nb[h];
-				const double *qn = nb >= 0 ? &prim[4 * nb] : &gb[4 * (-1 - nb)];
-				for (int v = 0; v < NV; ++v) {
-					lo[v] = fmin(lo[v], qn[v]);
-					hi[v] = fmax(hi[v], qn[v]);
-				}
-			}
-			for (long h = m->hs_offset[c]; h < m->hs_offset[c + 1]; ++h) {
-				for (int v = 0; v < NV; ++v) {
-					double mn = lo[v] - q[v], mx = hi[v] - q[v];
-					double d = ux[v] * m->hs_gp[2 * h] + uy[v] * m->hs_gp[2 * h + 1];
-					double ph = 1.0;
-					if (o.limiter == CCFD_LIM_BARTH_JESPERSEN) {
-						/* src/reconstruction.c:25-96 */
-						if (d > 0.0)
-							ph = fmin(1.0, mx / d);
-						else if (d < 0.0)
-							ph = fmin(1.0, mn / d);
-					} else {
-						/* src/reconstruction.c:103-192 */
-						double e2 = eps2[c], d2 = d * d;
-						if (d > 0.0)
-							ph = 1.0 / d * (((mx * mx + e2) * d + 2.0 * d2 * mx) /
-									(mx * mx + 2.0 * d2 + d * mx + e2));
-						else if (d < 0.0)
-							ph = 1.0 / d * (((mn * mn + e2) * d + 2.0 * d2 * mn) /
-									(mn * mn + 2.0 * d2 + d * mn + e2));
-					}
-					phi[v] = fmin(phi[v], ph);
-				}
-			}
-			for (int v = 0; v < NV; ++v) {
-				ux[v] *= phi[v];
-				uy[v] *= phi[v];
-			}
-		}
+		for (long c = 0; c < N; ++c)
+			o_gradient(&o, m, prim, gb, c, &g[8 * c]);
 	}
-	/* setBCatSides + fluxCalculation, src/boundary.c:300-314,
-	 * src/fluxCalculation.c:882-998 */
-	for (long f = 0; f < F; ++f) {
-		long c0 = m->face_cells[2 * f], c1 = m->face_cells[2 * f + 1];
-		long h0 = m->face_hs[2 * f], h1 = m->face_hs[2 * f + 1];
-		const double *n = &m->face_n[2 * f];
-		double L[4], R[4], q1[4] = {0, 0, 0, 0};
-		const double *g1x = NULL, *g1y = NULL;
-		static const double zero4[4] = {0, 0, 0, 0};
-		for (int v = 0; v < NV; ++v)
-			L[v] = prim[4 * c0 + v] + m->hs_gp[2 * h0] * g[8 * c0 + v] +
-			       m->hs_gp[2 * h0 + 1] * g[8 * c0 + 4 + v];
-		if (c1 >= 0) {
-			for (int v = 0; v < NV; ++v) {
-				R[v] = prim[4 * c1 + v] + m->hs_gp[2 * h1] * g[8 * c1 + v] +
-				       m->hs_gp[2 * h1 + 1] * g[8 * c1 + 4 + v];
-				q1[v] = prim[4 * c1 + v];
-			}
-			g1x = &g[8 * c1];
-			g1y = &g[8 * c1 + 4];
-		} else {
-			long b = -1 - c1;
-			o_boundary(&o, &cs->bc_table[m->bc_index[b]], n, t, L, R, &m->bc_x[2 * b]);
-			if (wall_p)
-				wall_p[b] = L[3];
-			memcpy(q1, &gb[4 * b], sizeof(q1));
-			g1x = g1y = zero4;
-		}
-		fin s = {L[0], R[0], n[0] * L[1] + n[1] * L[2], n[0] * R[1] + n[1] * R[2],
-			 -n[1] * L[1] + n[0] * L[2], -n[1] * R[1] + n[0] * R[2], L[3], R[3]};
-		double fc[4], *F4 = &ff[4 * f];
-		o_flux(&o, &s, fc);
-		F4[0] = fc[0];
-		F4[1] = n[0] * fc[1] - n[1] * fc[2];
-		F4[2] = n[1] * fc[1] + n[0] * fc[2];
-		F4[3] = fc[3];
-		if (o.eqn == CCFD_NAVIER_STOKES) {
-			const double *bb = &m->face_bb[3 * f];
-			double bx = bb[0] / bb[2], by = bb[1] / bb[2];
-			double st[4], gx[4], gy[4], fx[4], fy[4];
-			for (int v = 0; v < NV; ++v) {
-				st[v] = 0.5 * (R[v] + L[v]);
-				double mx = 0.5 * (g[8 * c0 + v] + g1x[v]);
-				double my = 0.5 * (g[8 * c0 + 4 + v] + g1y[v]);
-				double corr = mx * bx + my * by - (q1[v] - prim[4 * c0 + v]) / bb[2];
-				gx[v] = mx - corr * bx;
-				gy[v] = my - corr * by;
-			}
-			/* diffusionFlux, src/fluxCalculation.c:855-873 */
-			double mu = o.mu, k = o.gam / (o.gam1 * o.Pr * st[0] * st[0]);
-			fx[0] = fy[0] = 0.0;
-			fx[1] = (4.0 / 3.0 * gx[1] - 2.0 / 3.0 * gy[2]) * mu;
-			fx[2] = (gy[1] + gx[2]) * mu;
-			fx[3] = (4.0 / 3.0 * st[1] * gx[1] - 2.0 / 3.0 * st[1] * gy[2] + (gx[2] + gy[1]) * st[2]
-				 + k * (st[0] * gx[3] - st[3] * gx[0])) * mu;
-			fy[1] = (gy[1] + gx[2]) * mu;
-			fy[2] = (4.0 / 3.0 * gy[2] - 2.0 / 3.0 * gx[1]) * mu;
-			fy[3] = (4.0 / 3.0 * st[2] * gy[2] - 2.0 / 3.0 * st[2] * gx[1] + (gy[1] + gx[2]) * st[1]
-				 + k * (st[0] * gy[3] - st[3] * gy[0])) * mu;
-			for (int v = 0; v < NV; ++v)
-				F4[v] -= (fx[v] * n[0] + fy[v] * n[1]);
-		}
-		for (int v = 0; v < NV; ++v)
-			F4[v] *= m->face_len[f];
-	}
-	/* per-cell sum in side-list order, src/finiteVolume.c:96-120 */
-	for (long c = 0; c < N; ++c) {
-		double s[4] = {0.0, 0.0, 0.0, 0.0};
-		for (long h = m->hs_offset[c]; h < m->hs_offset[c + 1]; ++h) {
-			const double *F4 = &ff[4 * m->hs_face[h]];
-			for (int v = 0; v < NV; ++v)
-				s[v] += m->hs_sign[h] > 0 ? F4[v] : -F4[v];
-		}
-		double src[4] = {0.0, 0.0, 0.0, 0.0};
-		if (cs->params.source_func)
-			o_cell_source(&o, m, c, t, src);
-		for (int v = 0; v < NV; ++v)
-			u_t[4 * c + v] = (src[v] - s[v]) * m->cell_geo[4 * c + 1];
-	}
+	for (long f = 0; f < F; ++f)
+		o_face_flux(&o, cs, prim, g, gb, f, t, &ff[4 * f], wall_p);
+	for (long c = 0; c < N; ++c)
+		o_cell_ut(&o, cs, ff, c, t, &u_t[4 * c]);
 	if (grad)
 		memcpy(grad, g, sizeof(double) * 8 * N);
 	if (fflux)
@@ -1034,5 +1063,614 @@ out:
 	info[6] = finished;
 	info[7] = converged;
 	free(cons); free(cons0); free(ut);
+	return st;
+}
+
+/* ======================================================================
+ * Implicit path, restated: buildMatrix / calcDinv / LUSGS
+ * (src/linearSolver.c:136-333) in block-sparse storage, and
+ * implicitTimeStep / GMRES_M / matrixVector (src/timeDiscretization.c:
+ * 412-552, src/linearSolver.c:343-510).
+ *
+ * The reference stores dRdU densely, (4N)^2 doubles, and obtains its
+ * columns from 4N residual evaluations over the whole mesh; both are out of
+ * reach beyond a few thousand cells.  Here a column (cell i, variable v)
+ * is evaluated on the stencil it reaches: the residuals of cell i and of
+ * its face neighbours, from the fluxes of their faces, the gradients of the
+ * cells on those faces and the ghost states those gradients read -- the
+ * same per-cell and per-face arithmetic as oracle_residual, so every
+ * recorded residual equals the one a whole-mesh evaluation gives.
+ * Columns run in the reference's order (cells, then variables); with
+ * in_place the perturbation is undone by subtracting the step again, as
+ * the reference does (pVar += rEps0 ... pVar -= rEps0), so the state and
+ * every later column carry that rounding exactly as there.
+ * ==================================================================== */
+
+typedef struct {
+	double *g, *gb, *ff;
+	long *stamp_f, *stamp_c, *stamp_b, *faces, *cells;
+	long stamp;
+} olocal;
+
+static void o_local_free(olocal *L)
+{
+	free(L->g); free(L->gb); free(L->ff);
+	free(L->stamp_f); free(L->stamp_c); free(L->stamp_b); free(L->faces); free(L->cells);
+}
+
+static int o_local_init(olocal *L, const ccfd_mesh *m)
+{
+	const long N = m->n_cells, F = m->n_faces, B = m->n_bc;
+	memset(L, 0, sizeof(*L));
+	L->g = calloc(8 * N, sizeof(double));
+	L->gb = calloc(4 * (B + 1), sizeof(double));
+	L->ff = calloc(4 * F, sizeof(double));
+	L->stamp_f = calloc(F, sizeof(long));
+	L->stamp_c = calloc(N, sizeof(long));
+	L->stamp_b = calloc(B + 1, sizeof(long));
+	L->faces = malloc(sizeof(long) * F);
+	L->cells = malloc(sizeof(long) * N);
+	if (!L->g || !L->gb || !L->ff || !L->stamp_f || !L->stamp_c || !L->stamp_b || !L->faces ||
+	    !L->cells) {
+		o_local_free(L);
+		return CCFD_ERR_NOMEM;
+	}
+	return CCFD_OK;
+}
+
+/* u_t (rows of ut) of the nt cells tgt at state prim and time t */
+static void o_local_ut(orc *o, const ccfd_case *cs, olocal *L, const double *prim, double t,
+		       const long *tgt, int nt, double *ut)
+{
+	const ccfd_mesh *m = &cs->mesh;
+	long nf = 0, nc = 0, st = ++L->stamp;
+	for (int k = 0; k < nt; ++k)
+		for (long h = m->hs_offset[tgt[k]]; h < m->hs_offset[tgt[k] + 1]; ++h) {
+			long f = m->hs_face[h];
+			if (L->stamp_f[f] != st) {
+				L->stamp_f[f] = st;
+				L->faces[nf++] = f;
+			}
+		}
+	if (o->order == 2) {
+		for (long k = 0; k < nf; ++k)
+			for (int s = 0; s < 2; ++s) {
+				long c = m->face_cells[2 * L->faces[k] + s];
+				if (c >= 0 && L->stamp_c[c] != st) {
+					L->stamp_c[c] = st;
+					L->cells[nc++] = c;
+				}
+			}
+		for (long k = 0; k < nc; ++k)
+			for (long h = m->hs_offset[L->cells[k]]; h < m->hs_offset[L->cells[k] + 1]; ++h) {
+				long nb = m->hs_nb[h];
+				if (nb >= 0 || L->stamp_b[-1 - nb] == st)
+					continue;
+				L->stamp_b[-1 - nb] = st;
+				o_ghost_bary(o, -1 - nb, t, prim, &L->gb[4 * (-1 - nb)]);
+			}
+		for (long k = 0; k < nc; ++k)
+			o_gradient(o, m, prim, L->gb, L->cells[k], &L->g[8 * L->cells[k]]);
+	}
+	for (long k = 0; k < nf; ++k)
+		o_face_flux(o, cs, prim, L->g, L->gb, L->faces[k], t, &L->ff[4 * L->faces[k]], NULL);
+	for (int k = 0; k < nt; ++k)
+		o_cell_ut(o, cs, L->ff, tgt[k], t, &ut[4 * k]);
+}
+
+/* 4x4 inverse by Laplace expansion in complementary 2x2 minors of the first
+ * two and the last two rows; 0 if |det| <= DBL_EPSILON (the singularity test
+ * of calcDinv, src/linearSolver.c:155-157) */
+static int o_inv4(const double *a, double *r)
+{
+	double s0 = a[0] * a[5] - a[4] * a[1], s1 = a[0] * a[6] - a[4] * a[2];
+	double s2 = a[0] * a[7] - a[4] * a[3], s3 = a[1] * a[6] - a[5] * a[2];
+	double s4 = a[1] * a[7] - a[5] * a[3], s5 = a[2] * a[7] - a[6] * a[3];
+	double c5 = a[10] * a[15] - a[14] * a[11], c4 = a[9] * a[15] - a[13] * a[11];
+	double c3 = a[9] * a[14] - a[13] * a[10], c2 = a[8] * a[15] - a[12] * a[11];
+	double c1 = a[8] * a[14] - a[12] * a[10], c0 = a[8] * a[13] - a[12] * a[9];
+	double det = s0 * c5 - s1 * c4 + s2 * c3 + s3 * c2 - s4 * c1 + s5 * c0;
+	if (fabs(det) <= 2.220446049250313e-16)
+		return 0;
+	double q = 1.0 / det;
+	r[0] = (a[5] * c5 - a[6] * c4 + a[7] * c3) * q;
+	r[1] = (-a[1] * c5 + a[2] * c4 - a[3] * c3) * q;
+	r[2] = (a[13] * s5 - a[14] * s4 + a[15] * s3) * q;
+	r[3] = (-a[9] * s5 + a[10] * s4 - a[11] * s3) * q;
+	r[4] = (-a[4] * c5 + a[6] * c2 - a[7] * c1) * q;
+	r[5] = (a[0] * c5 - a[2] * c2 + a[3] * c1) * q;
+	r[6] = (-a[12] * s5 + a[14] * s2 - a[15] * s1) * q;
+	r[7] = (a[8] * s5 - a[10] * s2 + a[11] * s1) * q;
+	r[8] = (a[4] * c4 - a[5] * c2 + a[7] * c0) * q;
+	r[9] = (-a[0] * c4 + a[1] * c2 - a[3] * c0) * q;
+	r[10] = (a[12] * s4 - a[13] * s2 + a[15] * s0) * q;
+	r[11] = (-a[8] * s4 + a[9] * s2 - a[11] * s0) * q;
+	r[12] = (-a[4] * c3 + a[5] * c1 - a[6] * c0) * q;
+	r[13] = (a[0] * c3 - a[1] * c1 + a[2] * c0) * q;
+	r[14] = (-a[12] * s3 + a[13] * s1 - a[14] * s0) * q;
+	r[15] = (a[8] * s3 - a[9] * s1 + a[10] * s0) * q;
+	return 1;
+}
+
+/* buildMatrix + calcDinv (src/linearSolver.c:136-252).  prim: primitive
+ * state (perturbed and restored in place), r_xk: residual at the state
+ * (R_XK), t: evaluation time of the perturbed residuals (the reference
+ * passes the step's start time), dt: time step.  Out: D, Dinv [N][16] and
+ * O [H][16] (row-major 4x4 blocks: rows = residual variables, columns =
+ * perturbed primitive variables; O[h] is the block of the row cell of
+ * half-side h and the column cell across it, zero at boundary sides).
+ * in_place: restore by subtraction (the reference's rounding) instead of
+ * the saved value. */
+int oracle_build_matrix(const ccfd_case *cs, double *prim, const double *r_xk, double t, double dt,
+			int in_place, double *D, double *Dinv, double *O)
+{
+	const ccfd_mesh *m = &cs->mesh;
+	const long N = m->n_cells, H = m->n_half_sides;
+	const double rEps0 = sqrt(2.220446049250313e-16), srEps0 = 1.0 / rEps0;
+	orc o;
+	double *eps2 = o_venk_eps2(cs);
+	o_init(&o, cs, eps2);
+	olocal L;
+	if (o_local_init(&L, m) != CCFD_OK) {
+		free(eps2);
+		return CCFD_ERR_NOMEM;
+	}
+	memset(D, 0, sizeof(double) * 16 * N);
+	memset(O, 0, sizeof(double) * 16 * H);
+	long tgt[64];
+	double ut[4 * 64];
+	for (long i = 0; i < N; ++i) {
+		int nt = 0;
+		tgt[nt++] = i;
+		for (long h = m->hs_offset[i]; h < m->hs_offset[i + 1] && nt < 64; ++h)
+			if (m->hs_nb[h] >= 0)
+				tgt[nt++] = m->hs_nb[h];
+		for (int iv = 0; iv < NV; ++iv) {
+			const double save = prim[4 * i + iv];
+			prim[4 * i + iv] += rEps0;
+			o_local_ut(&o, cs, &L, prim, t, tgt, nt, ut);
+			if (in_place)
+				prim[4 * i + iv] -= rEps0;
+			else
+				prim[4 * i + iv] = save;
+			for (int jv = 0; jv < NV; ++jv)
+				D[16 * i + 4 * jv + iv] += (ut[jv] - r_xk[4 * i + jv]) * srEps0;
+			/* column of cell i in the rows of its face neighbours j: the
+			 * block (j, i), kept at every half-side of j that faces i */
+			int k = 1;
+			for (long h = m->hs_offset[i]; h < m->hs_offset[i + 1]; ++h) {
+				long j = m->hs_nb[h];
+				if (j < 0)
+					continue;
+				const double *uj = &ut[4 * k++];
+				for (long h2 = m->hs_offset[j]; h2 < m->hs_offset[j + 1]; ++h2) {
+					if (m->hs_nb[h2] != i)
+						continue;
+					for (int jv = 0; jv < NV; ++jv)
+						O[16 * h2 + 4 * jv + iv] += (uj[jv] - r_xk[4 * j + jv]) * srEps0;
+				}
+			}
+		}
+	}
+	/* I - dt dR/dU (src/linearSolver.c:226-233) and the inverses */
+	int st = CCFD_OK;
+	for (long k = 0; k < 16 * H; ++k)
+		O[k] *= -dt;
+	for (long i = 0; i < N; ++i) {
+		for (int k = 0; k < 16; ++k)
+			D[16 * i + k] *= -dt;
+		for (int a = 0; a < NV; ++a)
+			D[16 * i + 5 * a] += 1.0;
+		if (!o_inv4(&D[16 * i], &Dinv[16 * i]))
+			st = CCFD_ERR_SINGULAR;
+	}
+	o_local_free(&L);
+	free(eps2);
+	if (o.vacuum && st == CCFD_OK)
+		st = CCFD_ERR_VACUUM;
+	return st;
+}
+
+/* LUSGS (src/linearSolver.c:261-333): forward and backward sweeps in cell
+ * order; x = M^-1 b, xs ([N][4]) is the intermediate vector. */
+void oracle_lusgs(const ccfd_case *cs, const double *Dinv, const double *O, const double *b,
+		  double *x, double *xs)
+{
+	const ccfd_mesh *m = &cs->mesh;
+	const long N = m->n_cells;
+	memset(x, 0, sizeof(double) * 4 * N);
+	memset(xs, 0, sizeof(double) * 4 * N);
+	for (long i = 0; i < N; ++i) {
+		double s[4] = {0.0, 0.0, 0.0, 0.0};
+		for (long h = m->hs_offset[i]; h < m->hs_offset[i + 1]; ++h) {
+			long j = m->hs_nb[h];
+			if (j < 0 || j >= i)
+				continue;
+			for (int a = 0; a < NV; ++a)
+				for (int c = 0; c < NV; ++c)
+					s[a] += O[16 * h + 4 * a + c] * xs[4 * j + c];
+		}
+		for (int a = 0; a < NV; ++a) {
+			double r = 0.0;
+			for (int c = 0; c < NV; ++c)
+				r += Dinv[16 * i + 4 * a + c] * (b[4 * i + c] - s[c]);
+			xs[4 * i + a] = r;
+		}
+	}
+	for (long i = N - 1; i >= 0; --i) {
+		double s[4] = {0.0, 0.0, 0.0, 0.0};
+		for (long h = m->hs_offset[i]; h < m->hs_offset[i + 1]; ++h) {
+			long j = m->hs_nb[h];
+			if (j <= i)
+				continue;
+			for (int a = 0; a < NV; ++a)
+				for (int c = 0; c < NV; ++c)
+					s[a] += O[16 * h + 4 * a + c] * x[4 * j + c];
+		}
+		for (int a = 0; a < NV; ++a) {
+			double r = 0.0;
+			for (int c = 0; c < NV; ++c)
+				r += Dinv[16 * i + 4 * a + c] * s[c];
+			x[4 * i + a] = xs[4 * i + a] - r;
+		}
+	}
+}
+
+/* vectorDotProduct (src/linearSolver.c:115-128), element order */
+static double o_dot(long N, const double *a, const double *b)
+{
+	double r = 0.0;
+	for (long i = 0; i < N; ++i)
+		for (int v = 0; v < NV; ++v)
+			r += a[4 * i + v] * b[4 * i + v];
+	return r;
+}
+
+/* implicit-step work arrays */
+typedef struct {
+	long N;
+	int K;
+	double *Q, *FX0, *FXK, *XK, *RXK, *dX, *R0, *W, *V, *Z, *U, *ut, *xs;
+	double *D, *Dinv, *O, *prim_m;
+	double *wall_p;
+	long newton, gmres;
+} oimp;
+
+static void o_imp_free(oimp *I)
+{
+	free(I->Q); free(I->FX0); free(I->FXK); free(I->XK); free(I->RXK); free(I->dX);
+	free(I->R0); free(I->W); free(I->V); free(I->Z); free(I->U); free(I->ut); free(I->xs);
+	free(I->D); free(I->Dinv); free(I->O); free(I->prim_m); free(I->wall_p);
+}
+
+static int o_imp_init(oimp *I, const ccfd_case *cs)
+{
+	const ccfd_mesh *m = &cs->mesh;
+	const long N = m->n_cells;
+	memset(I, 0, sizeof(*I));
+	I->N = N;
+	I->K = cs->params.n_kdim > 0 ? cs->params.n_kdim : 1;
+	size_t v = sizeof(double) * 4 * N;
+	I->Q = malloc(v); I->FX0 = malloc(v); I->FXK = malloc(v); I->XK = malloc(v);
+	I->RXK = malloc(v); I->dX = malloc(v); I->R0 = malloc(v); I->W = malloc(v);
+	I->U = malloc(v); I->ut = malloc(v); I->xs = malloc(v); I->prim_m = malloc(v);
+	I->V = malloc(v * (I->K + 1));
+	I->Z = malloc(v * I->K);
+	I->wall_p = calloc(m->n_bc + 1, sizeof(double));
+	if (cs->params.precond) {
+		I->D = malloc(sizeof(double) * 16 * N);
+		I->Dinv = malloc(sizeof(double) * 16 * N);
+		I->O = malloc(sizeof(double) * 16 * (m->n_half_sides + 1));
+	}
+	if (!I->Q || !I->FX0 || !I->FXK || !I->XK || !I->RXK || !I->dX || !I->R0 || !I->W || !I->U ||
+	    !I->ut || !I->xs || !I->prim_m || !I->V || !I->Z || !I->wall_p ||
+	    (cs->params.precond && (!I->D || !I->Dinv || !I->O))) {
+		o_imp_free(I);
+		return CCFD_ERR_NOMEM;
+	}
+	return CCFD_OK;
+}
+
+/* matrixVector (src/linearSolver.c:343-373): res = v - alpha dt
+ * (R(XK + eps v) - R_XK) / eps, eps = rEps0 / |v|; prim is left at the
+ * perturbed state (as the reference leaves pVar) */
+static int o_matvec(orc *o, const ccfd_case *cs, oimp *I, double *prim, double time, double dt,
+		    double alpha, const double *v, double *res)
+{
+	const long N = I->N;
+	const double rEps0 = sqrt(2.220446049250313e-16);
+	double epsFD = o_dot(N, v, v);
+	epsFD = rEps0 / sqrt(epsFD);
+	for (long i = 0; i < N; ++i) {
+		for (int k = 0; k < NV; ++k)
+			I->U[4 * i + k] = I->XK[4 * i + k] + epsFD * v[4 * i + k];
+		o_cons_prim(o, &I->U[4 * i], &prim[4 * i]);
+	}
+	int st = oracle_residual(cs, prim, time, I->ut, NULL, NULL, I->wall_p);
+	for (long i = 0; i < N; ++i)
+		for (int k = 0; k < NV; ++k)
+			res[4 * i + k] = v[4 * i + k] - alpha * dt * (I->ut[4 * i + k] - I->RXK[4 * i + k]) / epsFD;
+	return st;
+}
+
+/* GMRES_M (src/linearSolver.c:385-510); t0: step start (buildMatrix time) */
+static int o_gmres(orc *o, const ccfd_case *cs, oimp *I, double *prim, double time, double t0,
+		   double dt, double alpha, const double *B, double normB, double *abortCrit,
+		   int in_place)
+{
+	const long N = I->N;
+	const int K = I->K;
+	const size_t VS = 4 * N;
+	*abortCrit = cs->params.eps_gmres * normB;
+	double normR0 = normB;
+	for (long i = 0; i < 4 * N; ++i) {
+		I->R0[i] = -B[i];
+		I->dX[i] = 0.0;
+		I->V[i] = I->R0[i] / normR0;
+	}
+	double gam[K + 1], H[K + 1][K + 1], C[K], S[K];
+	gam[0] = normR0;
+	int st = CCFD_OK;
+	if (cs->params.precond) {
+		/* buildMatrix runs at the state pVar holds (consPrim of XK) */
+		if ((st = oracle_build_matrix(cs, prim, I->RXK, t0, dt, in_place, I->D, I->Dinv, I->O)))
+			return st;
+	}
+	for (int m = 0; m < K; ++m) {
+		I->gmres++;
+		double *Vm = I->V + VS * m, *Zm = I->Z + VS * m;
+		if (cs->params.precond)
+			oracle_lusgs(cs, I->Dinv, I->O, Vm, Zm, I->xs);
+		else
+			memcpy(Zm, Vm, sizeof(double) * VS);
+		if ((st = o_matvec(o, cs, I, prim, time, dt, alpha, Zm, I->W)))
+			return st;
+		for (int nn = 0; nn <= m; ++nn) {
+			H[nn][m] = o_dot(N, I->V + VS * nn, I->W);
+			for (long i = 0; i < 4 * N; ++i)
+				I->W[i] -= H[nn][m] * I->V[VS * nn + i];
+		}
+		double res = o_dot(N, I->W, I->W);
+		H[m + 1][m] = sqrt(res);
+		for (int nn = 0; nn <= m - 1; ++nn) {
+			double tmp = C[nn] * H[nn][m] + S[nn] * H[nn + 1][m];
+			H[nn + 1][m] = -S[nn] * H[nn][m] + C[nn] * H[nn + 1][m];
+			H[nn][m] = tmp;
+		}
+		double bet = sqrt(H[m][m] * H[m][m] + H[m + 1][m] * H[m + 1][m]);
+		S[m] = H[m + 1][m] / bet;
+		C[m] = H[m][m] / bet;
+		H[m][m] = bet;
+		gam[m + 1] = -S[m] * gam[m];
+		gam[m] = C[m] * gam[m];
+		if ((fabs(gam[m + 1]) <= *abortCrit) || (m == K - 1)) {
+			double alp[K];
+			for (int nn = m; nn >= 0; --nn) {
+				alp[nn] = gam[nn];
+				for (int q = nn + 1; q <= m; ++q)
+					alp[nn] -= H[nn][q] * alp[q];
+				alp[nn] /= H[nn][nn];
+			}
+			for (int nn = 0; nn <= m; ++nn)
+				for (long i = 0; i < 4 * N; ++i)
+					I->dX[i] += alp[nn] * I->Z[VS * nn + i];
+			return CCFD_OK;
+		}
+		for (long i = 0; i < 4 * N; ++i)
+			I->V[VS * (m + 1) + i] = I->W[i] / H[m + 1][m];
+	}
+	return CCFD_ERR_GMRES;
+}
+
+/* implicitTimeStep (src/timeDiscretization.c:412-552) from the step start
+ * time t: cons / prim are the state (updated), ut the residual of the last
+ * evaluation; res (4) = globalResidual of it */
+static int o_implicit_step(orc *o, const ccfd_case *cs, oimp *I, double *cons, double *prim,
+			   double t, double dt, int in_place, double res[4])
+{
+	const ccfd_params *p = &cs->params;
+	const ccfd_mesh *m = &cs->mesh;
+	const long N = I->N;
+	const double alpha = 1.0, beta = 1.0;
+	const double eps2newton = p->eps_newton * p->eps_newton, eps2newton_sq = sqrt(eps2newton);
+	int st;
+	for (long i = 0; i < N; ++i) {
+		memcpy(&I->Q[4 * i], &cons[4 * i], sizeof(double) * 4);
+		o_cons_prim(o, &cons[4 * i], &prim[4 * i]);
+	}
+	double time = t + beta * dt;
+	if ((st = oracle_residual(cs, prim, time, I->ut, NULL, NULL, I->wall_p)))
+		return st;
+	for (long i = 0; i < 4 * N; ++i) {
+		I->FX0[i] = cons[i] - I->Q[i] - alpha * dt * I->ut[i];
+		I->XK[i] = cons[i];
+		I->RXK[i] = I->ut[i];
+		I->FXK[i] = I->FX0[i];
+	}
+	double norm2_F_X0 = o_dot(N, I->FX0, I->FX0);
+	double eps2newtonLoc = fmax(1e-8 * 1e-8 * N * eps2newton / norm2_F_X0, eps2newton);
+	double norm2_F_XK = norm2_F_X0;
+	int nInner = 0;
+	double abortCrit = 0.0, norm2_old = norm2_F_XK, gamA, gamB;
+	while ((norm2_F_XK > eps2newtonLoc * norm2_F_X0) && (nInner < p->n_newton_iter)) {
+		if (nInner == 0) {
+			abortCrit = 0.999;
+			norm2_old = norm2_F_XK;
+		} else {
+			gamA = p->gamma_ew * norm2_F_XK / norm2_old;
+			if (p->gamma_ew * abortCrit * abortCrit < 0.1)
+				gamB = fmin(0.999, gamA);
+			else
+				gamB = fmin(0.999, fmax(gamA, p->gamma_ew * abortCrit * abortCrit));
+			abortCrit = fmin(0.999, fmax(gamB, 0.5 * eps2newton_sq / sqrt(norm2_F_XK)));
+			norm2_old = norm2_F_XK;
+		}
+		nInner++;
+		if ((st = o_gmres(o, cs, I, prim, time, t, dt, alpha, I->FXK, sqrt(norm2_F_XK), &abortCrit,
+				  in_place)))
+			return st;
+		for (long i = 0; i < N; ++i) {
+			for (int k = 0; k < NV; ++k) {
+				I->XK[4 * i + k] += I->dX[4 * i + k];
+				cons[4 * i + k] = I->XK[4 * i + k];
+			}
+			o_cons_prim(o, &cons[4 * i], &prim[4 * i]);
+		}
+		if ((st = oracle_residual(cs, prim, time, I->ut, NULL, NULL, I->wall_p)))
+			return st;
+		for (long i = 0; i < 4 * N; ++i) {
+			I->RXK[i] = I->ut[i];
+			I->FXK[i] = cons[i] - I->Q[i] - alpha * dt * I->ut[i];
+		}
+		norm2_F_XK = o_dot(N, I->FXK, I->FXK);
+	}
+	I->newton += nInner;
+	if (nInner == p->n_newton_iter)
+		return CCFD_ERR_NEWTON;
+	double acc[4] = {0, 0, 0, 0};
+	for (long c = 0; c < N; ++c)
+		for (int v = 0; v < NV; ++v)
+			acc[v] += m->cell_geo[4 * c] * I->ut[4 * c + v] * I->ut[4 * c + v];
+	for (int v = 0; v < NV; ++v)
+		res[v] = sqrt(acc[v] * m->total_area_q);
+	return CCFD_OK;
+}
+
+/* lift and drag of calcCoef (src/analyze.c:292-387) from the interior face
+ * pressures at the wall faces (BC code wall_id), summed in BCside order */
+static void o_clcd(const ccfd_case *cs, const double *wall_p, double *cl_out, double *cd_out)
+{
+	const ccfd_mesh *m = &cs->mesh;
+	const ccfd_params *p = &cs->params;
+	const double pi = acos(-1.0);
+	double v = cs->exact.ref_state[0][1] / cos(cs->exact.alpha * pi / 180.0);
+	double qInfQ = 1.0 / (cs->exact.ref_state[0][0] * 0.5 * v * v);
+	double qInfLq = qInfQ / p->ref_length;
+	double cl = 0.0, cd = 0.0;
+	for (long b = 0; b < m->n_bc; ++b) {
+		const ccfd_bc *bc = &cs->bc_table[m->bc_index[b]];
+		if (bc->type * 100 + bc->id != p->wall_id)
+			continue;
+		long f = m->bc_face[b];
+		cl += m->face_n[2 * f + 1] * wall_p[b] * m->face_len[f];
+		cd += m->face_n[2 * f] * wall_p[b] * m->face_len[f];
+	}
+	cl *= qInfLq;
+	cd *= qInfLq;
+	double a = cs->exact.alpha * pi / 180.0;
+	*cl_out = cl * cos(a) - cd * sin(a);
+	*cd_out = cd * cos(a) + cl * sin(a);
+}
+
+/* Implicit time loop of timeDisc: per step calcTimeStep, implicitTimeStep,
+ * the wing coefficients, the reference's absolute stop test and the
+ * relative one (params.rel_abort_residual).  ser_cfl_max > 0 turns on
+ * switched evolution relaxation of the CFL number (Mulder and van Leer,
+ * 1985): before step n >= 2, CFL = min(ser_cfl_max, CFL_0 * r_1 / r_{n-1}),
+ * r the abort variable's global residual after a step, and the viscous
+ * number follows, DFL = DFL_0 * CFL / CFL_0.  in_place: the
+ * reference's in-place restore in buildMatrix.  prim is updated in place;
+ * info[0..11] = t, steps, res[0..3], finished, converged, Newton and GMRES
+ * iterations, cl, cd; hist (optional, nsteps x 8): t, dt, res[0..3], cl, cd
+ * per step. */
+int oracle_run_implicit(const ccfd_case *cs, double *prim, long nsteps, double ser_cfl_max,
+			int in_place, double *info, double *hist)
+{
+	ccfd_case c2 = *cs;
+	ccfd_params *p = &c2.params;
+	const ccfd_mesh *m = &cs->mesh;
+	const long N = m->n_cells;
+	const double cfl0 = p->cfl, dfl0 = p->dfl;
+	orc o;
+	o_init(&o, cs, NULL);
+	oimp I;
+	if (o_imp_init(&I, cs) != CCFD_OK)
+		return CCFD_ERR_NOMEM;
+	double *cons = malloc(sizeof(double) * 4 * N);
+	if (!cons) {
+		o_imp_free(&I);
+		return CCFD_ERR_NOMEM;
+	}
+	for (long c = 0; c < N; ++c)
+		o_prim_cons(&o, &prim[4 * c], &cons[4 * c]);
+	double t = 0.0;
+	double print_time = (floor(0.0 / p->io_time_interval) + 1) * p->io_time_interval;
+	long io_iter = p->io_iter_interval > 0 ? p->io_iter_interval : 1;
+	long print_iter = io_iter;
+	double res[4] = {0, 0, 0, 0}, r_first = 0.0, r_prev = 0.0, cl = 0.0, cd = 0.0;
+	int finished = 0, converged = 0, st = CCFD_OK;
+	long iter, done = 0;
+	for (iter = 1; iter <= p->max_iter; ++iter) {
+		if (nsteps > 0 && iter > nsteps)
+			break;
+		if (ser_cfl_max > 0.0 && iter >= 2 && r_prev > 0.0) {
+			p->cfl = fmin(ser_cfl_max, cfl0 * r_first / r_prev);
+			p->dfl = dfl0 * p->cfl / cfl0;
+		}
+		double dt;
+		if ((st = oracle_time_step(&c2, prim, t, print_time, &dt)) != CCFD_OK)
+			break;
+		o.vacuum = 0;
+		if ((st = o_implicit_step(&o, &c2, &I, cons, prim, t, dt, in_place, res)) != CCFD_OK)
+			break;
+		double cl_old = cl, cd_old = cd, rcl = 0.0, rcd = 0.0;
+		if (p->calc_wing) {
+			o_clcd(cs, I.wall_p, &cl, &cd);
+			rcl = fabs(cl_old - cl) / dt;
+			rcd = fabs(cd_old - cd) / dt;
+		}
+		t += dt;
+		if (hist) {
+			double *h = &hist[8 * done];
+			h[0] = t; h[1] = dt;
+			for (int v = 0; v < 4; ++v)
+				h[2 + v] = res[v];
+			h[6] = cl; h[7] = cd;
+		}
+		done++;
+		double ra = res[p->abort_variable];
+		if (iter == 1)
+			r_first = ra;
+		r_prev = ra;
+		if (p->t_end - t <= 1e-15) {
+			finished = 1;
+			break;
+		}
+		if (p->stationary) {
+			int conv = 0;
+			if (fabs(ra) <= p->abort_residual) {
+				if (p->cl_abort_residual > 0.0)
+					conv = fabs(rcl) <= p->cl_abort_residual;
+				else if (p->cd_abort_residual > 0.0)
+					conv = fabs(rcd) <= p->cd_abort_residual;
+				else
+					conv = 1;
+			}
+			if (p->rel_abort_residual > 0.0 && ra <= p->rel_abort_residual * r_first)
+				conv = 1;
+			if (conv) {
+				converged = 1;
+				break;
+			}
+		}
+		if ((print_time - t <= 1e-15) || (iter == print_iter)) {
+			if (print_time - t <= 1e-15)
+				print_time += p->io_time_interval;
+			if (iter == print_iter)
+				print_iter += io_iter;
+		}
+	}
+	info[0] = t;
+	info[1] = (double)done;
+	for (int v = 0; v < 4; ++v)
+		info[2 + v] = res[v];
+	info[6] = finished;
+	info[7] = converged;
+	info[8] = (double)I.newton;
+	info[9] = (double)I.gmres;
+	info[10] = cl;
+	info[11] = cd;
+	free(cons);
+	o_imp_free(&I);
 	return st;
 }

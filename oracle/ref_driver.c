@@ -29,6 +29,17 @@
  * dataOutput (solution file, and exact-solution file with exactSolution =
  * T).
  *
+ *   jacobian <t> <dt> [state] [vector]
+ *                        buildMatrix(t, dt) (src/linearSolver.c:186-252) at
+ *                        the state, with R_XK = fvTimeDerivative(t + dt) as
+ *                        at the first Newton iteration of implicitTimeStep;
+ *                        dumps the diagonal blocks D, their inverses Dinv,
+ *                        the face-neighbour blocks of the dense dRdU per
+ *                        half-side, the state after buildMatrix (it perturbs
+ *                        and restores pVar in place) and, given a raw f64
+ *                        vector file (N*4, cell order), LUSGS of it
+ *                        (src/linearSolver.c:261-333); needs precond = T
+ *
  * Dump format: magic "CCFDDMP1", then records of
  *   char name[32]; int32 type (0 = f64, 1 = i64); int32 pad; int64 count; data
  */
@@ -59,6 +70,11 @@ void explicitTimeStepEuler(double time, double dt, double resIter[NVAR + 2]);
 void explicitTimeStepRK(double time, double dt, double resIter[NVAR + 2]);
 void implicitTimeStep(double time, double dt, double resIter[NVAR + 2]);
 void calcCoef(void);
+void buildMatrix(double time, double dt);
+void LUSGS(double **B, double **delX);
+extern double ***D;
+extern double ***Dinv;
+extern double **dRdU;
 
 static FILE *dumpFile;
 
@@ -294,6 +310,15 @@ int main(int argc, char *argv[])
 		bool write_out = getenv("CCFD_REF_OUTPUT") != NULL;
 		const char *rel = getenv("CCFD_REF_REL_ABORT");
 		double relAbort = rel ? strtod(rel, NULL) : 0.0, relFirst = 0.0;
+		/* switched evolution relaxation of the CFL number (Mulder and van
+		 * Leer, 1985) around the reference's own step: before step n >= 2,
+		 * cfl = min(cap, CFL_0 * r_1 / r_{n-1}), r the abort variable's
+		 * residual after a step (the reference's global cfl,
+		 * src/timeDiscretization.c:72, read by calcTimeStep), and the
+		 * viscous number follows, dfl = DFL_0 * cfl / CFL_0 */
+		const char *ser = getenv("CCFD_REF_SER_CFL_MAX");
+		double serMax = ser ? strtod(ser, NULL) : 0.0, cfl0 = cfl, dfl0 = dfl, serFirst = 0.0,
+		       serPrev = 0.0;
 		long nsteps = argc > 4 ? strtol(argv[4], NULL, 10) : 0;
 		if (argc > 5)
 			load_state(argv[5]);
@@ -309,6 +334,10 @@ int main(int argc, char *argv[])
 		for (iter = 1; iter <= maxIter; ++iter) {
 			if (nsteps > 0 && iter > nsteps)
 				break;
+			if (serMax > 0.0 && iter >= 2 && serPrev > 0.0) {
+				cfl = fmin(serMax, cfl0 * serFirst / serPrev);
+				dfl = dfl0 * cfl / cfl0;
+			}
 			calcTimeStep(printTime, &dt, &visc);
 			memset(resIter, 0, sizeof(resIter));
 			if (!isImplicit) {
@@ -333,6 +362,9 @@ int main(int argc, char *argv[])
 				resIter[4] = fabs(resIter[4] - wing.cl) / firstElem->dt;
 				resIter[5] = fabs(resIter[5] - wing.cd) / firstElem->dt;
 			}
+			if (iter == 1)
+				serFirst = resIter[abortVariable];
+			serPrev = resIter[abortVariable];
 			wall[nhist] = omp_get_wtime() - tStart;
 			double *h = &hist[8 * nhist++];
 			h[0] = t; h[1] = dt;
@@ -409,6 +441,84 @@ int main(int argc, char *argv[])
 		}
 		free(hist);
 		free(wall);
+	} else if (!strcmp(mode, "jacobian")) {
+		double tb = argc > 4 ? strtod(argv[4], NULL) : 0.0;
+		double dtb = argc > 5 ? strtod(argv[5], NULL) : 1e-3;
+		if (argc > 6 && strcmp(argv[6], "-"))
+			load_state(argv[6]);
+		if (!usePrecond) {
+			fprintf(stderr, "ccfd_ref: jacobian needs precond = T\n");
+			return 2;
+		}
+		double dt;
+		bool visc;
+		calcTimeStep(printTime, &dt, &visc);
+		t = tb;
+		fvTimeDerivative(tb + dtb);
+		for (long i = 0; i < nElems; ++i)
+			for (int v = 0; v < NVAR; ++v)
+				R_XK[v][i] = elem[i]->u_t[v];
+		buildMatrix(tb, dtb);
+		double *dd = malloc(sizeof(double) * 16 * nElems);
+		double *di = malloc(sizeof(double) * 16 * nElems);
+		long nhs = 0;
+		for (long i = 0; i < nElems; ++i)
+			nhs += elem[i]->elemType;
+		double *off = calloc(16 * (nhs + 1), sizeof(double));
+		double *pv = malloc(sizeof(double) * 4 * nElems);
+		long k = 0;
+		for (long i = 0; i < nElems; ++i) {
+			for (int a = 0; a < 4; ++a) {
+				pv[4 * i + a] = elem[i]->pVar[a];
+				for (int b = 0; b < 4; ++b) {
+					dd[16 * i + 4 * a + b] = D[i][a][b];
+					di[16 * i + 4 * a + b] = Dinv[i][a][b];
+				}
+			}
+			for (side_t *sd = elem[i]->firstSide; sd; sd = sd->nextElemSide, ++k) {
+				long j = sd->connection->elem->id;
+				if (j < 0 || j >= nElems)
+					continue;
+				for (int a = 0; a < 4; ++a)
+					for (int b = 0; b < 4; ++b)
+						off[16 * k + 4 * a + b] = dRdU[4 * i + a][4 * j + b];
+			}
+		}
+		dump_f64("jac_d", dd, 16 * nElems);
+		dump_f64("jac_dinv", di, 16 * nElems);
+		dump_f64("jac_off", off, 16 * nhs);
+		dump_f64("pvar_after", pv, 4 * nElems);
+		if (argc > 7) {
+			FILE *f = fopen(argv[7], "rb");
+			if (!f) {
+				fprintf(stderr, "ccfd_ref: cannot open vector file %s\n", argv[7]);
+				return 2;
+			}
+			double **bv = malloc(sizeof(double *) * NVAR), **xv = malloc(sizeof(double *) * NVAR);
+			for (int v = 0; v < NVAR; ++v) {
+				bv[v] = malloc(sizeof(double) * nElems);
+				xv[v] = malloc(sizeof(double) * nElems);
+			}
+			double *raw = malloc(sizeof(double) * 4 * nElems);
+			if (fread(raw, sizeof(double), 4 * nElems, f) != (size_t)(4 * nElems)) {
+				fprintf(stderr, "ccfd_ref: short vector file\n");
+				return 2;
+			}
+			fclose(f);
+			for (long i = 0; i < nElems; ++i)
+				for (int v = 0; v < NVAR; ++v)
+					bv[v][i] = raw[4 * i + v];
+			LUSGS(bv, xv);
+			for (long i = 0; i < nElems; ++i)
+				for (int v = 0; v < NVAR; ++v)
+					raw[4 * i + v] = xv[v][i];
+			dump_f64("lusgs", raw, 4 * nElems);
+		}
+		double *rx = malloc(sizeof(double) * 4 * nElems);
+		for (long i = 0; i < nElems; ++i)
+			for (int v = 0; v < NVAR; ++v)
+				rx[4 * i + v] = R_XK[v][i];
+		dump_f64("r_xk_used", rx, 4 * nElems);
 	} else {
 		fprintf(stderr, "ccfd_ref: unknown mode %s\n", mode);
 		return 2;

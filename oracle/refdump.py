@@ -50,7 +50,8 @@ def run_ref(ini_text: str, mode: str, *args, eqn: str = "euler",
             fast: bool = False, state: np.ndarray | None = None,
             threads: int | None = None, workdir: str | None = None,
             files: dict | None = None, timeout: float = 3600.0,
-            output: bool = False, rel_abort: float | None = None) -> dict:
+            output: bool = False, rel_abort: float | None = None,
+            vector: np.ndarray | None = None, ser_cfl_max: float | None = None) -> dict:
     """Run the reference driver on an .ini text in a scratch directory.
 
     ``state`` (N x 4 primitive states in reference cell order) replaces the
@@ -58,7 +59,10 @@ def run_ref(ini_text: str, mode: str, *args, eqn: str = "euler",
     directory (the reference's parser drops '/' from values, so a mesh file
     must sit in its working directory).  ``output``: the run ends with the
     reference's dataOutput; its files come back as ``out["output_files"]``
-    ({name: text}).  Returns the parsed dump.
+    ({name: text}).  ``vector`` (N x 4, cell order) is passed after the
+    state file (mode ``jacobian``: the right-hand side of LUSGS).
+    ``ser_cfl_max``: switched-evolution-relaxation CFL cap of the driver's
+    time loop.  Returns the parsed dump.
     """
     exe = ref_binary(eqn, fast)
     if not os.access(exe, os.X_OK):
@@ -77,6 +81,12 @@ def run_ref(ini_text: str, mode: str, *args, eqn: str = "euler",
             if len(args) == 0:
                 argv.append("0")
             argv.append(sp)
+        if vector is not None:
+            vp = os.path.join(tmp, "vector.bin")
+            np.ascontiguousarray(vector, dtype=np.float64).tofile(vp)
+            if state is None:
+                argv.append("-")
+            argv.append(vp)
         env = dict(os.environ)
         if threads is not None:
             env["OMP_NUM_THREADS"] = str(threads)
@@ -85,6 +95,8 @@ def run_ref(ini_text: str, mode: str, *args, eqn: str = "euler",
             env["CCFD_REF_OUTPUT"] = "1"
         if rel_abort is not None:
             env["CCFD_REF_REL_ABORT"] = repr(float(rel_abort))
+        if ser_cfl_max is not None:
+            env["CCFD_REF_SER_CFL_MAX"] = repr(float(ser_cfl_max))
         r = subprocess.run(argv, cwd=tmp, env=env, capture_output=True,
                            text=True, timeout=timeout)
         if r.returncode != 0:

@@ -47,6 +47,13 @@ def lib():
         L.oracle_run_explicit.argtypes = [C.c_void_p, dp, C.c_long, dp]
         L.oracle_errors.restype = C.c_int
         L.oracle_errors.argtypes = [C.c_void_p, dp, C.c_double, C.c_int, dp]
+        L.oracle_build_matrix.restype = C.c_int
+        L.oracle_build_matrix.argtypes = [C.c_void_p, dp, dp, C.c_double, C.c_double, C.c_int,
+                                          dp, dp, dp]
+        L.oracle_lusgs.restype = None
+        L.oracle_lusgs.argtypes = [C.c_void_p, dp, dp, dp, dp, dp]
+        L.oracle_run_implicit.restype = C.c_int
+        L.oracle_run_implicit.argtypes = [C.c_void_p, dp, C.c_long, C.c_double, C.c_int, dp, dp]
         _lib = L
     return _lib
 
@@ -106,3 +113,56 @@ def run_explicit(case, prim: np.ndarray | None = None, nsteps: int = 0):
         raise RuntimeError(f"oracle_run_explicit status {st}")
     return p, {"t": info[0], "iterations": int(info[1]), "residual": info[2:6].tolist(),
                "finished": bool(info[6]), "converged": bool(info[7])}
+
+
+def build_matrix(case, prim: np.ndarray, r_xk: np.ndarray, time: float, dt: float,
+                 in_place: bool = True):
+    """buildMatrix + calcDinv restated in block-sparse form.  Returns the
+    state after the column evaluations (perturbed and restored in place like
+    the reference when in_place), D and Dinv [N,4,4] and the off-diagonal
+    block of every half-side [H,4,4] (row cell of the half-side, column cell
+    across it; zero at boundary sides)."""
+    n = case.n_cells
+    h = case.c.mesh.n_half_sides
+    p = np.array(prim, dtype=np.float64).reshape(n, 4).copy()
+    r = np.ascontiguousarray(r_xk, dtype=np.float64).reshape(n, 4)
+    D = np.zeros((n, 4, 4))
+    Di = np.zeros((n, 4, 4))
+    O = np.zeros((h, 4, 4))
+    st = lib().oracle_build_matrix(_case_ptr(case), _dp(p), _dp(r), float(time), float(dt),
+                                   int(bool(in_place)), _dp(D), _dp(Di), _dp(O))
+    if st != 0:
+        raise RuntimeError(f"oracle_build_matrix status {st}")
+    return p, D, Di, O
+
+
+def lusgs(case, Dinv: np.ndarray, O: np.ndarray, b: np.ndarray) -> np.ndarray:
+    """LUSGS restated: the preconditioned vector M^-1 b [N,4]."""
+    n = case.n_cells
+    Di = np.ascontiguousarray(Dinv, dtype=np.float64)
+    Oc = np.ascontiguousarray(O, dtype=np.float64)
+    bb = np.ascontiguousarray(b, dtype=np.float64).reshape(n, 4)
+    x = np.zeros((n, 4))
+    xs = np.zeros((n, 4))
+    lib().oracle_lusgs(_case_ptr(case), _dp(Di), _dp(Oc), _dp(bb), _dp(x), _dp(xs))
+    return x
+
+
+def run_implicit(case, nsteps: int, prim: np.ndarray | None = None, ser_cfl_max: float = 0.0,
+                 in_place: bool = True):
+    """The implicit time loop restated (implicitTimeStep with GMRES_M and,
+    with precond, the restated buildMatrix / LUSGS).  Returns the final
+    primitive state, an info dict and the per-step history rows
+    (t, dt, res[4], cl, cd)."""
+    n = case.n_cells
+    p = np.array(case.prim0() if prim is None else prim, dtype=np.float64).reshape(n, 4).copy()
+    info = np.zeros(12)
+    cap = nsteps if nsteps > 0 else int(case.params.max_iter)
+    hist = np.zeros((max(cap, 1), 8))
+    st = lib().oracle_run_implicit(_case_ptr(case), _dp(p), int(nsteps), float(ser_cfl_max),
+                                   int(bool(in_place)), _dp(info), _dp(hist))
+    k = int(info[1])
+    return p, {"status": st, "t": info[0], "iterations": k, "res": info[2:6].copy(),
+               "finished": bool(info[6]), "converged": bool(info[7]),
+               "newton_iterations": int(info[8]), "gmres_iterations": int(info[9]),
+               "cl": info[10], "cd": info[11]}, hist[:k].copy()

@@ -14,7 +14,7 @@ import pytest
 
 import ccfd_b200 as cc
 from ccfd_b200 import meshgen
-from oracle import restated
+from oracle import refdump, restated
 from tests.golden import cases as CASES
 from tests.helpers import l1_linf, rel_max_err, sod_frobenius
 
@@ -318,3 +318,24 @@ def test_state_upload_returns_after_its_copy():
     assert np.array_equal(a.get_state(), b.get_state())
     a.close()
     b.close()
+
+
+@pytest.mark.skipif(not refdump.have_ref(), reason="compiled reference not built")
+def test_sod_400x20_to_t_end_matches_compiled_reference():
+    """The small plain configuration: Sod shock tube on [0,1]x[0,0.05],
+    400 x 20 Cartesian quads (the reference's own generator), Roe, second
+    order least squares with Barth-Jespersen, 3-stage RK (timeOrder 2),
+    CFL 0.5, to t_end = 0.2, against the compiled reference run live."""
+    ini = meshgen.sod_ini(400, 20, t_end=0.2, flux=2, order=2, limiter=1, cfl=0.5)
+    case = cc.CaseData.from_text(ini)
+    assert case.n_cells == 8000
+    s = cc.Solver(case, reorder=True)
+    rep = s.run(0)
+    prim = s.get_state()
+    s.close()
+    d = refdump.run_ref(ini, "run", 0, threads=8)
+    ref = d["pvar"].reshape(-1, 4)
+    assert rep["finished"] and abs(rep["t"] - 0.2) <= 1e-14
+    assert rep["iterations"] == int(d["run_info"][1])
+    l1, linf = l1_linf(prim, ref)
+    assert l1 <= RUN_TOL and linf <= RUN_TOL
