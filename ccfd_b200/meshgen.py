@@ -475,9 +475,13 @@ def airfoil_ini(mesh_file: str, mach: float = 0.5, alpha: float = 1.0, navier_st
                 reynolds: float = 5000.0, flux: int = 2, implicit: bool = True,
                 precond: bool = True, n_kdim: int = 30, rel_res: float = 1e-8,
                 cfl: float = 1e3, max_iter: int = 100000, precision: int = 0,
-                wall_code: int | None = None, venk_k: float = 5.0) -> str:
+                wall_code: int | None = None, venk_k: float = 5.0, dfl: float | None = None,
+                ser_cfl_max: float | None = None) -> str:
     """Steady airfoil case: far field 501 (characteristic) with rho = p = 1,
-    wall 101 (Euler) or 201 (adiabatic no-slip, Navier-Stokes)."""
+    wall 101 (Euler) or 201 (adiabatic no-slip, Navier-Stokes).  ``dfl``:
+    viscous time-step number (DFL; the reference's default otherwise);
+    ``ser_cfl_max``: CFL ramp by switched evolution relaxation up to this
+    value (extension key serCFLmax)."""
     base = mesh_file[:-4] if mesh_file.endswith(".msh") else mesh_file
     wall = wall_code if wall_code is not None else (201 if navier_stokes else 101)
     gam = 1.4
@@ -510,7 +514,7 @@ venk_k = {venk_k}
 timeOrder = 1
 nRKstages = 1
 CFL = {cfl}
-implicit = {'T' if implicit else 'F'}
+{f"DFL = {dfl!r}" + chr(10) if dfl is not None else ""}{f"serCFLmax = {ser_cfl_max!r}" + chr(10) if ser_cfl_max else ""}implicit = {'T' if implicit else 'F'}
 precond = {'T' if precond else 'F'}
 nKdim = {n_kdim}
 nNewtonIter = 100

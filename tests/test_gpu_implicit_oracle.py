@@ -36,15 +36,13 @@ def _rel(a, b):
 
 
 def _airfoil(tmp, ni, nj, ns, cfl, max_iter, h0=1e-2, r_far=5.0, kdim=30, rel=1e-8, mach=0.5, alpha=2.0,
-             reynolds=500.0, precision=0, ser=0.0):
+             reynolds=500.0, precision=0, ser=None, dfl=None):
     wall = 201 if ns else 101
     meshgen.naca_ogrid(0.0, 0.0, 0.12, ni, nj, r_far=r_far, h0=h0, wall_code=wall).write_gmsh(
         os.path.join(tmp, "af.msh"))
     ini = meshgen.airfoil_ini("af", mach=mach, alpha=alpha, navier_stokes=ns, reynolds=reynolds, flux=2,
                               implicit=True, precond=True, n_kdim=kdim, cfl=cfl, max_iter=max_iter,
-                              rel_res=rel, precision=precision)
-    if ser:
-        ini += f"serCFLmax = {ser!r}\n"
+                              rel_res=rel, precision=precision, dfl=dfl, ser_cfl_max=ser)
     return cc.CaseData.from_text(ini, tmp)
 
 
@@ -111,16 +109,22 @@ def test_c3_airfoil_implicit_steps_match_restated():
     assert abs(rep["cl"] - info["cl"]) <= TOL and abs(rep["cd"] - info["cd"]) <= TOL
 
 
-def test_steady_state_matches_restated():
+@pytest.mark.parametrize("ns", [False, True])
+def test_steady_state_matches_restated(ns):
+    # Euler: CFL 20 ramped to at most 300; Navier-Stokes (Re 500): CFL and
+    # DFL 10 ramped to at most 3000
     with tempfile.TemporaryDirectory() as tmp:
-        case = _airfoil(tmp, 32, 12, False, cfl=20.0, max_iter=1500, ser=300.0)
+        if ns:
+            case = _airfoil(tmp, 32, 12, True, cfl=10.0, max_iter=1500, ser=3000.0, dfl=10.0)
+        else:
+            case = _airfoil(tmp, 32, 12, False, cfl=20.0, max_iter=1500, ser=300.0)
     s = cc.Solver(case, reorder=True)
     try:
         rep = s.run(0)
         prim = s.get_state()
     finally:
         s.close()
-    po, info, hist = restated.run_implicit(case, 0, ser_cfl_max=300.0)
+    po, info, hist = restated.run_implicit(case, 0, ser_cfl_max=case.params.ser_cfl_max)
     assert info["converged"] and rep["converged"]
     # both at a relative residual of 1e-8 (possibly a step apart)
     assert abs(rep["iterations"] - info["iterations"]) <= 2
