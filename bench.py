@@ -201,7 +201,8 @@ def make_case(tmpdir: str, precision: int = 0):
     return cc.CaseData.from_text(ini, tmpdir), ini, path
 
 
-def run_mixed(tmpdir: str, steps: int, warmup: int, prim_fp64, nrk: int, bytes_stage: int):
+def run_mixed(tmpdir: str, steps: int, warmup: int, prim_fp64, nrk: int, bytes_stage: int,
+              oracle_steps: int = 0):
     """The same workload with FP32 reconstruction / face fluxes and FP64
     accumulation and state: throughput, stage-kernel time and the state's
     deviation from the FP64 run after the same steps."""
@@ -221,12 +222,99 @@ def run_mixed(tmpdir: str, steps: int, warmup: int, prim_fp64, nrk: int, bytes_s
     avg = res_ms / max(res_cnt, 1)
     scale = np.abs(prim_fp64).max(axis=0)
     d = np.abs(prim - prim_fp64) / scale
-    return {"value": n * nrk * done / (rep["device_ms"] / 1e3), "unit": UNIT,
-            "ms_per_step": rep["device_ms"] / max(done, 1), "dtype": "f32 flux / f64 accumulation",
-            "stage_avg_ms": avg, "stage_achieved_gbs": bytes_stage / (avg / 1e3) / 1e9,
-            "state_vs_fp64": {"l1": float(d.mean()), "linf": float(d.max()),
-                              "after_steps": int(rep["iterations"]),
-                              "norm": "per variable, relative to max|U_fp64|"}}
+    out = {"value": n * nrk * done / (rep["device_ms"] / 1e3), "unit": UNIT,
+           "ms_per_step": rep["device_ms"] / max(done, 1), "dtype": "f32 flux / f64 accumulation",
+           "stage_avg_ms": avg, "stage_achieved_gbs": bytes_stage / (avg / 1e3) / 1e9,
+           "state_vs_fp64": {"l1": float(d.mean()), "linf": float(d.max()),
+                             "after_steps": int(rep["iterations"]),
+                             "norm": "per variable, relative to max|U_fp64|"}}
+    if oracle_steps > 0:
+        # against the FP64 oracle (C restatement, pinned bit for bit to the
+        # compiled reference) after the same steps from the initial state
+        from oracle import restated
+        s = cc.Solver(case, reorder=True)
+        s.run(oracle_steps)
+        pm = s.get_state()
+        s.close()
+        po, _ = restated.run_explicit(case, nsteps=oracle_steps)
+        e = np.abs(pm - po) / np.abs(po).max(axis=0)
+        out["state_vs_oracle"] = {"l1": float(e.mean()), "linf": float(e.max()), "after_steps": oracle_steps,
+                                  "norm": "per variable, relative to max|U_oracle|"}
+    return out
+
+
+def run_sod_c1(threads: int) -> dict:
+    """The small plain configuration: Sod shock tube, 400 x 20 quads, Roe,
+    second order Barth-Jespersen, RK3, CFL 0.5, to t_end = 0.2: device time
+    of the run against the compiled reference on the host cores (its own
+    time loop), and the final state's deviation from it."""
+    import ccfd_b200 as cc
+    from ccfd_b200 import meshgen
+    from oracle import refdump
+    ini = meshgen.sod_ini(400, 20, t_end=0.2, flux=2, order=2, limiter=1, cfl=0.5)
+    case = cc.CaseData.from_text(ini)
+    s = cc.Solver(case, reorder=True)
+    s.run(3)  # warm-up (graph capture); the timed run starts again from t = 0
+    s.close()
+    s = cc.Solver(case, reorder=True)
+    rep = s.run(0)
+    prim = s.get_state()
+    s.close()
+    n, steps = case.n_cells, int(rep["iterations"])
+    out = {"workload": "Sod shock tube, 400x20 quads (8,000 cells), Roe, 2nd order Barth-Jespersen, RK3, "
+                       "CFL 0.5, t_end 0.2, FP64",
+           "cells": n, "steps": steps, "gpu_ms": rep["device_ms"],
+           "gpu_cell_updates_per_s": n * 3 * steps / (rep["device_ms"] / 1e3),
+           "note": "8,000 cells fit in L2: launch-bound, not a roofline workload"}
+    if refdump.have_ref("euler", fast=True):
+        os.environ["OMP_PROC_BIND"] = "close"
+        os.environ["OMP_PLACES"] = "cores"
+        d = refdump.run_ref(ini, "run", 0, fast=True, threads=threads)
+        wall = float(d["step_wall"][-1])
+        ref = d["pvar"].reshape(-1, 4)
+        out["reference"] = {"wall_s": wall, "cell_updates_per_s": n * 3 * int(d["run_info"][1]) / wall,
+                            "threads": threads, "steps": int(d["run_info"][1])}
+        out["state_vs_reference_linf"] = float(np.abs(prim - ref).max())
+    return out
+
+
+def run_airfoil_c3(steps: int = 3) -> dict:
+    """The implicit Navier-Stokes configuration's mesh and physics (NACA
+    0012 O-grid 256 x 128 quads, first cell 1e-4 chord, far field 20 chords,
+    Mach 0.5, Re 5,000, AoA 1 deg, Roe, VK K=5, JFNK-GMRES Krylov 30 with
+    LU-SGS, CFL 10): `steps` implicit steps on the GPU against the restated
+    oracle (block-sparse buildMatrix / LU-SGS; the reference's dense Jacobian
+    would need 137 GB) timed on one host core."""
+    import ccfd_b200 as cc
+    from ccfd_b200 import meshgen
+    from oracle import restated
+    with tempfile.TemporaryDirectory() as tmp:
+        meshgen.naca_ogrid(0.0, 0.0, 0.12, 256, 128, r_far=20.0, h0=1e-4, wall_code=201).write_gmsh(
+            os.path.join(tmp, "c3.msh"))
+        ini = meshgen.airfoil_ini("c3", mach=0.5, alpha=1.0, navier_stokes=True, reynolds=5000.0, flux=2,
+                                  implicit=True, precond=True, n_kdim=30, cfl=10.0, max_iter=100)
+        case = cc.CaseData.from_text(ini, tmp)
+    s = cc.Solver(case, reorder=True)
+    s.run(1)  # warm-up (set-up of the lockstep set)
+    s.close()
+    s = cc.Solver(case, reorder=True)
+    rep = s.run(steps)
+    prim = s.get_state()
+    s.close()
+    t0 = time.perf_counter()
+    po, info, _ = restated.run_implicit(case, steps)
+    cpu_s = time.perf_counter() - t0
+    n = case.n_cells
+    return {"workload": "NACA 0012 O-grid 256x128 (32,768 cells), Navier-Stokes Re 5000, Mach 0.5, AoA 1 deg, "
+                        f"Roe, VK K=5, JFNK-GMRES(30) + LU-SGS, CFL 10, {steps} implicit steps",
+            "cells": n, "newton_iterations": rep["newton_iterations"], "gmres_iterations": rep["gmres_iterations"],
+            "gpu_ms_per_step": rep["device_ms"] / steps,
+            "restated_cpu": {"s_per_step": cpu_s / steps, "cores": 1, "kind": "restated",
+                             "newton_iterations": info["newton_iterations"],
+                             "gmres_iterations": info["gmres_iterations"]},
+            "speedup_vs_restated_cpu": (cpu_s / steps) / (rep["device_ms"] / 1e3 / steps),
+            "state_vs_restated": float((np.abs(prim - po).max(axis=0) / np.abs(po).max(axis=0)).max()),
+            "cl_cd_vs_restated": [abs(rep["cl"] - info["cl"]), abs(rep["cd"] - info["cd"])]}
 
 
 def run_batched_airfoils(n_cases: int, steps: int, cfl: float) -> dict:
@@ -307,7 +395,7 @@ def run_serving(n_req: int, load: float, budget: int, seed: int = 20260005) -> d
     arrival times (first come, first served, measured service times)."""
     import ccfd_b200 as cc
     from ccfd_b200 import workloads
-    reqs = workloads.stream_specs(n_req, seed, riemann_n=(256, 768), cylinder_cells=(50_000, 100_000))
+    reqs = workloads.stream_specs(n_req, seed, riemann_n=(256, 2048), cylinder_cells=(50_000, 400_000))
     with tempfile.TemporaryDirectory() as tmp:
         cases = [workloads.stream_case(r, tmp, f"q{k}") for k, r in enumerate(reqs)]
     # plain loop: per request upload, run, read the result back, release
@@ -321,7 +409,7 @@ def run_serving(n_req: int, load: float, budget: int, seed: int = 20260005) -> d
         service.append(time.perf_counter() - t0)
         service_dev.append(rep["device_ms"] / 1e3)
 
-    def serve(arrivals):
+    def serve(arrivals, budget=budget):
         srv = cc.Server(0, hbm_budget_bytes=budget, max_running=4096)
         ids, done, lat = {}, {}, {}
         order = np.argsort(arrivals, kind="stable")
@@ -351,8 +439,14 @@ def run_serving(n_req: int, load: float, budget: int, seed: int = 20260005) -> d
         srv.close()
         return done, lat, makespan, max_used, host
 
-    done, _, makespan_all, _, host_all = serve(np.zeros(len(cases)))
+    done, _, makespan_all, max_used_all, host_all = serve(np.zeros(len(cases)))
     capacity = len(cases) / makespan_all
+    # admission under pressure: the closed loop again with a budget of 1.5x
+    # the largest request's estimate, so requests wait for memory to free up
+    est = [cc.estimate_device_bytes(c) for c in cases]
+    tight = int(1.5 * max(est))
+    done_t, _, makespan_t, max_used_t, _ = serve(np.zeros(len(cases)), budget=tight)
+    same_t = all(np.array_equal(done_t[j][1], done[j][1]) for j in range(len(cases)))
     rate = load * capacity
     rng = np.random.Generator(np.random.PCG64(seed + 7))
     arrivals = np.cumsum(rng.exponential(1.0 / rate, len(cases)))
@@ -371,9 +465,13 @@ def run_serving(n_req: int, load: float, budget: int, seed: int = 20260005) -> d
     return {
         "workload": f"{n_req} requests (seed {seed}): " + ", ".join(
             f"{kinds.count(k)} {k}" for k in ("riemann", "cylinder", "airfoil"))
-            + "; Riemann 256^2..768^2 quads HLLC 200 RK3 steps, cylinder NS Re 100 M 0.2 50k..100k "
+            + "; Riemann 256^2..2048^2 quads HLLC 200 RK3 steps, cylinder NS Re 100 M 0.2 50k..400k "
               "triangles 1000 RK3 steps, airfoils 5 implicit steps (JFNK + LU-SGS, CFL 1)",
         "cells_total": int(sum(cells)), "hbm_budget_bytes": budget, "max_resident_bytes": int(max_used),
+        "max_resident_bytes_closed_loop": int(max_used_all),
+        "tight_budget": {"hbm_budget_bytes": tight, "largest_request_estimate": int(max(est)),
+                         "sum_of_estimates": int(sum(est)), "max_resident_bytes": int(max_used_t),
+                         "capacity_solves_per_s": len(cases) / makespan_t, "results_equal": bool(same_t)},
         "capacity_solves_per_s": capacity, "arrival_rate_per_s": rate, "load": load,
         "served": {"solves_per_s": len(cases) / makespan, "p50_s": float(np.percentile(lat_s, 50)),
                    "p99_s": float(np.percentile(lat_s, 99))},
@@ -517,6 +615,8 @@ def main() -> int:
     ap.add_argument("--no-mixed", action="store_true", help="skip the mixed-precision run")
     ap.add_argument("--no-batch", action="store_true", help="skip the batched-airfoil comparison")
     ap.add_argument("--no-serve", action="store_true", help="skip the served stream")
+    ap.add_argument("--no-configs", action="store_true",
+                    help="skip the Sod 400x20 and the 32k-cell Navier-Stokes airfoil legs")
     ap.add_argument("--airfoils", type=int, default=32)
     ap.add_argument("--airfoil-steps", type=int, default=5)
     ap.add_argument("--requests", type=int, default=24)
@@ -595,13 +695,17 @@ def main() -> int:
         bytes_fused = algorithmic_bytes_per_stage(m, venk=True)
         mixed = None
         if not args.no_mixed:
-            mixed = run_mixed(tmp, args.steps, args.warmup, prim_fp64, nrk, bytes_stage)
-        batched = serving = None
+            mixed = run_mixed(tmp, args.steps, args.warmup, prim_fp64, nrk, bytes_stage,
+                              oracle_steps=0 if args.no_cpu else 2)
+        batched = serving = sod = c3 = None
         if rank == 0 or world > 1:
             if not args.no_batch:
                 batched = run_batched_airfoils(args.airfoils, args.airfoil_steps, cfl=1.0)
             if not args.no_serve:
                 serving = run_serving(args.requests, load=0.8, budget=150 * 10**9)
+            if not args.no_configs:
+                sod = run_sod_c1(host_cpu()["physical_cores"])
+                c3 = None if args.no_cpu else run_airfoil_c3()
         avg_res_ms = res_ms / max(res_cnt, 1)
         achieved = bytes_stage / (avg_res_ms / 1e3) / 1e9
         traffic, traffic_note = stage_traffic()
@@ -656,6 +760,8 @@ def main() -> int:
             "mixed_precision": mixed,
             "batched_airfoils": batched,
             "serving": serving,
+            "sod_400x20": sod,
+            "airfoil_ns_32k": c3,
         }
         print(json.dumps(line), flush=True)
     if dist is not None:
