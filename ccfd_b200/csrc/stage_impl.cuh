@@ -30,6 +30,7 @@
 #include <cuda_runtime.h>
 
 #include <atomic>
+#include <map>
 #include <mutex>
 
 #include "kernels.cuh"
@@ -674,14 +675,16 @@ __global__ void __launch_bounds__(StageShape<FT>::threads, StageShape<FT>::min_b
     stage_body<FLUX, ORDER, NS, FT>(L, blockIdx.x);
 }
 
-// many instances in one launch over their concatenated tiles: CTA b runs
-// tile tmap[b].y of instance tmap[b].x.  An RK stage takes the instance's
-// launch record for the stage and the buffer parity in its control block
-// (Ls[inst][par][stage]); a residual evaluation (stride 1) takes
-// Ls[inst] and is skipped while *skip is nonzero.
+// Many instances in one persistent launch over their concatenated tiles:
+// each CTA walks the tile map (entries blockIdx.x, blockIdx.x + gridDim.x,
+// ...; entry b is tile tmap[b].y of instance tmap[b].x), so uneven
+// instances share one grid sized to the device.  An RK stage takes the
+// instance's launch record for the stage and the buffer parity in its
+// control block (Ls[inst][par][stage]); a residual evaluation (stride 1)
+// takes Ls[inst] and is skipped while *skip is nonzero.
 template <int FLUX, int ORDER, int NS, typename FT>
 __global__ void __launch_bounds__(StageShape<FT>::threads, StageShape<FT>::min_blocks)
-    k_stage_batch(const StageLaunch* __restrict__ Ls, const int2* __restrict__ tmap, int rk_mode,
+    k_stage_batch(const StageLaunch* __restrict__ Ls, const int2* __restrict__ tmap, int n_tiles, int rk_mode,
                   int stage) {
     // The member's launch record goes to shared memory.  In RK mode the
     // records of both buffer parities are copied while one thread reads the
@@ -691,7 +694,9 @@ __global__ void __launch_bounds__(StageShape<FT>::threads, StageShape<FT>::min_b
     constexpr int W = (int)(sizeof(StageLaunch) / 16);
     __shared__ int4 s_rec[2 * W];
     __shared__ int s_go, s_sel;
-    const int2 tm = tmap[blockIdx.x];
+    for (int b = blockIdx.x; b < n_tiles; b += gridDim.x) {
+    __syncthreads();  // the previous entry's record is no longer read
+    const int2 tm = tmap[b];
     if (rk_mode) {
         const StageLaunch* rec = Ls + (size_t)tm.x * 2 * kBatchStages;
         const int4* a = reinterpret_cast<const int4*>(rec + stage);
@@ -712,12 +717,46 @@ __global__ void __launch_bounds__(StageShape<FT>::threads, StageShape<FT>::min_b
         }
     }
     __syncthreads();
-    if (!s_go) return;
+    if (!s_go) continue;
     const StageLaunch& L = *reinterpret_cast<const StageLaunch*>(s_rec + s_sel * W);
-    if (L.mode < 0) return;
+    if (L.mode < 0) continue;
     stage_body<FLUX, ORDER, NS, FT>(L, tm.y);
+    }
 }
 
+
+// grid of a persistent launch: as many CTAs as the device holds at once
+// (SMs x resident CTAs per SM), at most one per tile; the occupancy is
+// looked up once per kernel, shared-memory size and device
+template <typename K>
+inline int persistent_grid(K kern, int threads, int smem, int n_tiles) {
+    struct Key {
+        const void* k;
+        int smem, dev;
+        bool operator<(const Key& o) const {
+            return k != o.k ? k < o.k : smem != o.smem ? smem < o.smem : dev < o.dev;
+        }
+    };
+    static std::mutex mu;
+    static std::map<Key, int> cache;
+    int dev = 0;
+    cudaGetDevice(&dev);
+    const Key key{reinterpret_cast<const void*>(kern), smem, dev};
+    int slots;
+    {
+        std::lock_guard<std::mutex> lk(mu);
+        auto it = cache.find(key);
+        if (it == cache.end()) {
+            int sms = 1, per = 1;
+            cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+            if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kern, threads, smem) != cudaSuccess || per < 1)
+                per = 1;
+            it = cache.emplace(key, sms * per).first;
+        }
+        slots = it->second;
+    }
+    return n_tiles < slots ? n_tiles : slots;
+}
 
 template <typename FT>
 inline int stage_smem_bytes_t(const TileDev& T) {
