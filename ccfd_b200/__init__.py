@@ -176,7 +176,9 @@ def set_device(device: int) -> None:
 class Solver:
     """One case resident on the current CUDA device."""
 
-    def __init__(self, case: CaseData, reorder: bool = True, params: N.Params | None = None):
+    def __init__(self, case: CaseData, reorder: int = 1, params: N.Params | None = None):
+        """Upload a case; ``reorder`` is the device cell order (0 the
+        reference's numbering, 1 Hilbert curve, 2 reverse Cuthill-McKee)."""
         self.case = case
         self._ctx = C.c_void_p()
         prm = params if params is not None else case.params

@@ -275,7 +275,8 @@ extern "C" int ccfd_upload_case(ccfd_ctx* ctx, const ccfd_mesh* m, const ccfd_bc
     // cell order: Hilbert curve of the barycentres (or the reference order);
     // results do not depend on it, only the storage order changes
     std::vector<int>& cperm = S.cperm;
-    if (reorder) ccfd_hilbert_order(m, cperm);
+    if (reorder == 2) ccfd_rcm_order(m, cperm);
+    else if (reorder) ccfd_hilbert_order(m, cperm);
     else {
         cperm.resize(N);
         for (long i = 0; i < N; ++i) cperm[i] = (int)i;

@@ -74,6 +74,45 @@ void ccfd_hilbert_order(const ccfd_mesh* m, std::vector<int>& cell_order) {
     cell_order.swap(a);
 }
 
+// Reverse Cuthill-McKee ordering of the cell graph (face neighbours):
+// breadth-first levels from a cell of least degree (per connected
+// component), neighbours in order of increasing degree, the whole order
+// reversed (Cuthill and McKee 1969, George 1971).
+void ccfd_rcm_order(const ccfd_mesh* m, std::vector<int>& cell_order) {
+    const long N = m->n_cells;
+    std::vector<int> deg(N), order;
+    order.reserve(N);
+    for (long c = 0; c < N; ++c) {
+        int d = 0;
+        for (long h = m->hs_offset[c]; h < m->hs_offset[c + 1]; ++h) d += m->hs_nb[h] >= 0;
+        deg[c] = d;
+    }
+    std::vector<char> seen(N, 0);
+    std::vector<int> by_deg(N), nb;
+    for (long c = 0; c < N; ++c) by_deg[c] = (int)c;
+    std::stable_sort(by_deg.begin(), by_deg.end(), [&](int a, int b) { return deg[a] < deg[b]; });
+    for (int start : by_deg) {
+        if (seen[start]) continue;
+        seen[start] = 1;
+        size_t head = order.size();
+        order.push_back(start);
+        while (head < order.size()) {
+            const int c = order[head++];
+            nb.clear();
+            for (long h = m->hs_offset[c]; h < m->hs_offset[c + 1]; ++h) {
+                const long e = m->hs_nb[h];
+                if (e >= 0 && !seen[e]) {
+                    seen[e] = 1;
+                    nb.push_back((int)e);
+                }
+            }
+            std::stable_sort(nb.begin(), nb.end(), [&](int a, int b) { return deg[a] < deg[b]; });
+            order.insert(order.end(), nb.begin(), nb.end());
+        }
+    }
+    cell_order.assign(order.rbegin(), order.rend());
+}
+
 namespace {
 
 // tiles [ta, tb) built by one thread: their concatenated arrays and per-tile

@@ -38,6 +38,9 @@ struct TileSet {
 // the barycentres
 void ccfd_hilbert_order(const ccfd_mesh* m, std::vector<int>& cell_order);
 
+// device order of cells by reverse Cuthill-McKee on the face-neighbour graph
+void ccfd_rcm_order(const ccfd_mesh* m, std::vector<int>& cell_order);
+
 // Build the tiles for a mesh whose cells are already in device order.
 // cperm: device -> reference cell; cinv: reference -> device cell;
 // fdev: reference face -> device interior face id (-1 for boundary faces).

@@ -270,10 +270,12 @@ int ccfd_set_device(int device);
 /* Create a context on the current CUDA device.  Replaces the init* globals. */
 int ccfd_create(const ccfd_params *params, ccfd_ctx **out);
 void ccfd_destroy(ccfd_ctx *ctx);
-/* Upload mesh connectivity / geometry once (mesh.c output -> device SoA),
- * boundary table and exact-function data.  Optionally reorders cells and
- * faces for locality (reorder = 1: reverse Cuthill-McKee); results are
- * independent of the ordering. */
+/* Upload mesh connectivity / geometry once (mesh.c output -> device
+ * arrays), boundary table and exact-function data.  Cells (and faces, by
+ * owner) are stored in a locality order: reorder = 0 the reference's
+ * numbering, 1 a Hilbert curve through the barycentres (the fastest
+ * measured), 2 reverse Cuthill-McKee on the face-neighbour graph; results
+ * are independent of the ordering. */
 int ccfd_upload_case(ccfd_ctx *ctx, const ccfd_mesh *mesh, const ccfd_bc *bc,
 		     int n_bc, const ccfd_exact *exact, int reorder);
 /* State in reference cell order, [N][4], primitive or conservative.  Setting

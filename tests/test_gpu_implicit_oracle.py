@@ -132,3 +132,49 @@ def test_steady_state_matches_restated(ns):
     rho = np.abs(prim[:, 0] - po[:, 0]).max() / np.abs(po[:, 0]).max()
     assert rho <= TOL
     assert abs(rep["cl"] - info["cl"]) <= TOL and abs(rep["cd"] - info["cd"]) <= TOL
+
+
+def test_mixed_precision_steady_state_matches_fp64_oracle():
+    # FP32 Krylov basis and LU-SGS sweeps, FP64 residuals and Newton update:
+    # converged to the same relative residual of 1e-8, the steady state is
+    # the FP64 one
+    with tempfile.TemporaryDirectory() as tmp:
+        fp64 = _airfoil(tmp, 32, 12, False, cfl=20.0, max_iter=1500, ser=300.0)
+        mixed = _airfoil(tmp, 32, 12, False, cfl=20.0, max_iter=1500, ser=300.0, precision=1)
+    s = cc.Solver(mixed, reorder=True)
+    try:
+        rep = s.run(0)
+        prim = s.get_state()
+    finally:
+        s.close()
+    po, info, _ = restated.run_implicit(fp64, 0, ser_cfl_max=300.0)
+    assert rep["converged"] and info["converged"]
+    assert np.abs(prim[:, 0] - po[:, 0]).max() / np.abs(po[:, 0]).max() <= 1e-6
+    assert abs(rep["cl"] - info["cl"]) <= 1e-6 and abs(rep["cd"] - info["cd"]) <= 1e-6
+
+
+def test_mixed_batch_of_airfoils_converges_to_fp64_lift_and_drag():
+    # three airfoil flows converged in one batch, FP64 and mixed precision
+    flows = [(0.5, 2.0), (0.4, 1.0), (0.6, -1.0)]
+    results = {}
+    for precision in (0, 1):
+        cases = []
+        with tempfile.TemporaryDirectory() as tmp:
+            for mach, alpha in flows:
+                cases.append(_airfoil(tmp, 32, 12, False, cfl=20.0, max_iter=1500, ser=300.0, mach=mach,
+                                      alpha=alpha, precision=precision))
+        b = cc.Batch(0)
+        members = [cc.Solver(c) for c in cases]
+        try:
+            for m in members:
+                b.add(m, 0)
+            while b.step(64):
+                pass
+            results[precision] = [b.report(m) for m in members]
+        finally:
+            b.close()
+            for m in members:
+                m.close()
+    for r64, r32 in zip(results[0], results[1]):
+        assert r64["converged"] and r32["converged"]
+        assert abs(r64["cl"] - r32["cl"]) <= 1e-6 and abs(r64["cd"] - r32["cd"]) <= 1e-6
