@@ -109,20 +109,21 @@ __device__ __forceinline__ double4 to_d4(const float4& v) {
 
 // Limited least-squares gradient of one cell (src/reconstruction.c:25-192,
 // 252-312).  nbr(k, qn) fetches the k-th neighbour state in side order,
-// gw(k) the side's (GP.x, GP.y, w.x, w.y).
-template <typename T, class Nbr, class GW>
+// gw(k) the side's (GP.x, GP.y, w.x, w.y), gp(k) the side's GP again for
+// the limiter.  The limiter runs side by side (each side's offset is
+// fetched once and only two of its values are live); the minimum over
+// sides and variables does not depend on the order, so the result is the
+// reference's.
+template <typename T, class Nbr, class GW, class GP>
 __device__ __forceinline__ void cell_gradient(int limiter, const T q[4], int nh, T eps2, Nbr nbr,
-                                              GW gw, T ux[4], T uy[4]) {
+                                              GW gw, GP gp, T ux[4], T uy[4]) {
     T umin[4] = {q[0], q[1], q[2], q[3]}, umax[4] = {q[0], q[1], q[2], q[3]};
-    T gpx[4] = {0, 0, 0, 0}, gpy[4] = {0, 0, 0, 0};
 #pragma unroll
     for (int v = 0; v < 4; ++v) ux[v] = uy[v] = T(0.0);
 #pragma unroll
     for (int k = 0; k < 4; ++k) {
         if (k < nh) {
             double4 g = gw(k);
-            gpx[k] = T(g.x);
-            gpy[k] = T(g.y);
             const T wx = T(g.z), wy = T(g.w);
             T qn[4];
             nbr(k, qn);
@@ -137,26 +138,35 @@ __device__ __forceinline__ void cell_gradient(int limiter, const T q[4], int nh,
         }
     }
     T phi[4] = {T(1.0), T(1.0), T(1.0), T(1.0)};
+    T mn[4], mx[4];
 #pragma unroll
     for (int v = 0; v < 4; ++v) {
-        T mn = umin[v] - q[v], mx = umax[v] - q[v];
-        T mn2 = mn * mn, mx2 = mx * mx;
+        mn[v] = umin[v] - q[v];
+        mx[v] = umax[v] - q[v];
+    }
 #pragma unroll
-        for (int k = 0; k < 4; ++k) {
-            if (k < nh) {
-                T uD = ux[v] * gpx[k] + uy[v] * gpy[k];
+    for (int k = 0; k < 4; ++k) {
+        if (k < nh) {
+            T gpx, gpy;
+            gp(k, gpx, gpy);
+#pragma unroll
+            for (int v = 0; v < 4; ++v) {
+                T uD = ux[v] * gpx + uy[v] * gpy;
                 T pl = T(1.0);
                 if (limiter == 1) {
-                    if (uD > T(0.0)) pl = fmin(T(1.0), mx / uD);
-                    else if (uD < T(0.0)) pl = fmin(T(1.0), mn / uD);
+                    if (uD > T(0.0)) pl = fmin(T(1.0), mx[v] / uD);
+                    else if (uD < T(0.0)) pl = fmin(T(1.0), mn[v] / uD);
                 } else {
                     T uD2 = uD * uD;
-                    if (uD > T(0.0))
-                        pl = T(1.0) / uD * (((mx2 + eps2) * uD + T(2.0) * uD2 * mx) /
-                                            (mx2 + T(2.0) * uD2 + uD * mx + eps2));
-                    else if (uD < T(0.0))
-                        pl = T(1.0) / uD * (((mn2 + eps2) * uD + T(2.0) * uD2 * mn) /
-                                            (mn2 + T(2.0) * uD2 + uD * mn + eps2));
+                    if (uD > T(0.0)) {
+                        const T mx2 = mx[v] * mx[v];
+                        pl = T(1.0) / uD * (((mx2 + eps2) * uD + T(2.0) * uD2 * mx[v]) /
+                                            (mx2 + T(2.0) * uD2 + uD * mx[v] + eps2));
+                    } else if (uD < T(0.0)) {
+                        const T mn2 = mn[v] * mn[v];
+                        pl = T(1.0) / uD * (((mn2 + eps2) * uD + T(2.0) * uD2 * mn[v]) /
+                                            (mn2 + T(2.0) * uD2 + uD * mn[v] + eps2));
+                    }
                 }
                 phi[v] = fmin(phi[v], pl);
             }
@@ -526,7 +536,12 @@ __device__ __forceinline__ void stage_body(const StageLaunch& L, const int t) {
                 hgp[lo + k] = cvt2<FT>(g.x, g.y);
                 return g;
             };
-            cell_gradient<FT>(L.limiter, q, nh, eps2, nbr, gw, ux, uy);
+            auto gp = [&](int k, FT& x, FT& y) {
+                const V2 g = hgp[lo + k];
+                x = g.x;
+                y = g.y;
+            };
+            cell_gradient<FT>(L.limiter, q, nh, eps2, nbr, gw, gp, ux, uy);
             gs[2 * i] = mk4(ux);
             gs[2 * i + 1] = mk4(uy);
         }
