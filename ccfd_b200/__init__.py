@@ -88,6 +88,20 @@ def mesh_arrays(m: N.Mesh) -> dict:
     }
 
 
+def colour_cells(hs_offset: np.ndarray, hs_nb: np.ndarray, budget: int = -1) -> tuple[np.ndarray, int]:
+    """Distance-3 colouring of the face-neighbour graph that groups the
+    columns of the block-sparse buildMatrix (``ccfd_colour_cells``); budget 0:
+    greedy only, negative: the solver's default tabu-search budget."""
+    off = np.ascontiguousarray(hs_offset, dtype=np.int64)
+    nb = np.ascontiguousarray(hs_nb, dtype=np.int64)
+    n = len(off) - 1
+    color = np.zeros(max(n, 1), dtype=np.int32)
+    nc = C.c_int(0)
+    _check(N.lib.ccfd_colour_cells(n, _lptr(off), _lptr(nb), int(budget),
+                                   color.ctypes.data_as(C.POINTER(C.c_int)), C.byref(nc)), "colour_cells")
+    return color[:n], nc.value
+
+
 class CaseData:
     """A case built by the C host layer from a reference ``.ini`` file."""
 

@@ -115,6 +115,7 @@ def _load():
         "ccfd_build_matrix": (c_int, [C.c_void_p, c_double, c_double, P(c_double), P(c_double),
                                       P(c_double)]),
         "ccfd_lusgs": (c_int, [C.c_void_p, P(c_double), P(c_double)]),
+        "ccfd_colour_cells": (c_int, [C.c_long, P(C.c_long), P(C.c_long), C.c_long, P(C.c_int), P(C.c_int)]),
         "ccfd_set_profiling": (c_int, [C.c_void_p, c_int]),
         "ccfd_get_profile": (c_int, [C.c_void_p, P(c_double), P(c_long), c_int]),
         "ccfd_global_residual_noalloc": (c_int, [C.c_void_p, C.c_void_p, c_long, c_double,

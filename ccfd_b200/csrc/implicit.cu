@@ -46,6 +46,7 @@
 #include <vector>
 
 #include "ccfd_ctx.cuh"
+#include "colouring.h"
 #include "host/ccfd_host.h"
 #include "kernels.cuh"
 
@@ -914,53 +915,13 @@ int ccfd_implicit_setup(ccfd_ctx* ctx, const std::vector<int>& hs_off, const std
                         break;
                     }
             }
-        // distance-3 greedy colouring: a cell's colour differs from every
-        // cell within three face-neighbour steps.  The colour count depends
-        // on the order the greedy pass visits the cells; the Jacobian does
-        // not (any valid colouring gives the same entries), so the fewest
-        // colours of a few visiting orders win.
-        auto greedy = [&](const std::vector<int>& order, std::vector<int>& color) {
-            color.assign(N, -1);
-            std::vector<int> mark(N, -1), frontier, next, seen, used;
-            int ncol = 0;
-            for (long k = 0; k < N; ++k) {
-                const int d = order[k];
-                seen.clear();
-                frontier.assign(1, d);
-                mark[d] = d;
-                seen.push_back(d);
-                for (int r = 0; r < 3; ++r) {
-                    next.clear();
-                    for (int c : frontier)
-                        for (int h = hs_off[c]; h < hs_off[c + 1]; ++h) {
-                            int e = hs_nb[h];
-                            if (e >= 0 && mark[e] != d) {
-                                mark[e] = d;
-                                next.push_back(e);
-                                seen.push_back(e);
-                            }
-                        }
-                    frontier.swap(next);
-                }
-                used.assign(ncol + 1, 0);
-                for (int e : seen)
-                    if (color[e] >= 0) used[color[e]] = 1;
-                int c = 0;
-                while (c < ncol && used[c]) ++c;
-                color[d] = c;
-                if (c == ncol) ++ncol;
-            }
-            return ncol;
-        };
-        std::vector<int> color, trial, order(N);
-        for (long d = 0; d < N; ++d) order[d] = (int)d;
-        int ncol = greedy(order, color);
-        for (long i = 0; i < N; ++i) order[i] = ctx->dev_of_cell[i];  // reference numbering
-        int nc2 = greedy(order, trial);
-        if (nc2 < ncol) {
-            ncol = nc2;
-            color.swap(trial);
-        }
+        // distance-3 colouring: a cell's colour differs from every cell
+        // within three face-neighbour steps (greedy in device and in
+        // reference order, then colours removed by a bounded tabu search);
+        // any valid colouring gives the same entries
+        std::vector<int> color;
+        const int ncol = ccfd_distance3_colouring(N, hs_off.data(), hs_nb.data(), ctx->dev_of_cell.data(),
+                                                  ccfd_colouring_budget(N), color);
         std::vector<int> coff(ncol + 1, 0), ccells(N);
         for (long d = 0; d < N; ++d) coff[color[d] + 1]++;
         for (int c = 0; c < ncol; ++c) coff[c + 1] += coff[c];

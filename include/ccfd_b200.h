@@ -327,6 +327,15 @@ int ccfd_build_matrix(ccfd_ctx *ctx, double t, double dt, double *d, double *din
  * ccfd_build_matrix, b and x [N][4] in reference cell order (mixed
  * precision: the sweep runs on the FP32 blocks). */
 int ccfd_lusgs(ccfd_ctx *ctx, const double *b, double *x);
+/* The column grouping of the block-sparse buildMatrix: a distance-3
+ * colouring of the face-neighbour graph (the reference evaluates one column
+ * per residual, src/linearSolver.c:186-252; columns of cells more than three
+ * face-neighbour steps apart are evaluated in one residual pass).  hs_offset
+ * [n_cells + 1] and hs_nb (negative: boundary side) as in ccfd_mesh; budget:
+ * tabu-search moves per colour-removal attempt, negative for the default the
+ * solver uses.  Out: color_out [n_cells], *n_colors.  Host only. */
+int ccfd_colour_cells(long n_cells, const long *hs_offset, const long *hs_nb, long budget,
+                      int *color_out, int *n_colors);
 /* Profiling of the residual evaluations inside the timed step graphs: with
  * profiling on, every residual evaluation of a step (gradient, face flux and
  * update kernels of one Runge-Kutta stage) is bracketed by CUDA events on the
