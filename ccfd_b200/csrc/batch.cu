@@ -30,6 +30,7 @@ struct VariantGroup {
     int n_tiles = 0, smem_bytes = 0;
     StageLaunch* d_recs = nullptr;
     int2* d_tmap = nullptr;
+    int* d_ctr = nullptr;  // tile claim counters of the group's launches
 };
 
 __global__ void k_gather_ctrl(const Ctrl* const* __restrict__ src, Ctrl* __restrict__ dst, int n) {
@@ -81,6 +82,7 @@ static void drop_group_memory(ccfd_batch* b) {
     for (auto& g : b->groups) {
         if (g.d_recs) cudaFreeAsync(g.d_recs, b->stream);
         if (g.d_tmap) cudaFreeAsync(g.d_tmap, b->stream);
+        if (g.d_ctr) cudaFreeAsync(g.d_ctr, b->stream);
     }
     b->groups.clear();
     for (auto& g : b->graph)
@@ -160,6 +162,8 @@ static int rebuild(ccfd_batch* b) {
         g.smem_bytes = stage_smem_bytes(big, g.fp32);
         CKB(ccfd_malloc_async((void**)&g.d_recs, sizeof(StageLaunch) * recs.size(), b->stream));
         CKB(ccfd_malloc_async((void**)&g.d_tmap, sizeof(int2) * tmap.size(), b->stream));
+        CKB(ccfd_malloc_async((void**)&g.d_ctr, sizeof(int) * 2, b->stream));
+        CKB(cudaMemsetAsync(g.d_ctr, 0, sizeof(int) * 2, b->stream));
         CKB(cudaMemcpyAsync(g.d_recs, recs.data(), sizeof(StageLaunch) * recs.size(), cudaMemcpyHostToDevice,
                             b->stream));
         CKB(cudaMemcpyAsync(g.d_tmap, tmap.data(), sizeof(int2) * tmap.size(), cudaMemcpyHostToDevice,
@@ -205,6 +209,7 @@ static void launch_steps(ccfd_batch* b, int steps) {
                 BatchLaunch B;
                 B.recs = g.d_recs;
                 B.tmap = g.d_tmap;
+                B.ctr = g.d_ctr;
                 B.n_tiles = g.n_tiles;
                 B.smem_bytes = g.smem_bytes;
                 B.rk_mode = 1;

@@ -1022,6 +1022,7 @@ struct ImpGroup {
     int n_tiles = 0, smem = 0;
     StageLaunch *rec_mv = nullptr, *rec_nt = nullptr, *rec_jac = nullptr;
     int2* tmap = nullptr;
+    int* ctr = nullptr;  // tile claim counters of the group's launches
 };
 
 struct ImpSet {
@@ -1046,6 +1047,7 @@ static void set_free(ImpSet* M) {
         cudaFreeAsync(g.rec_nt, M->stream);
         cudaFreeAsync(g.rec_jac, M->stream);
         cudaFreeAsync(g.tmap, M->stream);
+        cudaFreeAsync(g.ctr, M->stream);
     }
     if (M->dev) cudaFreeAsync(M->dev, M->stream);
     if (M->d_count) cudaFreeAsync(M->d_count, M->stream);
@@ -1175,6 +1177,8 @@ static int set_build(const std::vector<ccfd_ctx*>& members, cudaStream_t stream,
         CKM(ccfd_malloc_async((void**)&g.rec_nt, rb, stream));
         CKM(ccfd_malloc_async((void**)&g.rec_jac, rb, stream));
         CKM(ccfd_malloc_async((void**)&g.tmap, sizeof(int2) * tmap.size(), stream));
+        CKM(ccfd_malloc_async((void**)&g.ctr, sizeof(int) * 2, stream));
+        CKM(cudaMemsetAsync(g.ctr, 0, sizeof(int) * 2, stream));
         CKM(cudaMemcpyAsync(g.rec_mv, mv.data(), rb, cudaMemcpyHostToDevice, stream));
         CKM(cudaMemcpyAsync(g.rec_nt, nt.data(), rb, cudaMemcpyHostToDevice, stream));
         CKM(cudaMemcpyAsync(g.rec_jac, jac.data(), rb, cudaMemcpyHostToDevice, stream));
@@ -1192,6 +1196,7 @@ static void residuals(ImpSet* M, RecKind kind) {
         BatchLaunch B;
         B.recs = kind == REC_MV ? g.rec_mv : kind == REC_NT ? g.rec_nt : g.rec_jac;
         B.tmap = g.tmap;
+        B.ctr = g.ctr;
         B.n_tiles = g.n_tiles;
         B.smem_bytes = g.smem;
         B.rk_mode = 0;

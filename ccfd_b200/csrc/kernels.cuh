@@ -78,6 +78,7 @@ struct BatchLaunch {
     int n_tiles, smem_bytes;
     int rk_mode, stage;
     int flux_id, order, ns, fp32;
+    int* ctr;                 // [2] tile claim counter and finished CTAs, zero between launches
 };
 
 void launch_stage(const StageLaunch& L, cudaStream_t st);

@@ -691,16 +691,20 @@ __global__ void __launch_bounds__(StageShape<FT>::threads, StageShape<FT>::min_b
 }
 
 // Many instances in one persistent launch over their concatenated tiles:
-// each CTA walks the tile map (entries blockIdx.x, blockIdx.x + gridDim.x,
-// ...; entry b is tile tmap[b].y of instance tmap[b].x), so uneven
-// instances share one grid sized to the device.  An RK stage takes the
-// instance's launch record for the stage and the buffer parity in its
-// control block (Ls[inst][par][stage]); a residual evaluation (stride 1)
-// takes Ls[inst] and is skipped while *skip is nonzero.
+// each CTA claims the next entry of the tile map from a counter (entry b is
+// tile tmap[b].y of instance tmap[b].x) until none is left, so uneven
+// instances share one grid sized to the device, and CTAs that cannot start
+// at once (SMs held by other work of the device) leave their share to the
+// running ones instead of holding the launch back.  ctr[0] is the next
+// entry, ctr[1] the CTAs done; the last CTA to finish resets both for the
+// next launch on the stream.  An RK stage takes the instance's launch
+// record for the stage and the buffer parity in its control block
+// (Ls[inst][par][stage]); a residual evaluation (stride 1) takes Ls[inst]
+// and is skipped while *skip is nonzero.
 template <int FLUX, int ORDER, int NS, typename FT>
 __global__ void __launch_bounds__(StageShape<FT>::threads, StageShape<FT>::min_blocks)
     k_stage_batch(const StageLaunch* __restrict__ Ls, const int2* __restrict__ tmap, int n_tiles, int rk_mode,
-                  int stage) {
+                  int stage, int* __restrict__ ctr) {
     // The member's launch record goes to shared memory.  In RK mode the
     // records of both buffer parities are copied while one thread reads the
     // member's control block, so resolving the record costs one round trip
@@ -708,34 +712,42 @@ __global__ void __launch_bounds__(StageShape<FT>::threads, StageShape<FT>::min_b
     static_assert(sizeof(StageLaunch) % 16 == 0, "launch record copied in 16-byte words");
     constexpr int W = (int)(sizeof(StageLaunch) / 16);
     __shared__ int4 s_rec[2 * W];
-    __shared__ int s_go, s_sel;
-    for (int b = blockIdx.x; b < n_tiles; b += gridDim.x) {
-    __syncthreads();  // the previous entry's record is no longer read
-    const int2 tm = tmap[b];
-    if (rk_mode) {
-        const StageLaunch* rec = Ls + (size_t)tm.x * 2 * kBatchStages;
-        const int4* a = reinterpret_cast<const int4*>(rec + stage);
-        const int4* b = reinterpret_cast<const int4*>(rec + kBatchStages + stage);
-        for (int k = threadIdx.x; k < 2 * W; k += blockDim.x) s_rec[k] = k < W ? a[k] : b[k - W];
-        if (threadIdx.x == 0) {
-            const Ctrl* c = rec[0].ctrl;
-            s_go = c->active;
-            s_sel = c->par;
+    __shared__ int s_go, s_sel, s_b;
+    for (;;) {
+        __syncthreads();  // the previous entry's record is no longer read
+        if (threadIdx.x == 0) s_b = atomicAdd(&ctr[0], 1);
+        __syncthreads();
+        const int b = s_b;
+        if (b >= n_tiles) break;
+        const int2 tm = tmap[b];
+        if (rk_mode) {
+            const StageLaunch* rec = Ls + (size_t)tm.x * 2 * kBatchStages;
+            const int4* a = reinterpret_cast<const int4*>(rec + stage);
+            const int4* c = reinterpret_cast<const int4*>(rec + kBatchStages + stage);
+            for (int k = threadIdx.x; k < 2 * W; k += blockDim.x) s_rec[k] = k < W ? a[k] : c[k - W];
+            if (threadIdx.x == 0) {
+                const Ctrl* cb = rec[0].ctrl;
+                s_go = cb->active;
+                s_sel = cb->par;
+            }
+        } else {
+            const int4* a = reinterpret_cast<const int4*>(Ls + tm.x);
+            for (int k = threadIdx.x; k < W; k += blockDim.x) s_rec[k] = a[k];
+            if (threadIdx.x == 0) {
+                const int* skip = Ls[tm.x].skip;
+                s_go = !(skip && *skip);
+                s_sel = 0;
+            }
         }
-    } else {
-        const int4* a = reinterpret_cast<const int4*>(Ls + tm.x);
-        for (int k = threadIdx.x; k < W; k += blockDim.x) s_rec[k] = a[k];
-        if (threadIdx.x == 0) {
-            const int* skip = Ls[tm.x].skip;
-            s_go = !(skip && *skip);
-            s_sel = 0;
-        }
+        __syncthreads();
+        if (!s_go) continue;
+        const StageLaunch& L = *reinterpret_cast<const StageLaunch*>(s_rec + s_sel * W);
+        if (L.mode < 0) continue;
+        stage_body<FLUX, ORDER, NS, FT>(L, tm.y);
     }
-    __syncthreads();
-    if (!s_go) continue;
-    const StageLaunch& L = *reinterpret_cast<const StageLaunch*>(s_rec + s_sel * W);
-    if (L.mode < 0) continue;
-    stage_body<FLUX, ORDER, NS, FT>(L, tm.y);
+    if (threadIdx.x == 0 && atomicAdd(&ctr[1], 1) == (int)gridDim.x - 1) {
+        atomicExch(&ctr[0], 0);
+        atomicExch(&ctr[1], 0);
     }
 }
 
