@@ -89,6 +89,7 @@ struct ImpDev {
     int fp32;
     float4 *Vf, *Zf, *dxsf;
     float *Dinvf, *Of;
+    double4* rjb;  // mixed precision: R(U, t) of the FP32-flux evaluation, base of the Jacobian columns
     int* flag;  // [0] GMRES cycle done, [1] final m, [2] singular, [3] non-finite
     int* ctl;   // Ctl words
     Ctrl* ctrl;
@@ -113,6 +114,7 @@ struct ImpState {
     bool fp32 = false;           // mixed precision: the FP32 arrays below instead
     float4 *Vf = nullptr, *Zf = nullptr, *dxsf = nullptr;
     float *Dinvf = nullptr, *Of = nullptr;
+    double4* RJB = nullptr;      // mixed precision: base residual of the Jacobian columns
     double* sc = nullptr;        // device scalars
     int* flag = nullptr;         // [0] gmres done, [1] m_final, [2] singular, [3] non-finite
     int* ctl = nullptr;          // Ctl words
@@ -534,6 +536,16 @@ __global__ void kb_newton_check(const ImpDev* __restrict__ I) {
 }
 
 // ---------------------------------------------------------------- Jacobian
+// Perturbation of the finite-difference columns.  FP64: sqrt(DBL_EPSILON), as
+// buildMatrix (src/linearSolver.c:199).  Mixed precision evaluates the
+// columns with FP32 reconstruction and fluxes (the preconditioner only sets
+// how fast GMRES converges, not the converged state), where a step below the
+// FP32 resolution of the state would vanish: sqrt(FLT_EPSILON), the step that
+// balances truncation and rounding error, with an FP32-flux R(U) as base.
+__device__ __forceinline__ double jac_eps(const ImpDev& d) {
+    return d.fp32 ? sqrt((double)FLT_EPSILON) : sqrt(DBL_EPSILON);
+}
+
 // gate of colour c: members that build a preconditioner and have colour c
 __global__ void kb_jac_gate(const ImpDev* __restrict__ I, int c) {
     MEMBER;
@@ -556,7 +568,7 @@ __global__ void kb_jac_perturb(const ImpDev* __restrict__ I, int c, int v, int a
     const int off = d.color_off[c], n = d.color_off[c + 1] - off;
     int k = blockIdx.x * blockDim.x + threadIdx.x;
     if (k >= n) return;
-    const double reps = sqrt(DBL_EPSILON);
+    const double reps = jac_eps(d);
     int cell = d.color_cells[off + k];
     double q[4];
     ld(d.prim[cell], q);
@@ -572,18 +584,19 @@ __global__ void kb_jac_collect(const ImpDev* __restrict__ I, int c, int v) {
     const int off = d.color_off[c], n = d.color_off[c + 1] - off;
     int k = blockIdx.x * blockDim.x + threadIdx.x;
     if (k >= n) return;
-    const double sreps = 1.0 / sqrt(DBL_EPSILON);
+    const double sreps = 1.0 / jac_eps(d);
+    const double4* base = d.fp32 ? d.rjb : d.RXK;
     int cell = d.color_cells[off + k];
     double u[4], r[4];
     ld(d.ut[cell], u);
-    ld(d.RXK[cell], r);
+    ld(base[cell], r);
 #pragma unroll
     for (int j = 0; j < 4; ++j) d.D[16 * (long)cell + 4 * j + v] = 0.0 + (u[j] - r[j]) * sreps;
     for (int h = d.hs_off[cell]; h < d.hs_off[cell + 1]; ++h) {
         int e = d.hs_nb[h];
         if (e < 0) continue;
         ld(d.ut[e], u);
-        ld(d.RXK[e], r);
+        ld(base[e], r);
         long t = d.twin[h];
 #pragma unroll
         for (int j = 0; j < 4; ++j) {
@@ -897,6 +910,7 @@ int ccfd_implicit_setup(ccfd_ctx* ctx, const std::vector<int>& hs_off, const std
         if ((st = ialloc(ctx, &S->D, 16 * (size_t)N))) return st;
         if (S->fp32) {
             if ((st = ialloc(ctx, &S->Dinvf, 16 * (size_t)N)) || (st = ialloc(ctx, &S->Of, 16 * (size_t)H)) ||
+                (st = ialloc(ctx, &S->RJB, N)) ||
                 (st = ialloc(ctx, &S->dxsf, N)))
                 return st;
         } else if ((st = ialloc(ctx, &S->Dinv, 16 * (size_t)N)) || (st = ialloc(ctx, &S->O, 16 * (size_t)H)) ||
@@ -1019,8 +1033,9 @@ int ccfd_implicit_setup(ccfd_ctx* ctx, const std::vector<int>& hs_off, const std
 // columns at t) over the concatenated tiles of the members.
 struct ImpGroup {
     int flux, order, ns, fp32;
-    int n_tiles = 0, smem = 0;
-    StageLaunch *rec_mv = nullptr, *rec_nt = nullptr, *rec_jac = nullptr;
+    int jac32 = 0;       // Jacobian columns (and their base) with FP32 fluxes (mixed-precision members)
+    int n_tiles = 0, smem = 0, smem_jac = 0;
+    StageLaunch *rec_mv = nullptr, *rec_nt = nullptr, *rec_jac = nullptr, *rec_jb = nullptr;
     int2* tmap = nullptr;
     int* ctr = nullptr;  // tile claim counters of the group's launches
 };
@@ -1046,6 +1061,7 @@ static void set_free(ImpSet* M) {
         cudaFreeAsync(g.rec_mv, M->stream);
         cudaFreeAsync(g.rec_nt, M->stream);
         cudaFreeAsync(g.rec_jac, M->stream);
+        cudaFreeAsync(g.rec_jb, M->stream);
         cudaFreeAsync(g.tmap, M->stream);
         cudaFreeAsync(g.ctr, M->stream);
     }
@@ -1083,6 +1099,7 @@ static ImpDev make_dev(ccfd_ctx* ctx) {
     d.D = S->D; d.Dinv = S->Dinv; d.O = S->O; d.sc = S->sc; d.partial = S->partial;
     d.fp32 = S->fp32;
     d.Vf = S->Vf; d.Zf = S->Zf; d.dxsf = S->dxsf; d.Dinvf = S->Dinvf; d.Of = S->Of;
+    d.rjb = S->RJB;
     d.flag = S->flag;
     d.ctl = S->ctl;
     d.ctrl = ctx->ctrl;
@@ -1105,7 +1122,7 @@ static int set_build(const std::vector<ccfd_ctx*>& members, cudaStream_t stream,
     M->n = (int)members.size();
     M->stream = stream;
     std::vector<ImpDev> hd;
-    std::map<std::tuple<int, int, int, int>, std::vector<int>> by_variant;
+    std::map<std::tuple<int, int, int, int, int>, std::vector<int>> by_variant;
     for (int k = 0; k < M->n; ++k) {
         ccfd_ctx* ctx = members[k];
         ImpState* S = (ImpState*)ctx->implicit_state;
@@ -1125,7 +1142,7 @@ static int set_build(const std::vector<ccfd_ctx*>& members, cudaStream_t stream,
         }
         StageLaunch probe;
         ccfd_fill_stage(ctx, probe);
-        by_variant[std::make_tuple(probe.flux_id, probe.order, probe.ns, probe.fp32)].push_back(k);
+        by_variant[std::make_tuple(probe.flux_id, probe.order, probe.ns, probe.fp32, (int)S->fp32)].push_back(k);
     }
     CKM(ccfd_malloc_async((void**)&M->dev, sizeof(ImpDev) * M->n, stream));
     CKM(cudaMemcpyAsync(M->dev, hd.data(), sizeof(ImpDev) * M->n, cudaMemcpyHostToDevice, stream));
@@ -1133,9 +1150,9 @@ static int set_build(const std::vector<ccfd_ctx*>& members, cudaStream_t stream,
     M->h_count = &M->h_count_v;
     for (auto& kv : by_variant) {
         ImpGroup g;
-        std::tie(g.flux, g.order, g.ns, g.fp32) = kv.first;
+        std::tie(g.flux, g.order, g.ns, g.fp32, g.jac32) = kv.first;
         const std::vector<int>& idx = kv.second;
-        std::vector<StageLaunch> mv(idx.size()), nt(idx.size()), jac(idx.size());
+        std::vector<StageLaunch> mv(idx.size()), nt(idx.size()), jac(idx.size()), jb(idx.size());
         std::vector<int2> tmap;
         TileDev big;
         memset(&big, 0, sizeof(big));
@@ -1163,7 +1180,11 @@ static int set_build(const std::vector<ccfd_ctx*>& members, cudaStream_t stream,
             L.prim_in = ctx->prim_buf[ctx->cur ^ 1];
             L.u_t = S->ut;
             L.skip = S->ctl + CTL_SKIP_JAC;
+            L.fp32 = g.jac32;
             jac[j] = L;
+            // their base in mixed precision: R(U, t) with FP32 fluxes
+            L.u_t = S->RJB;
+            jb[j] = L;
             for (int t = 0; t < ctx->tiles.n_tiles; ++t) tmap.push_back(make_int2((int)j, t));
             big.max_e = std::max(big.max_e, ctx->tiles.max_e);
             big.max_g = std::max(big.max_g, ctx->tiles.max_g);
@@ -1172,10 +1193,15 @@ static int set_build(const std::vector<ccfd_ctx*>& members, cudaStream_t stream,
         }
         g.n_tiles = (int)tmap.size();
         g.smem = stage_smem_bytes(big, g.fp32);
+        g.smem_jac = stage_smem_bytes(big, g.jac32);
         size_t rb = sizeof(StageLaunch) * idx.size();
         CKM(ccfd_malloc_async((void**)&g.rec_mv, rb, stream));
         CKM(ccfd_malloc_async((void**)&g.rec_nt, rb, stream));
         CKM(ccfd_malloc_async((void**)&g.rec_jac, rb, stream));
+        if (g.jac32) {
+            CKM(ccfd_malloc_async((void**)&g.rec_jb, rb, stream));
+            CKM(cudaMemcpyAsync(g.rec_jb, jb.data(), rb, cudaMemcpyHostToDevice, stream));
+        }
         CKM(ccfd_malloc_async((void**)&g.tmap, sizeof(int2) * tmap.size(), stream));
         CKM(ccfd_malloc_async((void**)&g.ctr, sizeof(int) * 2, stream));
         CKM(cudaMemsetAsync(g.ctr, 0, sizeof(int) * 2, stream));
@@ -1189,24 +1215,53 @@ static int set_build(const std::vector<ccfd_ctx*>& members, cudaStream_t stream,
     return CCFD_OK;
 }
 
-enum RecKind { REC_MV, REC_NT, REC_JAC };
+// residual evaluations of a set: matrix-vector products, Newton residuals,
+// Jacobian columns, and the FP32-flux base of the columns of mixed-precision
+// members (their groups only)
+enum RecKind { REC_MV, REC_NT, REC_JAC, REC_JB };
 
 static void residuals(ImpSet* M, RecKind kind) {
     for (auto& g : M->groups) {
+        if (kind == REC_JB && !g.jac32) continue;
+        const bool jac = kind == REC_JAC || kind == REC_JB;
         BatchLaunch B;
-        B.recs = kind == REC_MV ? g.rec_mv : kind == REC_NT ? g.rec_nt : g.rec_jac;
+        B.recs = kind == REC_MV ? g.rec_mv : kind == REC_NT ? g.rec_nt : kind == REC_JAC ? g.rec_jac : g.rec_jb;
         B.tmap = g.tmap;
         B.ctr = g.ctr;
         B.n_tiles = g.n_tiles;
-        B.smem_bytes = g.smem;
+        B.smem_bytes = jac ? g.smem_jac : g.smem;
         B.rk_mode = 0;
         B.stage = 0;
         B.flux_id = g.flux;
         B.order = g.order;
         B.ns = g.ns;
-        B.fp32 = g.fp32;
+        B.fp32 = jac ? g.jac32 : g.fp32;
         launch_stage_batch(B, M->stream);
     }
+}
+
+// buildMatrix + calcDinv (src/linearSolver.c:186-252, :136-179) of the
+// members that build a preconditioner: a perturbed copy of the state, the
+// base of the mixed-precision columns, every colour and variable, blocks
+// and inverses
+static void build_jacobian(ImpSet* M, cudaStream_t st) {
+    const dim3 gv(M->max_nb, M->n), g1(1, M->n);
+    kb_jac_copy<<<gv, kB, 0, st>>>(M->dev);
+    if (M->pc32) {
+        kb_jac_gate<<<g1, 32, 0, st>>>(M->dev, 0);
+        residuals(M, REC_JB);
+    }
+    const dim3 gc((M->max_colsize + kB - 1) / kB, M->n);
+    for (int c = 0; c < M->max_col; ++c) {
+        kb_jac_gate<<<g1, 32, 0, st>>>(M->dev, c);
+        for (int v = 0; v < 4; ++v) {
+            kb_jac_perturb<<<gc, kB, 0, st>>>(M->dev, c, v, 1);
+            residuals(M, REC_JAC);
+            kb_jac_collect<<<gc, kB, 0, st>>>(M->dev, c, v);
+            kb_jac_perturb<<<gc, kB, 0, st>>>(M->dev, c, v, 0);
+        }
+    }
+    kb_jac_finish<<<gv, kB, 0, st>>>(M->dev);
 }
 
 static int count_on(ImpSet* M, int what, int* out) {
@@ -1237,19 +1292,7 @@ static int set_step(ImpSet* M) {
         kb_gmres_init<<<gv, kB, 0, st>>>(M->dev);
         kb_gmres_flags<<<g1, 32, 0, st>>>(M->dev);
         if (M->any_precond) {
-            // buildMatrix (src/linearSolver.c:186-252)
-            kb_jac_copy<<<gv, kB, 0, st>>>(M->dev);
-            const dim3 gc((M->max_colsize + kB - 1) / kB, M->n);
-            for (int c = 0; c < M->max_col; ++c) {
-                kb_jac_gate<<<g1, 32, 0, st>>>(M->dev, c);
-                for (int v = 0; v < 4; ++v) {
-                    kb_jac_perturb<<<gc, kB, 0, st>>>(M->dev, c, v, 1);
-                    residuals(M, REC_JAC);
-                    kb_jac_collect<<<gc, kB, 0, st>>>(M->dev, c, v);
-                    kb_jac_perturb<<<gc, kB, 0, st>>>(M->dev, c, v, 0);
-                }
-            }
-            kb_jac_finish<<<gv, kB, 0, st>>>(M->dev);
+            build_jacobian(M, st);
             kb_jac_check<<<g1, 32, 0, st>>>(M->dev);
         }
         for (int m = 0; m < M->max_K; ++m) {
@@ -1426,18 +1469,7 @@ extern "C" int ccfd_build_matrix(ccfd_ctx* ctx, double t, double dt, double* d_o
     else CK(cudaMemsetAsync(S->O, 0, sizeof(double) * 16 * (size_t)H, st));
     const dim3 gv(M->max_nb, M->n), g1(1, M->n);
     residuals(M, REC_NT);  // R_XK = R(U, t + dt)
-    kb_jac_copy<<<gv, kB, 0, st>>>(M->dev);
-    const dim3 gc((M->max_colsize + kB - 1) / kB, M->n);
-    for (int col = 0; col < M->max_col; ++col) {
-        kb_jac_gate<<<g1, 32, 0, st>>>(M->dev, col);
-        for (int v = 0; v < 4; ++v) {
-            kb_jac_perturb<<<gc, kB, 0, st>>>(M->dev, col, v, 1);
-            residuals(M, REC_JAC);
-            kb_jac_collect<<<gc, kB, 0, st>>>(M->dev, col, v);
-            kb_jac_perturb<<<gc, kB, 0, st>>>(M->dev, col, v, 0);
-        }
-    }
-    kb_jac_finish<<<gv, kB, 0, st>>>(M->dev);
+    build_jacobian(M, st);
     CK(cudaGetLastError());
     std::vector<double> D(16 * N), Di(16 * N), O(16 * H);
     int flag[8];

@@ -315,7 +315,9 @@ int ccfd_run_implicit(ccfd_ctx *ctx, long nsteps, ccfd_report *report);
 /* buildMatrix + calcDinv (src/linearSolver.c:186-252, :136-179) at the
  * context's state, as at the first Newton iteration of an implicit step from
  * time t with step dt: R_XK = R(U, t + dt), the finite-difference columns
- * R(U + sqrt(DBL_EPSILON) e_k, t) of the primitive variables.  Out (each may
+ * R(U + sqrt(DBL_EPSILON) e_k, t) of the primitive variables (mixed
+ * precision: columns and their base R(U, t) with FP32 reconstruction and
+ * fluxes, step sqrt(FLT_EPSILON); FP32 blocks).  Out (each may
  * be NULL), reference cell order, row-major 4x4 blocks (rows: residual
  * variables, columns: perturbed primitive variables): d and dinv [N][16],
  * the diagonal blocks of I - dt dR/dU and their inverses; off [H][16], per
