@@ -11,8 +11,11 @@
 // the cells of the removed colour take random colours, and single-cell
 // moves that reduce the number of conflicting pairs most (ties broken at
 // random, recently left colours forbidden for a while unless a move beats
-// the best count so far) run until no conflict is left or the move budget
-// of the attempt is spent.
+// the best count so far) run until no conflict is left or the attempt has
+// examined its budget of candidate moves (each move scans every
+// conflicting cell against every other colour, so the budget bounds the
+// work, not the number of moves: an attempt at a colour count below the
+// optimum keeps many conflicts and would otherwise take seconds).
 #include "colouring.h"
 
 #include <stdint.h>
@@ -79,8 +82,9 @@ int greedy(long n, const std::vector<long>& boff, const std::vector<int>& badj, 
     return ncol;
 }
 
-// one attempt at a k-colouring from `color` (colours >= k re-drawn); true
-// and the colouring in `color` on success
+// one attempt at a k-colouring from `color` (colours >= k re-drawn) that
+// examines at most `budget` candidate moves; true and the colouring in
+// `color` on success
 bool tabu_k(long n, const std::vector<long>& boff, const std::vector<int>& badj, int k, long budget, Rng& rng,
             std::vector<int>& color) {
     std::vector<int> c(color);
@@ -109,8 +113,9 @@ bool tabu_k(long n, const std::vector<long>& boff, const std::vector<int>& badj,
         }
     };
     for (long d = 0; d < n; ++d) update((int)d);
-    long best = conf;
-    for (long it = 1; conf > 0 && it <= budget; ++it) {
+    long best = conf, examined = 0;
+    for (long it = 1; conf > 0 && examined <= budget; ++it) {
+        examined += (long)confl.size() * (k - 1) + 1;
         int bv = -1, bc = -1, bd = 1 << 30, ties = 0;
         for (int v : confl) {
             const int* g = &gamma[(size_t)v * k];
@@ -152,7 +157,7 @@ bool tabu_k(long n, const std::vector<long>& boff, const std::vector<int>& badj,
 
 }  // namespace
 
-long ccfd_colouring_budget(long n) { return 4096 + n / 8; }
+long ccfd_colouring_budget(long n) { return 1000000 + 64 * n; }
 
 int ccfd_distance3_colouring(long n, const int* hs_off, const int* hs_nb, const int* order2, long budget,
                              std::vector<int>& color) {

@@ -334,8 +334,9 @@ int ccfd_lusgs(ccfd_ctx *ctx, const double *b, double *x);
  * per residual, src/linearSolver.c:186-252; columns of cells more than three
  * face-neighbour steps apart are evaluated in one residual pass).  hs_offset
  * [n_cells + 1] and hs_nb (negative: boundary side) as in ccfd_mesh; budget:
- * tabu-search moves per colour-removal attempt, negative for the default the
- * solver uses.  Out: color_out [n_cells], *n_colors.  Host only. */
+ * candidate moves (cell, colour) the tabu search examines per colour-removal
+ * attempt, 0 for greedy only, negative for the default the solver uses.
+ * Out: color_out [n_cells], *n_colors.  Host only. */
 int ccfd_colour_cells(long n_cells, const long *hs_offset, const long *hs_nb, long budget,
                       int *color_out, int *n_colors);
 /* Profiling of the residual evaluations inside the timed step graphs: with

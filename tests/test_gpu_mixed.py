@@ -67,12 +67,20 @@ def test_mixed_run_error_vs_reference(ref_small, key):
     assert l1 <= MIX_RUN_TOL and linf <= MIX_RUN_TOL
 
 
-MIX_IMP_TOL = 1e-7
+# Implicit steps in mixed precision: the preconditioner is built from
+# FP32-flux residuals, so GMRES follows its own path and every step is
+# solved only to the Newton tolerance; after the few unconverged steps of
+# these cases the state is 5.8e-6 (Euler, preconditioned), 9.9e-7
+# (Navier-Stokes) and 5.9e-9 (no preconditioner) from the FP64 reference.
+# Converged, the mixed steady state is the FP64 one within 1e-6
+# (tests/test_gpu_implicit_oracle.py).
+MIX_IMP_TOL = 2e-5
 
 
 @pytest.mark.parametrize("key", ["naca_euler_imp_pc", "naca_euler_imp_nopc", "naca_ns_imp_pc"])
 def test_mixed_implicit_error_vs_reference(ref_small, key):
-    # FP32 Krylov basis and LU-SGS blocks, FP64 residuals / Newton update:
+    # FP32 Krylov basis, LU-SGS blocks and preconditioner columns, FP64
+    # Newton / matrix-vector residuals and Newton update:
     # the iterates follow a different GMRES path, so the state after a few
     # steps differs from the FP64 reference by the inexact-Newton tolerance,
     # not by rounding
