@@ -274,17 +274,18 @@ class Solver:
         return ms.value, cnt.value
 
     def autotune(self, state: np.ndarray | None = None) -> dict:
-        """Pick the stage kernel's tile size and cell ordering by timing
-        (ccfd_autotune); the solver keeps the fastest and `state` (default:
-        the case's initial state)."""
+        """Pick the stage kernel's tile size, cell ordering and CTA size by
+        timing (ccfd_autotune); the solver keeps the fastest and `state`
+        (default: the case's initial state)."""
         c = self.case.c
         prim = np.ascontiguousarray(self.case.prim0() if state is None else state,
                                     dtype=np.float64).reshape(self.n, 4)
-        tc, ro, ms = C.c_int(), C.c_int(), C.c_double()
+        tc, ro, th, ms = C.c_int(), C.c_int(), C.c_int(), C.c_double()
         _check(N.lib.ccfd_autotune(self._ctx, C.byref(c.mesh), c.bc_table, c.n_bc_table,
                                    C.byref(c.exact), _dptr(prim), C.byref(tc), C.byref(ro),
-                                   C.byref(ms)), "ccfd_autotune")
-        return {"tile_cells": tc.value, "hilbert_order": bool(ro.value), "ms_per_residual": ms.value}
+                                   C.byref(th), C.byref(ms)), "ccfd_autotune")
+        return {"tile_cells": tc.value, "hilbert_order": bool(ro.value), "threads": th.value,
+                "ms_per_residual": ms.value}
 
     def device_bytes(self) -> int:
         b = C.c_size_t()

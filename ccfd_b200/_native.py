@@ -121,7 +121,7 @@ def _load():
         "ccfd_global_residual_noalloc": (c_int, [C.c_void_p, C.c_void_p, c_long, c_double,
                                                  C.c_void_p, C.c_void_p]),
         "ccfd_autotune": (c_int, [C.c_void_p, P(Mesh), P(BC), c_int, P(Exact), P(c_double), P(c_int),
-                                  P(c_int), P(c_double)]),
+                                  P(c_int), P(c_int), P(c_double)]),
         "ccfd_wall_cp": (c_int, [C.c_void_p, P(c_double), P(c_double), P(c_double), P(c_int), P(c_int)]),
         "ccfd_write_cp": (c_int, [C.c_void_p, C.c_char_p]),
         "ccfd_errors": (c_int, [C.c_void_p, c_int, P(c_double)]),

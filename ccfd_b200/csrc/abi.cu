@@ -188,6 +188,8 @@ extern "C" int ccfd_create(const ccfd_params* params, ccfd_ctx** out) {
     }
     const char* tc = getenv("CCFD_TILE_CELLS");
     if (tc) ctx->tile_cells = std::max(32, std::min(2048, atoi(tc)));
+    const char* th = getenv("CCFD_STAGE_THREADS");
+    if (th) ctx->stage_threads = std::max(0, std::min(1024, atoi(th))) & ~31;
     *out = ctx;
     return CCFD_OK;
 }
@@ -444,6 +446,7 @@ extern "C" int ccfd_upload_case(ccfd_ctx* ctx, const ccfd_mesh* m, const ccfd_bc
     td.max_hs = ts.max_hs;
     td.max_f = ts.max_f;
     td.smem_bytes = stage_smem_bytes(td, 0);  // FP64 staging: the larger of the two layouts
+    td.threads = ctx->stage_threads;
     int smem_max = 0;
     CK(cudaDeviceGetAttribute(&smem_max, cudaDevAttrMaxSharedMemoryPerBlockOptin, ctx->device));
     if (td.smem_bytes > smem_max) {
@@ -929,11 +932,15 @@ extern "C" int ccfd_get_history(ccfd_ctx* ctx, double* rows, long max_rows, long
 // and the summation order per cell are the same for every tiling).
 extern "C" int ccfd_autotune(ccfd_ctx* ctx, const ccfd_mesh* m, const ccfd_bc* bc, int n_bc,
                              const ccfd_exact* ex, const double* prim, int* tile_cells_out,
-                             int* reorder_out, double* ms_out) {
+                             int* reorder_out, int* threads_out, double* ms_out) {
     if (!ctx || !m || !ex || !prim) return CCFD_ERR_ARG;
     if (ctx->batch) return CCFD_ERR_BUSY;
     CK(cudaSetDevice(ctx->device));
     static const int kTiles[] = {128, 192, 256, 320, 384};
+    // CTA sizes at or below the precision's launch bounds (FP64 384, FP32 256)
+    static const int kThreads64[] = {256, 320, 384}, kThreads32[] = {128, 192, 256};
+    const bool fp32 = ctx->params.precision == CCFD_MIXED && !ctx->params.implicit;
+    const int* thr_list = fp32 ? kThreads32 : kThreads64;
     const int kReps = 5;
     // the two timing events are released on every return path
     struct Events {
@@ -946,32 +953,39 @@ extern "C" int ccfd_autotune(ccfd_ctx* ctx, const ccfd_mesh* m, const ccfd_bc* b
     CK(cudaEventCreate(&ev.a));
     CK(cudaEventCreate(&ev.b));
     double best = 1e300;
-    int best_tile = ctx->tile_cells, best_order = 1;
+    int best_tile = ctx->tile_cells, best_order = 1, best_threads = ctx->stage_threads;
     for (int order = 1; order >= 0; --order)
         for (int tc : kTiles) {
             ctx->tile_cells = tc;
             int st = ccfd_upload_case(ctx, m, bc, n_bc, ex, order);
             if (st == CCFD_ERR_ARG) continue;  // tile too large for shared memory
             if (st || (st = ccfd_set_state(ctx, prim, CCFD_PRIMITIVE))) return st;
-            if ((st = ccfd_residual_device(ctx, 0.0))) return st;  // warm-up
-            CK(cudaEventRecord(ev.a, ctx->stream));
-            for (int r = 0; r < kReps; ++r)
-                if ((st = ccfd_residual_device(ctx, 0.0))) return st;
-            CK(cudaEventRecord(ev.b, ctx->stream));
-            CK(cudaEventSynchronize(ev.b));
-            float ms = 0.0f;
-            CK(cudaEventElapsedTime(&ms, ev.a, ev.b));
-            if (ms / kReps < best) {
-                best = ms / kReps;
-                best_tile = tc;
-                best_order = order;
+            // the CTA size changes the launch only: time each on the same tiles
+            for (int k = 0; k < 3; ++k) {
+                ctx->tiles.threads = thr_list[k];
+                if ((st = ccfd_residual_device(ctx, 0.0))) return st;  // warm-up
+                CK(cudaEventRecord(ev.a, ctx->stream));
+                for (int r = 0; r < kReps; ++r)
+                    if ((st = ccfd_residual_device(ctx, 0.0))) return st;
+                CK(cudaEventRecord(ev.b, ctx->stream));
+                CK(cudaEventSynchronize(ev.b));
+                float ms = 0.0f;
+                CK(cudaEventElapsedTime(&ms, ev.a, ev.b));
+                if (ms / kReps < best) {
+                    best = ms / kReps;
+                    best_tile = tc;
+                    best_order = order;
+                    best_threads = thr_list[k];
+                }
             }
         }
     ctx->tile_cells = best_tile;
+    ctx->stage_threads = best_threads;
     int st = ccfd_upload_case(ctx, m, bc, n_bc, ex, best_order);
     if (!st) st = ccfd_set_state(ctx, prim, CCFD_PRIMITIVE);
     if (tile_cells_out) *tile_cells_out = best_tile;
     if (reorder_out) *reorder_out = best_order;
+    if (threads_out) *threads_out = best_threads;
     if (ms_out) *ms_out = best;
     return st;
 }

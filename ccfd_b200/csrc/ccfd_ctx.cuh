@@ -19,6 +19,7 @@ struct ccfd_ctx {
     ccfd::TileDev tiles;
     ccfd::GhostDev ghosts;
     int tile_cells = 256;
+    int stage_threads = 0;  // CTA size of the stage kernel, 0: the precision's default
     ccfd_exact exact;
     double rk[6];
     double total_area_q = 0.0;

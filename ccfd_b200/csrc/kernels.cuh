@@ -10,6 +10,8 @@ struct TileDev {
     int n_tiles;
     int smem_bytes;
     int max_e, max_g, max_hs, max_f;
+    int threads;          // CTA size of the single-instance stage kernel (0: the precision's default)
+    int pad_[3];          // launch records stay a whole number of 16-byte words
     const int* e_off;     // [n_tiles + 1]
     const int4* counts;   // [n_tiles] (nT, nG, nE cells, nE)
     const int* e_ref;     // staged entries: device cell or -1-g

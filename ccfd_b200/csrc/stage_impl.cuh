@@ -62,9 +62,14 @@ struct SmemLimit {
     }
 };
 
+// Launch bounds of the stage kernels (threads, CTAs per SM: they fix the
+// registers, 80 in FP64) and the CTA size of a single-instance launch when
+// the context sets none: in FP64 256 threads, three CTAs of a 256-cell tile
+// per SM (0.147 against 0.151 ms per stage at 384 threads on the
+// 500k-triangle double Mach reflection; 320 threads: 0.169).
 template <typename FT> struct StageShape;
-template <> struct StageShape<double> { static constexpr int threads = 384, min_blocks = 2; };
-template <> struct StageShape<float> { static constexpr int threads = 256, min_blocks = 3; };
+template <> struct StageShape<double> { static constexpr int threads = 384, min_blocks = 2, single = 256; };
+template <> struct StageShape<float> { static constexpr int threads = 256, min_blocks = 3, single = 256; };
 
 __device__ __forceinline__ double stage_time(const Ctrl* ctrl, double tfix, double a_time) {
     return ctrl ? ctrl->t + a_time * ctrl->dt : tfix;
@@ -481,7 +486,9 @@ __device__ __forceinline__ void stage_body(const StageLaunch& L, const int t) {
     const TileDev& T = L.tiles;
     const Phys& P = L.phys;
     const int tid = threadIdx.x;
-    constexpr int kThreads = StageShape<FT>::threads;
+    // CTA size: the precision's default shape, or a smaller one chosen for the
+    // context (the launch bounds fix the registers; work is strided by it)
+    const int nthr = blockDim.x;
     const int4 cnt = T.counts[t];
     const int nT = cnt.x, nG = cnt.y, nEc = cnt.z, nE = cnt.w;
     const int e0 = T.e_off[t];
@@ -498,7 +505,7 @@ __device__ __forceinline__ void stage_body(const StageLaunch& L, const int t) {
     // few registers are live, into a per-cell buffer that the same thread
     // reads back in D (same cell-to-thread mapping)
     if (m.cell_src)
-        for (int i = tid; i < nT; i += kThreads) {
+        for (int i = tid; i < nT; i += nthr) {
             const int d = d_first + i;
             m.src_buf[d] = cell_source(P, m.hs_gw, m.hs_off[d], m.hs_off[d + 1], m.cell_src[d],
                                        m.cell_geo[d].x, time);
@@ -508,9 +515,9 @@ __device__ __forceinline__ void stage_body(const StageLaunch& L, const int t) {
     // boundary state at their mirrored barycentre (second order only: the
     // reference sets ghost cell states in its second-order reconstruction
     // and leaves them zero otherwise)
-    for (int e = tid; e < nEc; e += kThreads)
+    for (int e = tid; e < nEc; e += nthr)
         ps[e] = cvt4<FT>(L.prim_in[e < nT ? d_first + e : T.e_ref[e0 + e]]);
-    for (int e = nEc + tid; e < nE; e += kThreads) {
+    for (int e = nEc + tid; e < nE; e += nthr) {
         int g = -1 - T.e_ref[e0 + e];
         double4 gq = make_double4(0.0, 0.0, 0.0, 0.0);
         if (ORDER == 2)
@@ -523,7 +530,7 @@ __device__ __forceinline__ void stage_body(const StageLaunch& L, const int t) {
     // B: limited gradients of the tile and ring-1 cells
     const int hb = T.hs_off[t], gb = T.gl_off[t];
     if (ORDER == 2) {
-        for (int i = tid; i < nG; i += kThreads) {
+        for (int i = tid; i < nG; i += nthr) {
             int d = i < nT ? d_first + i : T.e_ref[e0 + i];
             int h0 = m.hs_off[d], nh = m.hs_off[d + 1] - h0;
             int lo = T.hs_loc[gb + i];
@@ -550,7 +557,7 @@ __device__ __forceinline__ void stage_body(const StageLaunch& L, const int t) {
 
     // C: fluxes of the tile's faces (interior faces, then boundary faces)
     const int f0 = T.f_off[t], nF = T.f_off[t + 1] - f0;
-    for (int j = tid; j < nF; j += kThreads) {
+    for (int j = tid; j < nF; j += nthr) {
         int fid = T.f_id[f0 + j];
         int lr = T.f_lr[f0 + j];
         int il = lr & 0xffff, ir = lr >> 16;
@@ -606,7 +613,7 @@ __device__ __forceinline__ void stage_body(const StageLaunch& L, const int t) {
     double dconv = 1e150, dvisc = 1e150;
     int bad = 0;
     const bool rk = L.mode == 1;
-    for (int i = tid; i < nT; i += kThreads) {
+    for (int i = tid; i < nT; i += nthr) {
         int d = d_first + i;
         int h0 = m.hs_off[d], h1 = m.hs_off[d + 1];
         double s[4] = {0.0, 0.0, 0.0, 0.0};

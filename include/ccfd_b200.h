@@ -392,13 +392,15 @@ int ccfd_errors(ccfd_ctx *ctx, int exact_func, double out[12]);
 
 /* Autotuner (no counterpart in the reference): re-uploads the case with
  * each candidate launch shape of the stage kernel (cells per tile 128..384,
- * Hilbert or reference cell order), times residual evaluations of state prim
- * ([n_cells][4] primitive, reference order) and keeps the fastest; the
- * context ends uploaded with that shape and with prim as its state.  Results
- * are independent of the shape.  Outputs may be NULL. */
+ * Hilbert or reference cell order) and times residual evaluations of state
+ * prim ([n_cells][4] primitive, reference order) at each CTA size (FP64
+ * 256 / 320 / 384 threads, FP32 fluxes 128 / 192 / 256, so cells and faces
+ * per thread vary with the tile), keeps the fastest; the context ends
+ * uploaded with that shape and with prim as its state.  Results are
+ * independent of the shape.  Outputs may be NULL. */
 int ccfd_autotune(ccfd_ctx *ctx, const ccfd_mesh *m, const ccfd_bc *bc, int n_bc,
 		  const ccfd_exact *ex, const double *prim, int *tile_cells, int *reorder,
-		  double *ms_per_residual);
+		  int *threads, double *ms_per_residual);
 
 /* Final-solution output in the reference's format (dataOutput, csvOutput,
  * curveOutput, src/output.c:53-112, 253-398): outputFormat = 3 (CSV) or 2

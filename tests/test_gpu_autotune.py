@@ -1,8 +1,8 @@
 """Autotuner of the stage kernel's launch shape (ccfd_autotune): it must
 pick a valid candidate, leave the context uploaded with the given state, and
-— since tiling and cell order change only the storage and launch shape —
-give residuals and states bit-identical to the default shape (the global
-residual, a sum of per-tile partials, to the last bits)."""
+— since tiling, cell order and CTA size change only the storage and launch
+shape — give residuals and states bit-identical to the default shape (the
+global residual, a sum of per-tile partials, to the last bits)."""
 import tempfile
 
 import numpy as np
@@ -26,6 +26,7 @@ def test_autotuned_shape_gives_identical_results(ref_small, key):
     tuned = cc.Solver(case)
     info = tuned.autotune(prim)
     assert info["tile_cells"] in (128, 192, 256, 320, 384)
+    assert info["threads"] in (256, 320, 384)
     assert info["ms_per_residual"] > 0.0
     assert np.array_equal(tuned.get_state(), prim)
     ut1 = tuned.fv_time_derivative(spec["time"])
@@ -38,3 +39,25 @@ def test_autotuned_shape_gives_identical_results(ref_small, key):
     np.testing.assert_allclose(rep0["residual"], rep1["residual"], rtol=1e-13, atol=0.0)
     base.close()
     tuned.close()
+
+
+@pytest.mark.parametrize("threads", [256, 320])
+def test_smaller_cta_gives_identical_results(ref_small, threads, monkeypatch):
+    # every CTA size within the launch bounds: same residual and run
+    spec = CASES.residual_cases()["dmr_f05_vk"]
+    with tempfile.TemporaryDirectory() as tmp:
+        case, _, _ = CASES.load_case(spec, tmp)
+    prim = ref_small["dmr_f05_vk/prim"].reshape(-1, 4)
+    base = cc.Solver(case)
+    monkeypatch.setenv("CCFD_STAGE_THREADS", str(threads))
+    other = cc.Solver(case)
+    try:
+        base.set_state(prim)
+        other.set_state(prim)
+        assert np.array_equal(base.fv_time_derivative(spec["time"]), other.fv_time_derivative(spec["time"]))
+        base.run(5)
+        other.run(5)
+        assert np.array_equal(base.get_state(), other.get_state())
+    finally:
+        base.close()
+        other.close()
