@@ -66,10 +66,12 @@ struct SmemLimit {
 // registers, 80 in FP64) and the CTA size of a single-instance launch when
 // the context sets none: in FP64 256 threads, three CTAs of a 256-cell tile
 // per SM (0.147 against 0.151 ms per stage at 384 threads on the
-// 500k-triangle double Mach reflection; 320 threads: 0.169).
+// 500k-triangle double Mach reflection; 320 threads: 0.169); with FP32
+// staging 128 threads on 192-cell tiles (the context's default tile size
+// in that precision), six CTAs per SM.
 template <typename FT> struct StageShape;
 template <> struct StageShape<double> { static constexpr int threads = 384, min_blocks = 2, single = 256; };
-template <> struct StageShape<float> { static constexpr int threads = 256, min_blocks = 3, single = 256; };
+template <> struct StageShape<float> { static constexpr int threads = 256, min_blocks = 3, single = 128; };
 
 __device__ __forceinline__ double stage_time(const Ctrl* ctrl, double tfix, double a_time) {
     return ctrl ? ctrl->t + a_time * ctrl->dt : tfix;
