@@ -617,7 +617,8 @@ def main() -> int:
     ap.add_argument("--no-serve", action="store_true", help="skip the served stream")
     ap.add_argument("--no-configs", action="store_true",
                     help="skip the Sod 400x20 and the 32k-cell Navier-Stokes airfoil legs")
-    ap.add_argument("--airfoils", type=int, default=32)
+    ap.add_argument("--airfoils", type=int, default=256,
+                    help="airfoils of the batched set (the configuration's 256 by default)")
     ap.add_argument("--airfoil-steps", type=int, default=5)
     ap.add_argument("--requests", type=int, default=24)
     ap.add_argument("--nx", type=int, default=NX)
