@@ -185,7 +185,9 @@ int ccfd_distance3_colouring(long n, const int* hs_off, const int* hs_nb, const 
 extern "C" int ccfd_colour_cells(long n_cells, const long* hs_offset, const long* hs_nb, long budget,
                                  int* color_out, int* n_colors) {
     if (n_cells < 0 || (n_cells > 0 && (!hs_offset || !hs_nb || !color_out)) || !n_colors) return CCFD_ERR_ARG;
-    if (n_cells > 0 && hs_offset[n_cells] > 0x7fffffffL) return CCFD_ERR_ARG;
+    if (n_cells > 0 && (hs_offset[0] != 0 || hs_offset[n_cells] > 0x7fffffffL)) return CCFD_ERR_ARG;
+    for (long i = 0; i < n_cells; ++i)
+        if (hs_offset[i + 1] < hs_offset[i]) return CCFD_ERR_ARG;
     std::vector<int> off(n_cells + 1), nb(n_cells > 0 ? hs_offset[n_cells] : 0);
     for (long i = 0; i <= n_cells; ++i) off[i] = (int)hs_offset[i];
     for (size_t h = 0; h < nb.size(); ++h) {

@@ -70,6 +70,11 @@ def test_empty_and_bad_arguments():
     assert n == 0 and len(c) == 0
     with pytest.raises(cc.CcfdError):
         cc.colour_cells(np.array([0, 1], np.int64), np.array([5], np.int64))
+    # offsets must start at zero and never decrease
+    with pytest.raises(cc.CcfdError):
+        cc.colour_cells(np.array([0, 2, 1], np.int64), np.array([1, -1], np.int64))
+    with pytest.raises(cc.CcfdError):
+        cc.colour_cells(np.array([1, 2], np.int64), np.array([-1, -1], np.int64))
 
 
 def test_batched_airfoil_grid_takes_at_most_ten_colours():
